@@ -1,0 +1,101 @@
+/* ps26119_backend.h — C ABI of the GPU backend plugin (libps26119.so).
+ *
+ * The reference's internal plugin boundary is the C++ class pdhg::Backend
+ * (src/pdhg/backend.h:36-69) with make_backend(use_gpu, error) (backend.h:87): vector handles,
+ * spmv / spmv_t, fused r²HPDHG steps, fp64 reductions and the KKT evaluation. This header
+ * exposes the same operations over the GPU implementation with plain C types, so a reference
+ * maintainer (or a test) can drive the GPU op by op exactly as tests/unit/test_gpu.cpp:33-95
+ * drives the CUDA backend against the CPU one.
+ *
+ * Every function returns 0 on success and a non-zero PS26119_* status on failure (with the
+ * reason in the thread's last-error text, ps26119_backend_last_error). Nothing throws.
+ */
+#ifndef PS26119_B200_BACKEND_H
+#define PS26119_B200_BACKEND_H
+
+#ifndef PS26119_API
+#if defined(__GNUC__)
+#define PS26119_API __attribute__((visibility("default")))
+#else
+#define PS26119_API
+#endif
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct ps26119_backend ps26119_backend;
+
+/* Scaling options (reference src/pdhg/scaling.h:32-46); NULL = defaults
+ * (12 geometric-mean sweeps when the entries span 10^4.5, Ruiz 10, Pock–Chambolle, bound and
+ * objective rescaling). */
+typedef struct {
+  int geometric_mean_iterations;
+  double geometric_mean_min_log10_range;
+  int ruiz_iterations;
+  int pock_chambolle;
+  int bound_objective_rescaling;
+} ps26119_scaling_options;
+
+/* Creates the backend and runs Backend::setup on the GPU: uploads the CSC model (host arrays,
+ * same layout as ps26119_solve_lp) and builds the scaled problem on the device
+ * (make_scaled_problem, reference src/pdhg/scaling.cpp:37-142). exact = 1 takes every
+ * reduction in the reference's summation order. Replaces make_backend(true, error)
+ * (reference src/pdhg/cpu_backend.cpp:293-310) + Backend::setup. */
+PS26119_API int ps26119_backend_new(ps26119_backend** out, int num_rows, int num_cols, int sense, double obj_offset,
+                        const double* c, const double* col_lower, const double* col_upper,
+                        const double* row_lower, const double* row_upper, const int* col_start,
+                        const int* row_index, const double* value, const ps26119_scaling_options* so,
+                        int exact);
+PS26119_API void ps26119_backend_free(ps26119_backend* b);
+PS26119_API const char* ps26119_backend_last_error(void);
+
+/* Backend::set_precision / create / upload / download / fill / copy / axpby (backend.h:43-51) */
+PS26119_API int ps26119_backend_set_precision(ps26119_backend* b, int mixed);
+PS26119_API int ps26119_backend_create(ps26119_backend* b, int dual); /* returns the handle (>= 0), or -1 */
+PS26119_API int ps26119_backend_upload(ps26119_backend* b, int v, const double* src);
+PS26119_API int ps26119_backend_download(ps26119_backend* b, int v, double* dst);
+PS26119_API int ps26119_backend_fill(ps26119_backend* b, int v, double a);
+PS26119_API int ps26119_backend_copy(ps26119_backend* b, int dst, int src);
+PS26119_API int ps26119_backend_axpby(ps26119_backend* b, double a, int x, double bb, int y);
+/* Backend::spmv / spmv_t (backend.h:52-53) */
+PS26119_API int ps26119_backend_spmv(ps26119_backend* b, int x, int out);
+PS26119_API int ps26119_backend_spmv_t(ps26119_backend* b, int y, int out);
+/* Backend::dot / norm2 / diff_norm2 (backend.h:54-56), result in *out */
+PS26119_API int ps26119_backend_dot(ps26119_backend* b, int x, int y, double* out);
+PS26119_API int ps26119_backend_norm2(ps26119_backend* b, int x, double* out);
+PS26119_API int ps26119_backend_diff_norm2(ps26119_backend* b, int x, int y, double* out);
+/* Backend::primal_step / dual_step / r2h_primal / r2h_dual (backend.h:58-61); yb = -1 skips ȳ */
+PS26119_API int ps26119_backend_primal_step(ps26119_backend* b, int x, int aty, double tau, int xh);
+PS26119_API int ps26119_backend_dual_step(ps26119_backend* b, int y, int ax, double sigma, int yh);
+PS26119_API int ps26119_backend_r2h_primal(ps26119_backend* b, int x, int x0, int aty, double tau, double w, double rho,
+                               int xh, int xb);
+PS26119_API int ps26119_backend_r2h_dual(ps26119_backend* b, int y, int y0, int ax, double sigma, double w, double rho,
+                             int yh, int yb);
+/* The engine's fused kernels: Ãᵀy + r2h_primal in one launch, Ãx̄ + r2h_dual in one launch
+ * (no reference counterpart as single calls; equal to spmv_t + r2h_primal, spmv + r2h_dual). */
+PS26119_API int ps26119_backend_fused_primal(ps26119_backend* b, int y, int x, int x0, double tau, double w, double rho,
+                                 int xh, int xb);
+PS26119_API int ps26119_backend_fused_dual(ps26119_backend* b, int xb, int y, int y0, double sigma, double w, double rho,
+                               int yh, int yb);
+/* Backend::kkt (backend.h:65): out[8] = primal_residual, dual_residual, primal_obj, dual_obj,
+ * b_norm, c_norm, primal_max_rel, dual_max_rel (termination.h:35-60) */
+PS26119_API int ps26119_backend_kkt(ps26119_backend* b, int xs, int ys, double* out);
+PS26119_API int ps26119_backend_sync(ps26119_backend* b);
+/* Scaled problem introspection: which = 0 Ã values (CSR), 1 Ãᵀ values (CSR), 2 c̃, 3 l̃, 4 ũ,
+ * 5 r̃l, 6 r̃u, 7 row scale, 8 column scale (the ScaledProblem fields, scaling.h:48-67).
+ * Returns the element count (dst may be NULL to query it), or -1. */
+PS26119_API long long ps26119_backend_scaled_get(ps26119_backend* b, int which, double* dst);
+/* Structure of Ã (which = 0, m+1 row pointers) or Ãᵀ (which = 1, n+1); returns nnz. */
+PS26119_API long long ps26119_backend_scaled_structure(ps26119_backend* b, int which, int* row_ptr, int* col);
+/* out[4] = bound_scale, obj_scale, log10_range, geometric_mean_applied */
+PS26119_API int ps26119_backend_scalars(ps26119_backend* b, double* out);
+/* ‖Ã‖₂ estimate (la::estimate_norm2, reference src/la/csr.cpp:86-132) */
+PS26119_API int ps26119_backend_norm2_estimate(ps26119_backend* b, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PS26119_B200_BACKEND_H */

@@ -233,7 +233,7 @@ class Backend:
         return {"bound_scale": out[0], "obj_scale": out[1], "log10_range": out[2],
                 "geometric_mean_applied": bool(out[3])}
 
-    def norm2(self) -> float:
+    def norm2_estimate(self) -> float:
         return self.L.ref_norm2(self.h)
 
     def set_precision(self, mixed: bool):

@@ -1,0 +1,467 @@
+// c_api.cpp — the C ABI (include/ps26119.h, include/ps26119_backend.h). Exceptions never
+// cross this boundary (reference src/core/c_api.cpp:1-304 for the five reference symbols).
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <exception>
+#include <memory>
+#include <new>
+#include <string>
+
+#include <cuda_runtime.h>
+
+#include "../../include/ps26119.h"
+#include "../../include/ps26119_backend.h"
+#include "solver.hpp"
+
+using namespace b200;
+
+namespace {
+
+thread_local ps26119_stats g_stats{};
+thread_local std::string g_backend_error;
+
+void set_text(char* dst, std::size_t cap, const std::string& s) { std::snprintf(dst, cap, "%s", s.c_str()); }
+
+void clear(ps26119_result* r) {  // c_api.cpp:22-26
+  std::memset(r, 0, sizeof *r);
+  r->status = PS26119_NOT_SOLVED;
+  r->check = -1;
+}
+
+// C options -> Options (c_api.cpp:29-56). Returns an error text, or nullptr.
+const char* to_options(const ps26119_options* opt, int num_rows, int num_cols, Options& o) {
+  if (!opt) return nullptr;
+  switch (opt->algorithm) {
+    case PS26119_ALG_ORACLE: o.algorithm = Algorithm::Oracle; break;
+    case PS26119_ALG_PDLP: o.algorithm = Algorithm::Pdlp; break;
+    case PS26119_ALG_R2HPDHG: o.algorithm = Algorithm::R2hpdhg; break;
+    case PS26119_ALG_SIMPLEX: o.algorithm = Algorithm::Simplex; break;
+    case PS26119_ALG_AUTO: o.algorithm = Algorithm::Auto; break;
+    default: return "unknown algorithm";
+  }
+  if (opt->precision != PS26119_PREC_FP64 && opt->precision != PS26119_PREC_MIXED) return "unknown precision";
+  o.precision = opt->precision == PS26119_PREC_MIXED ? Precision::Mixed : Precision::Fp64;
+  o.use_gpu = opt->use_gpu != 0;
+  if (!(opt->tolerance >= 0) || !std::isfinite(opt->tolerance)) return "tolerance must be a finite number >= 0";
+  if (!(opt->time_limit >= 0)) return "time_limit must be >= 0 (0 = default)";
+  if (opt->iteration_limit < 0) return "iteration_limit must be >= 0 (0 = default)";
+  if (opt->threads < 0) return "threads must be >= 0 (0 = all cores)";
+  if (opt->tolerance > 0) o.tolerance = opt->tolerance;
+  if (opt->time_limit > 0) o.time_limit = opt->time_limit;
+  if (opt->iteration_limit > 0) o.iteration_limit = opt->iteration_limit;
+  o.verbosity = opt->verbosity;
+  o.threads = opt->threads;
+  if (opt->warm_x) o.warm_x.assign(opt->warm_x, opt->warm_x + num_cols);
+  if (opt->warm_y) o.warm_y.assign(opt->warm_y, opt->warm_y + num_rows);
+  return nullptr;
+}
+
+const char* apply_engine_options(const ps26119_engine_options* eo, Options& o) {
+  if (!eo) return nullptr;
+  if (eo->check_every < 0) return "check_every must be >= 0";
+  o.presolve = eo->presolve != 0;
+  if (eo->check_every > 0) o.check_every = eo->check_every;
+  o.exact = eo->exact_reductions != 0;
+  if (eo->ruiz_iterations >= 0) o.scaling.ruiz_iterations = eo->ruiz_iterations;
+  if (eo->pock_chambolle >= 0) o.scaling.pock_chambolle = eo->pock_chambolle != 0;
+  if (eo->bound_objective_rescaling >= 0) o.scaling.bound_objective_rescaling = eo->bound_objective_rescaling != 0;
+  if (eo->reflection != 0) o.reflection = eo->reflection;
+  if (!(eo->warm_primal_weight >= 0)) return "warm_primal_weight must be >= 0";
+  o.warm_primal_weight = eo->warm_primal_weight;
+  return nullptr;
+}
+
+void fill_stats(const Solution& s, long long m, long long n, long long nnz) {
+  const EngineResult& R = s.engine_result;
+  g_stats = ps26119_stats{};
+  g_stats.setup_seconds = R.setup_seconds;
+  g_stats.loop_seconds = R.loop_seconds;
+  g_stats.finish_seconds = R.finish_seconds;
+  g_stats.presolve_seconds = s.presolve_seconds;
+  g_stats.primal_weight = R.primal_weight;
+  g_stats.eta = R.eta;
+  g_stats.checks = R.checks;
+  g_stats.restarts = R.restarts;
+  g_stats.iterations_to_fast = R.iterations_to_fast;
+  g_stats.switch_iteration = R.switch_iteration;
+  g_stats.kernel_launches = R.kernel_launches;
+  g_stats.m = m, g_stats.n = n, g_stats.nnz = nnz;
+  g_stats.spmv_kernel_ms = R.iter_kernel_ms;
+  g_stats.spmv_kernel_launches = R.iter_kernel_launches;
+}
+
+void fill(const Solution& s, ps26119_result* result) {  // c_api.cpp:58-71
+  result->status = static_cast<int>(s.status);
+  result->objective = s.objective;
+  result->dual_objective = s.dual_objective;
+  result->primal_residual = s.primal_residual;
+  result->dual_residual = s.dual_residual;
+  result->gap = s.gap;
+  result->certified_bound = s.certified_bound;
+  result->iterations = s.iterations;
+  result->seconds = s.seconds;
+  result->check = s.check == "PASS" ? 1 : s.check == "FAIL" ? 0 : -1;
+  set_text(result->engine, sizeof result->engine, s.engine);
+  set_text(result->message, sizeof result->message, s.message);
+}
+
+int solve_host(int num_rows, int num_cols, int sense, double obj_offset, const double* c, const double* col_lower,
+               const double* col_upper, const double* row_lower, const double* row_upper, const int* col_start,
+               const int* row_index, const double* value, const ps26119_options* opt,
+               const ps26119_engine_options* eo, ps26119_result* result, double* x, double* y, double* z,
+               double* dual_ray, double* primal_ray) {
+  if (!result) return PS26119_INVALID_ARGUMENT;
+  clear(result);
+  auto invalid = [&](const char* why) {
+    result->status = PS26119_INVALID_ARGUMENT;
+    set_text(result->message, sizeof result->message, why);
+    return result->status;
+  };
+  if (num_rows < 0 || num_cols < 0) return invalid("negative dimension");
+  if (!col_start) return invalid("col_start is NULL");
+  if (num_cols > 0 && (!c || !col_lower || !col_upper)) return invalid("column data is NULL");
+  if (num_rows > 0 && (!row_lower || !row_upper)) return invalid("row bounds are NULL");
+  const int nnz = col_start[num_cols];
+  if (nnz < 0) return invalid("col_start[n] < 0");
+  if (nnz > 0 && (!row_index || !value)) return invalid("matrix arrays are NULL");
+  try {
+    Model m;
+    m.num_rows = num_rows;
+    m.num_cols = num_cols;
+    m.sense = sense;
+    m.obj_offset = obj_offset;
+    m.obj.assign(c, c + num_cols);
+    m.col_lower.assign(col_lower, col_lower + num_cols);
+    m.col_upper.assign(col_upper, col_upper + num_cols);
+    m.row_lower.assign(row_lower, row_lower + num_rows);
+    m.row_upper.assign(row_upper, row_upper + num_rows);
+    m.col_start.assign(col_start, col_start + num_cols + 1);
+    m.row_index.assign(row_index, row_index + nnz);
+    m.value.assign(value, value + nnz);
+    if (auto err = m.validate(); !err.empty()) return invalid(("invalid model: " + err).c_str());
+    Options o;
+    if (const char* bad = to_options(opt, num_rows, num_cols, o)) return invalid(bad);
+    if (const char* bad = apply_engine_options(eo, o)) return invalid(bad);
+    const Solution s = solve(m, o);
+    fill(s, result);
+    fill_stats(s, s.engine_result.iterations > 0 ? num_rows : 0, num_cols, nnz);
+    auto out = [](double* dst, const std::vector<double>& v, int len) {
+      if (dst && v.size() == static_cast<std::size_t>(len)) std::memcpy(dst, v.data(), sizeof(double) * len);
+    };
+    out(x, s.x, num_cols);
+    out(y, s.y, num_rows);
+    out(z, s.z, num_cols);
+    out(dual_ray, s.dual_ray, num_rows);
+    out(primal_ray, s.primal_ray, num_cols);
+    return result->status;
+  } catch (const std::bad_alloc&) {
+    result->status = PS26119_NOT_SOLVED;
+    set_text(result->message, sizeof result->message, "out of memory");
+    return result->status;
+  } catch (const std::exception& e) {
+    result->status = PS26119_NUMERICAL_ERROR;
+    set_text(result->message, sizeof result->message, e.what());
+    return result->status;
+  } catch (...) {
+    result->status = PS26119_NUMERICAL_ERROR;
+    set_text(result->message, sizeof result->message, "unknown error");
+    return result->status;
+  }
+}
+
+}  // namespace
+
+struct ps26119_backend {
+  std::unique_ptr<GpuBackend> impl;
+};
+
+extern "C" {
+
+const char* ps26119_version(void) { return "0.1.0+b200"; }
+
+void ps26119_default_options(ps26119_options* opt) {  // c_api.cpp:179-192
+  if (!opt) return;
+  opt->algorithm = PS26119_ALG_AUTO;
+  opt->precision = PS26119_PREC_FP64;
+  opt->use_gpu = 0;
+  opt->tolerance = 1e-8;
+  opt->time_limit = 3600.0;
+  opt->iteration_limit = 100000000LL;
+  opt->verbosity = 0;
+  opt->threads = 1;
+  opt->warm_x = nullptr;
+  opt->warm_y = nullptr;
+}
+
+void ps26119_default_engine_options(ps26119_engine_options* eo) {
+  if (!eo) return;
+  eo->presolve = 1;
+  eo->check_every = 64;
+  eo->exact_reductions = 0;
+  eo->ruiz_iterations = -1;
+  eo->pock_chambolle = -1;
+  eo->bound_objective_rescaling = -1;
+  eo->reflection = 0.0;
+  eo->warm_primal_weight = 0.0;
+}
+
+int ps26119_solve_lp(int num_rows, int num_cols, int sense, double obj_offset, const double* c,
+                     const double* col_lower, const double* col_upper, const double* row_lower,
+                     const double* row_upper, const int* col_start, const int* row_index, const double* value,
+                     const ps26119_options* opt, ps26119_result* result, double* x, double* y, double* z) {
+  return solve_host(num_rows, num_cols, sense, obj_offset, c, col_lower, col_upper, row_lower, row_upper, col_start,
+                    row_index, value, opt, nullptr, result, x, y, z, nullptr, nullptr);
+}
+
+int ps26119_solve_lp_ex(int num_rows, int num_cols, int sense, double obj_offset, const double* c,
+                        const double* col_lower, const double* col_upper, const double* row_lower,
+                        const double* row_upper, const int* col_start, const int* row_index, const double* value,
+                        const ps26119_options* opt, ps26119_result* result, double* x, double* y, double* z,
+                        double* dual_ray, double* primal_ray) {
+  return solve_host(num_rows, num_cols, sense, obj_offset, c, col_lower, col_upper, row_lower, row_upper, col_start,
+                    row_index, value, opt, nullptr, result, x, y, z, dual_ray, primal_ray);
+}
+
+int ps26119_solve_lp_engine(int num_rows, int num_cols, int sense, double obj_offset, const double* c,
+                            const double* col_lower, const double* col_upper, const double* row_lower,
+                            const double* row_upper, const int* col_start, const int* row_index,
+                            const double* value, const ps26119_options* opt, const ps26119_engine_options* eo,
+                            ps26119_result* result, double* x, double* y, double* z, double* dual_ray,
+                            double* primal_ray) {
+  return solve_host(num_rows, num_cols, sense, obj_offset, c, col_lower, col_upper, row_lower, row_upper, col_start,
+                    row_index, value, opt, eo, result, x, y, z, dual_ray, primal_ray);
+}
+
+int ps26119_solve_mps(const char* path, const ps26119_options* opt, ps26119_result* result,
+                      const char* solution_path) {
+  (void)opt;
+  (void)solution_path;
+  if (!result) return PS26119_INVALID_ARGUMENT;
+  clear(result);
+  result->status = PS26119_INVALID_ARGUMENT;
+  set_text(result->message, sizeof result->message,
+           path ? "read error: MPS input is not supported by this library yet (pass the model in CSC form)"
+                : "path is NULL");
+  return result->status;
+}
+
+int ps26119_solve_lp_device(int num_rows, int num_cols, int sense, double obj_offset, const double* d_c,
+                            const double* d_col_lower, const double* d_col_upper, const double* d_row_lower,
+                            const double* d_row_upper, const int* d_col_start, const int* d_row_index,
+                            const double* d_value, const ps26119_options* opt, const ps26119_engine_options* eo,
+                            ps26119_result* result, double* d_x, double* d_y, double* d_z, void* stream) {
+  if (!result) return PS26119_INVALID_ARGUMENT;
+  clear(result);
+  auto invalid = [&](const char* why) {
+    result->status = PS26119_INVALID_ARGUMENT;
+    set_text(result->message, sizeof result->message, why);
+    return result->status;
+  };
+  if (num_rows < 0 || num_cols < 0) return invalid("negative dimension");
+  if (sense != 1 && sense != -1) return invalid("sense must be +1 or -1");
+  if (!d_col_start) return invalid("col_start is NULL");
+  if (num_cols > 0 && (!d_c || !d_col_lower || !d_col_upper)) return invalid("column data is NULL");
+  if (num_rows > 0 && (!d_row_lower || !d_row_upper)) return invalid("row bounds are NULL");
+  try {
+    Options o;
+    if (const char* bad = to_options(opt, 0, 0, o)) return invalid(bad);
+    if (const char* bad = apply_engine_options(eo, o)) return invalid(bad);
+    if (opt && (opt->warm_x || opt->warm_y)) return invalid("warm start is not supported by the device entry point");
+    if (o.algorithm != Algorithm::Auto && o.algorithm != Algorithm::R2hpdhg)
+      return invalid("the device entry point runs r2hpdhg only");
+    require_device();
+    int nnz = 0;
+    if (cudaMemcpy(&nnz, d_col_start + num_cols, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+      return invalid("col_start is not a device pointer on the current device");
+    if (nnz < 0) return invalid("col_start[n] < 0");
+    if (nnz > 0 && (!d_row_index || !d_value)) return invalid("matrix arrays are NULL");
+    DeviceModel M;
+    M.m = num_rows, M.n = num_cols, M.sense = sense, M.offset = obj_offset, M.nnz = nnz;
+    M.c = d_c, M.col_lower = d_col_lower, M.col_upper = d_col_upper, M.row_lower = d_row_lower;
+    M.row_upper = d_row_upper, M.col_start = d_col_start, M.row_index = d_row_index, M.value = d_value;
+    EngineOptions e;
+    e.tolerance = o.tolerance;
+    e.time_limit = o.time_limit;
+    e.iteration_limit = o.iteration_limit;
+    e.check_every = o.check_every;
+    e.mixed = o.precision == Precision::Mixed;
+    e.exact = o.exact;
+    e.scaling = o.scaling;
+    e.reflection = o.reflection;
+    e.warm_primal_weight = o.warm_primal_weight;
+    e.verbosity = o.verbosity;
+    const EngineResult R = run_engine(M, e, DeviceOutputs{d_x, d_y, d_z, nullptr, nullptr}, stream);
+    Solution s;
+    s.status = R.status;
+    s.iterations = R.iterations;
+    s.objective = R.objective;
+    s.dual_objective = R.dual_objective;
+    s.primal_residual = R.primal_residual;
+    s.dual_residual = R.dual_residual;
+    s.gap = R.gap;
+    s.seconds = R.seconds;
+    s.message = R.message;
+    s.engine_result = R;
+    if (s.status == Status::Optimal) {  // gate on the device-computed check (solve.cpp:163-184)
+      s.check = R.check ? "PASS" : "FAIL";
+      if (!R.check && o.tolerance < 1e-6) {
+        s.status = Status::NumericalError;
+        s.message += std::string(s.message.empty() ? "" : "; ") + "Optimal withdrawn, in-process check failed";
+      }
+    }
+    fill(s, result);
+    fill_stats(s, num_rows, num_cols, nnz);
+    return result->status;
+  } catch (const std::bad_alloc&) {
+    result->status = PS26119_NOT_SOLVED;
+    set_text(result->message, sizeof result->message, "out of memory");
+    return result->status;
+  } catch (const std::exception& e) {
+    result->status = PS26119_NUMERICAL_ERROR;
+    set_text(result->message, sizeof result->message, e.what());
+    return result->status;
+  }
+}
+
+void ps26119_last_stats(ps26119_stats* out) {
+  if (out) *out = g_stats;
+}
+
+// ------------------------------------------------------------------ backend ABI
+const char* ps26119_backend_last_error(void) { return g_backend_error.c_str(); }
+
+#define B200_GUARD(body)                                  \
+  try {                                                   \
+    if (!b || !b->impl) {                                 \
+      g_backend_error = "null backend";                   \
+      return PS26119_INVALID_ARGUMENT;                    \
+    }                                                     \
+    body;                                                 \
+    return 0;                                             \
+  } catch (const std::bad_alloc&) {                       \
+    g_backend_error = "out of memory";                    \
+    return PS26119_NOT_SOLVED;                            \
+  } catch (const std::exception& e) {                     \
+    g_backend_error = e.what();                           \
+    return PS26119_NUMERICAL_ERROR;                       \
+  }
+
+int ps26119_backend_new(ps26119_backend** out, int num_rows, int num_cols, int sense, double obj_offset,
+                        const double* c, const double* col_lower, const double* col_upper, const double* row_lower,
+                        const double* row_upper, const int* col_start, const int* row_index, const double* value,
+                        const ps26119_scaling_options* so, int exact) {
+  if (!out) return PS26119_INVALID_ARGUMENT;
+  *out = nullptr;
+  try {
+    Model m;
+    m.num_rows = num_rows, m.num_cols = num_cols, m.sense = sense, m.obj_offset = obj_offset;
+    if (num_rows < 0 || num_cols < 0 || !col_start) {
+      g_backend_error = "invalid dimensions or NULL col_start";
+      return PS26119_INVALID_ARGUMENT;
+    }
+    const int nnz = col_start[num_cols];
+    m.obj.assign(c, c + num_cols);
+    m.col_lower.assign(col_lower, col_lower + num_cols);
+    m.col_upper.assign(col_upper, col_upper + num_cols);
+    m.row_lower.assign(row_lower, row_lower + num_rows);
+    m.row_upper.assign(row_upper, row_upper + num_rows);
+    m.col_start.assign(col_start, col_start + num_cols + 1);
+    m.row_index.assign(row_index, row_index + nnz);
+    m.value.assign(value, value + nnz);
+    if (auto err = m.validate(); !err.empty()) {
+      g_backend_error = "invalid model: " + err;
+      return PS26119_INVALID_ARGUMENT;
+    }
+    ScalingOptions sc;
+    if (so) {
+      sc.geometric_mean_iterations = so->geometric_mean_iterations;
+      sc.geometric_mean_min_log10_range = so->geometric_mean_min_log10_range;
+      sc.ruiz_iterations = so->ruiz_iterations;
+      sc.pock_chambolle = so->pock_chambolle != 0;
+      sc.bound_objective_rescaling = so->bound_objective_rescaling != 0;
+    }
+    auto* b = new ps26119_backend;
+    try {
+      b->impl = GpuBackend::create(m.view(), sc, exact != 0);
+    } catch (...) {
+      delete b;
+      throw;
+    }
+    *out = b;
+    return 0;
+  } catch (const std::bad_alloc&) {
+    g_backend_error = "out of memory";
+    return PS26119_NOT_SOLVED;
+  } catch (const std::exception& e) {
+    g_backend_error = std::string("CUDA backend unavailable: ") + e.what();
+    return PS26119_NOT_SOLVED;
+  }
+}
+
+void ps26119_backend_free(ps26119_backend* b) { delete b; }
+
+int ps26119_backend_set_precision(ps26119_backend* b, int mixed) { B200_GUARD(b->impl->set_precision(mixed != 0)) }
+int ps26119_backend_create(ps26119_backend* b, int dual) {
+  try {
+    if (!b || !b->impl) return -1;
+    return b->impl->create_vector(dual != 0);
+  } catch (const std::exception& e) {
+    g_backend_error = e.what();
+    return -1;
+  }
+}
+int ps26119_backend_upload(ps26119_backend* b, int v, const double* src) { B200_GUARD(b->impl->upload(v, src)) }
+int ps26119_backend_download(ps26119_backend* b, int v, double* dst) { B200_GUARD(b->impl->download(v, dst)) }
+int ps26119_backend_fill(ps26119_backend* b, int v, double a) { B200_GUARD(b->impl->fill(v, a)) }
+int ps26119_backend_copy(ps26119_backend* b, int dst, int src) { B200_GUARD(b->impl->copy(dst, src)) }
+int ps26119_backend_axpby(ps26119_backend* b, double a, int x, double bb, int y) { B200_GUARD(b->impl->axpby(a, x, bb, y)) }
+int ps26119_backend_spmv(ps26119_backend* b, int x, int out) { B200_GUARD(b->impl->spmv(x, out)) }
+int ps26119_backend_spmv_t(ps26119_backend* b, int y, int out) { B200_GUARD(b->impl->spmv_t(y, out)) }
+int ps26119_backend_dot(ps26119_backend* b, int x, int y, double* out) { B200_GUARD(*out = b->impl->dot(x, y)) }
+int ps26119_backend_norm2(ps26119_backend* b, int x, double* out) { B200_GUARD(*out = b->impl->norm2(x)) }
+int ps26119_backend_diff_norm2(ps26119_backend* b, int x, int y, double* out) { B200_GUARD(*out = b->impl->diff_norm2(x, y)) }
+int ps26119_backend_primal_step(ps26119_backend* b, int x, int aty, double tau, int xh) {
+  B200_GUARD(b->impl->primal_step(x, aty, tau, xh))
+}
+int ps26119_backend_dual_step(ps26119_backend* b, int y, int ax, double sigma, int yh) {
+  B200_GUARD(b->impl->dual_step(y, ax, sigma, yh))
+}
+int ps26119_backend_r2h_primal(ps26119_backend* b, int x, int x0, int aty, double tau, double w, double rho, int xh,
+                               int xb) {
+  B200_GUARD(b->impl->r2h_primal(x, x0, aty, tau, w, rho, xh, xb))
+}
+int ps26119_backend_r2h_dual(ps26119_backend* b, int y, int y0, int ax, double sigma, double w, double rho, int yh,
+                             int yb) {
+  B200_GUARD(b->impl->r2h_dual(y, y0, ax, sigma, w, rho, yh, yb))
+}
+int ps26119_backend_fused_primal(ps26119_backend* b, int y, int x, int x0, double tau, double w, double rho, int xh,
+                                 int xb) {
+  B200_GUARD(b->impl->fused_primal(y, x, x0, tau, w, rho, xh, xb))
+}
+int ps26119_backend_fused_dual(ps26119_backend* b, int xb, int y, int y0, double sigma, double w, double rho, int yh,
+                               int yb) {
+  B200_GUARD(b->impl->fused_dual(xb, y, y0, sigma, w, rho, yh, yb))
+}
+int ps26119_backend_kkt(ps26119_backend* b, int xs, int ys, double* out) { B200_GUARD(b->impl->kkt(xs, ys, out)) }
+int ps26119_backend_sync(ps26119_backend* b) { B200_GUARD(b->impl->sync()) }
+long long ps26119_backend_scaled_get(ps26119_backend* b, int which, double* dst) {
+  try {
+    return b && b->impl ? b->impl->scaled_get(which, dst) : -1;
+  } catch (const std::exception& e) {
+    g_backend_error = e.what();
+    return -1;
+  }
+}
+long long ps26119_backend_scaled_structure(ps26119_backend* b, int which, int* row_ptr, int* col) {
+  try {
+    return b && b->impl ? b->impl->scaled_structure(which, row_ptr, col) : -1;
+  } catch (const std::exception& e) {
+    g_backend_error = e.what();
+    return -1;
+  }
+}
+int ps26119_backend_scalars(ps26119_backend* b, double* out) { B200_GUARD(b->impl->scalars(out)) }
+int ps26119_backend_norm2_estimate(ps26119_backend* b, double* out) { B200_GUARD(*out = b->impl->norm2_estimate()) }
+
+}  // extern "C"

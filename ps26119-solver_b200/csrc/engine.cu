@@ -1,0 +1,842 @@
+// engine.cu — the r²HPDHG solve on the device (≙ pdhg::solve_r2hpdhg, reference
+// src/pdhg/r2hpdhg.cpp:11-162, with EngineContext src/pdhg/engine.cpp:195-307).
+//
+// Execution model:
+//   * One CUDA stream per solve. Setup (structure, scaling, ‖Ã‖₂) runs on the device.
+//   * An EPOCH = K iterations, captured once per precision as a CUDA graph: 2K fused kernels
+//     (Ãᵀy + primal update, Ãx̄ + dual update) plus the epoch-start residual section, which
+//     returns at once unless the epoch starts a Halpern cycle (inner = 0). The step scalars
+//     (τ, σ, the Halpern counter) live in device memory and are refreshed by one small copy
+//     before each replay, so the graph is never rebuilt.
+//   * A CHECK after each epoch is a second graph (three variants: without ray test, with it,
+//     with the drift test as well). It ends by copying one small status block to pinned host
+//     memory; the host then takes exactly the reference's decisions (termination, ray test,
+//     precision promotion, restart, PID primal weight) in fp64 with the same libm calls.
+//   * In exact mode every sum uses the reference's order, so the whole trajectory is
+//     bit-identical to the reference CPU engine; in fast mode only the reductions differ
+//     (fixed-order trees), by rounding.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <limits>
+#include <string>
+
+#include "checks.cuh"
+#include "engine.hpp"
+#include "problem.cuh"
+
+namespace b200 {
+
+const char* status_name(Status s) {
+  switch (s) {
+    case Status::Optimal: return "Optimal";
+    case Status::Infeasible: return "Infeasible";
+    case Status::Unbounded: return "Unbounded";
+    case Status::IterationLimit: return "IterationLimit";
+    case Status::TimeLimit: return "TimeLimit";
+    case Status::NumericalError: return "NumericalError";
+    default: return "NotSolved";
+  }
+}
+
+void require_device() {
+  int count = 0;
+  const cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    throw std::runtime_error(std::string("no CUDA device: ") + cudaGetErrorString(e));
+  }
+  if (count == 0) throw std::runtime_error("no CUDA device");
+}
+
+namespace {
+
+constexpr double kFirstOrderFast = 1e-4, kFirstOrderInfeasible = 1e-8, kMixedPrecisionSwitch = 1e-6;
+constexpr double kVerifyPrimal = 1e-6, kVerifyDual = 1e-6, kVerifyGap = 1e-6;
+
+// termination.h:35-60
+struct Kkt {
+  double primal_residual = 0, dual_residual = 0, primal_obj = 0, dual_obj = 0, b_norm = 0, c_norm = 0;
+  double primal_max_rel = 0, dual_max_rel = 0, obj_shift = 0;
+  double rel_primal() const { return primal_residual / (1.0 + b_norm); }
+  double rel_dual() const { return dual_residual / (1.0 + c_norm); }
+  double rel_gap() const {
+    return std::fabs(primal_obj - dual_obj) / (1.0 + std::fabs(primal_obj + obj_shift) + std::fabs(dual_obj + obj_shift));
+  }
+  double rel_kkt() const {
+    double mx = rel_primal();
+    if (mx < rel_dual()) mx = rel_dual();
+    if (mx < rel_gap()) mx = rel_gap();
+    return mx;
+  }
+  bool converged(double eps) const {
+    if (rel_kkt() > eps) return false;
+    if (eps >= kVerifyPrimal) return true;
+    return primal_max_rel <= kVerifyPrimal && dual_max_rel <= kVerifyDual && rel_gap() <= kVerifyGap;
+  }
+  bool finite() const {
+    return std::isfinite(primal_residual) && std::isfinite(dual_residual) && std::isfinite(primal_obj) &&
+           std::isfinite(dual_obj);
+  }
+};
+
+double slot_max(const double* h, int s) { return h[s]; }  // bit pattern of a non-negative double
+
+template <class T>
+struct IterVecs {
+  DevBuf<T> x, x0, xh, xb, dx, ddx, y, y0, yh, yb, dy, adx, ddy;
+  void alloc(int n, int m) {
+    for (DevBuf<T>* v : {&x, &x0, &xh, &xb, &dx, &ddx}) v->alloc(static_cast<std::size_t>(n));
+    for (DevBuf<T>* v : {&y, &y0, &yh, &yb, &dy, &adx, &ddy}) v->alloc(static_cast<std::size_t>(m));
+  }
+};
+
+template <class T>
+__global__ void k_diff(long long n, const T* a, const T* b, T* out) {  // out = a − b as axpby(−1, b, 1, out=a)
+  B200_FOR(i, n) out[i] = static_cast<T>(-1.0) * b[i] + static_cast<T>(1.0) * a[i];
+}
+
+class Engine {
+ public:
+  Engine(const DeviceModel& M, const EngineOptions& o, cudaStream_t st) : M_(M), o_(o), st_(st) {
+    for (auto& e : ev_) B200_CHECK(cudaEventCreate(&e));
+  }
+  ~Engine() {
+    for (auto& g : g_epoch_)
+      if (g) cudaGraphExecDestroy(g);
+    for (auto& row : g_check_)
+      for (auto& g : row)
+        if (g) cudaGraphExecDestroy(g);
+    for (auto& e : ev_)
+      if (e) cudaEventDestroy(e);
+  }
+
+  EngineResult run(const DeviceOutputs& out);
+
+ private:
+  using clock = std::chrono::steady_clock;
+  double elapsed() const { return std::chrono::duration<double>(clock::now() - t0_).count(); }
+
+  template <class T> IterVecs<T>& vecs();
+  template <class T> void capture_epoch();
+  template <class T> void capture_check(int variant);
+  template <class T> void launch_residual(bool with_restart_terms, const int* skip, SumPlan& plan);
+  template <class T> void launch_kkt_scaled(const T* xs, const T* ys);
+  void launch_kkt_original();
+  template <class T> void launch_ray(const T* dx, const T* dy, double* r, double* d, int drift);
+  Kkt read_kkt(const double* h) const;
+  void setup();
+  void build_plans();
+  template <class T> void init_iterates();
+  bool apply_warm_start();
+  template <class T> void restart();
+  void promote();
+  double initial_primal_weight();
+  void finish(EngineResult& R, Status st, bool use_hat, long long it, const std::string& msg,
+              const DeviceOutputs& out, int ray_test);
+  template <class T> void finish_t(EngineResult& R, Status st, bool use_hat, long long it, const std::string& msg,
+                                   const DeviceOutputs& out, int ray_test);
+  void sync_results() {
+    B200_CHECK(cudaMemcpyAsync(hres_.get(), res_.get(), kNumSlots * sizeof(double), cudaMemcpyDeviceToHost, st_));
+    B200_CHECK(cudaStreamSynchronize(st_));
+  }
+  void clear_maxima() { B200_CHECK(cudaMemsetAsync(res_.get() + 32, 0, 16 * sizeof(double), st_)); }
+
+  DeviceModel M_;
+  const EngineOptions& o_;
+  cudaStream_t st_;
+  clock::time_point t0_;
+  ScaledDevice sp_;
+  IterVecs<double> vd_;
+  IterVecs<float> vf_;
+  bool mixed_now_ = false;
+  double eta_ = 1.0;
+  DevBuf<StepParams> params_;
+  PinnedBuf<StepParams> hparams_;
+  DevBuf<double> res_;
+  PinnedBuf<double> hres_;
+  DevBuf<double> rt_, kt_, rayt_, xo_, yo_, r1_, d1_, r2_, d2_, objt_;
+  SumPlan plan_r0_, plan_res_, plan_kkt_, plan_ray1_, plan_ray2_, plan_obj_, plan_chk_;
+  cudaGraphExec_t g_epoch_[2] = {nullptr, nullptr};
+  cudaGraphExec_t g_check_[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
+  long long epoch_kernels_[2] = {0, 0}, check_kernels_[2][3] = {{0, 0, 0}, {0, 0, 0}};
+  cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};
+  long long kernels_ = 0;  // counted launches (graph kernel nodes per replay)
+  long long capture_count_ = 0;
+  bool capturing_ = false;
+  double iter_ms_ = 0;
+  long long iter_launches_ = 0;
+  long long fast_it_ = -1, switch_it_ = -1;
+  double primal_weight_ = std::numeric_limits<double>::quiet_NaN();
+  // precision policy (engine.cpp:56-79)
+  double pol_best_ = 1e300;
+  int pol_since_best_ = 0;
+};
+
+template <> IterVecs<double>& Engine::vecs<double>() { return vd_; }
+template <> IterVecs<float>& Engine::vecs<float>() { return vf_; }
+
+#define B200_COUNT(k) (capturing_ ? capture_count_ += (k) : kernels_ += (k))
+
+void Engine::setup() {
+  sp_.build(M_, o_.scaling, o_.exact, st_);
+  if (o_.mixed) sp_.make_f32(st_);
+  const double norm = sp_.lanczos(st_);
+  eta_ = norm > 0 ? 0.998 / norm : 1.0;  // engine.cpp:203-204
+  kernels_ += sp_.kernels;
+  const int m = M_.m, n = M_.n;
+  vd_.alloc(n, m);
+  if (o_.mixed) vf_.alloc(n, m);
+  params_.alloc(1);
+  hparams_.alloc(1);
+  res_.alloc(kNumSlots);
+  hres_.alloc(kNumSlots);
+  B200_CHECK(cudaMemsetAsync(res_.get(), 0, kNumSlots * sizeof(double), st_));
+  const std::size_t mm = static_cast<std::size_t>(m), nn = static_cast<std::size_t>(n);
+  rt_.alloc(2 * nn + 3 * mm);
+  kt_.alloc(4 * (mm + nn));
+  rayt_.alloc(2 * (mm + nn) + 2 * nn);
+  xo_.alloc(nn), yo_.alloc(mm), r1_.alloc(mm), d1_.alloc(nn), r2_.alloc(mm), d2_.alloc(nn);
+  objt_.alloc(mm + 2 * nn);
+  build_plans();
+}
+
+void Engine::build_plans() {
+  const long long m = M_.m, n = M_.n;
+  double* R = res_.get();
+  double* px = rt_.get();
+  double* dxn = px + n;
+  double* py = dxn + n;
+  double* cross = py + m;
+  double* dyn = cross + m;
+  // fixed-point residual dots: la::parallel_sum order (64 chunks)
+  plan_r0_.add(px, 0, n, 0.0, SumOrder::kChunk64, R + kPx0);
+  plan_r0_.add(py, 0, m, 0.0, SumOrder::kChunk64, R + kPy0);
+  plan_r0_.add(cross, 0, m, 0.0, SumOrder::kChunk64, R + kCross0);
+  plan_res_.add(px, 0, n, 0.0, SumOrder::kChunk64, R + kPx);
+  plan_res_.add(py, 0, m, 0.0, SumOrder::kChunk64, R + kPy);
+  plan_res_.add(cross, 0, m, 0.0, SumOrder::kChunk64, R + kCross);
+  plan_res_.add(dxn, 0, n, 0.0, SumOrder::kChunk64, R + kDxn2);
+  plan_res_.add(dyn, 0, m, 0.0, SumOrder::kChunk64, R + kDyn2);
+  // KKT: host loops of kkt_general (rows, then columns for the continuing sums)
+  double* K0 = kt_.get();
+  const long long L = m + n;
+  plan_kkt_.add(K0, 0, m, 0.0, SumOrder::kSeq, R + kRp2);
+  plan_kkt_.add(K0 + L, 0, L, 0.0, SumOrder::kSeq, R + kD);
+  plan_kkt_.add(K0 + 2 * L, 0, L, 0.0, SumOrder::kSeq, R + kRd2);
+  plan_kkt_.add(K0 + 3 * L, m, L, 0.0, SumOrder::kSeq, R + kP);
+  double* T0 = rayt_.get();
+  plan_ray1_.add(T0, 0, L, 0.0, SumOrder::kSeq, R + kRayObj);
+  plan_ray1_.add(T0 + L, 0, L, 0.0, SumOrder::kSeq, R + kRayMag);
+  plan_ray1_.add(T0 + 2 * L, 0, n, 0.0, SumOrder::kSeq, R + kRayCd);
+  plan_ray1_.add(T0 + 2 * L + n, 0, n, 0.0, SumOrder::kSeq, R + kRayCmag);
+  plan_ray2_.add(T0, 0, L, 0.0, SumOrder::kSeq, R + kRayObj2);
+  plan_ray2_.add(T0 + L, 0, L, 0.0, SumOrder::kSeq, R + kRayMag2);
+  plan_ray2_.add(T0 + 2 * L, 0, n, 0.0, SumOrder::kSeq, R + kRayCd2);
+  plan_ray2_.add(T0 + 2 * L + n, 0, n, 0.0, SumOrder::kSeq, R + kRayCmag2);
+  // finish: objective = offset + Σ c x (Model::objective_value), check sums (solution_checker)
+  double* O = objt_.get();
+  plan_obj_.add(O, 0, n, M_.offset, SumOrder::kSeq, R + kObjective);
+  plan_chk_.add(O + n, 0, L, 0.0, SumOrder::kSeq, R + kChkDual);
+  plan_chk_.add(O, 0, n, 0.0, SumOrder::kSeq, R + kChkPrimal);
+  plan_r0_.build(o_.exact, skip_r0_flag(params_.get()));
+  plan_res_.build(o_.exact, nullptr);
+  plan_kkt_.build(o_.exact, nullptr);
+  plan_ray1_.build(o_.exact, nullptr);
+  plan_ray2_.build(o_.exact, nullptr);
+  plan_obj_.build(o_.exact, nullptr);
+  plan_chk_.build(o_.exact, nullptr);
+}
+
+// The residual: dx = x̄ − x̂, adx = Ã dx, dy = ȳ − ŷ and the terms of the five dots.
+template <class T>
+void Engine::launch_residual(bool with_restart_terms, const int* skip, SumPlan& plan) {
+  IterVecs<T>& v = vecs<T>();
+  const int m = M_.m, n = M_.n;
+  double* px = rt_.get();
+  double* dxn = px + n;
+  double* py = dxn + n;
+  double* cross = py + m;
+  double* dyn = cross + m;
+  k_res_x<T><<<grid_for(n), kBlock, 0, st_>>>(n, v.xb.get(), v.xh.get(), v.x0.get(), v.dx.get(), px,
+                                              with_restart_terms ? dxn : nullptr, skip);
+  B200_LAUNCH_CHECK();
+  EpiResY<T> e{v.yb.get(), v.yh.get(), v.y0.get(), v.dy.get(), v.adx.get(), py, cross,
+               with_restart_terms ? dyn : nullptr, skip};
+  launch_slab<T>(m, sp_.a_rp.get(), sp_.a_col.get(), sp_.A_val<T>(), v.dx.get(), e, st_);
+  plan.launch(st_);
+  B200_COUNT(2 + plan.kernel_count());
+}
+
+void Engine::launch_kkt_original() {
+  const int m = M_.m, n = M_.n;
+  const long long L = static_cast<long long>(m) + n;
+  double* K0 = kt_.get();
+  EpiKktRows er{{}, yo_.get(), M_.row_lower, M_.row_upper, K0, K0 + L, K0 + 2 * L, res_.get()};
+  launch_slab<double>(m, sp_.a_rp.get(), sp_.a_col.get(), sp_.a_v0.get(), xo_.get(), er, st_);
+  EpiKktCols ec{{}, xo_.get(), M_.c, M_.col_lower, M_.col_upper, static_cast<double>(M_.sense), m,
+                K0 + 3 * L, K0 + L, K0 + 2 * L, res_.get()};
+  launch_slab<double>(n, M_.col_start, M_.row_index, M_.value, yo_.get(), ec, st_);
+  plan_kkt_.launch(st_);
+  B200_COUNT(2 + plan_kkt_.kernel_count());
+}
+
+template <class T>
+void Engine::launch_kkt_scaled(const T* xs, const T* ys) {
+  const int m = M_.m, n = M_.n;
+  k_unscale_x<T><<<grid_for(n), kBlock, 0, st_>>>(n, xs, sp_.col_scale.get(), sp_.bound_scale, M_.col_lower,
+                                                  M_.col_upper, xo_.get());
+  k_unscale_y<T><<<grid_for(m), kBlock, 0, st_>>>(m, ys, sp_.row_scale.get(), sp_.obj_scale, yo_.get());
+  B200_LAUNCH_CHECK();
+  B200_COUNT(2);
+  launch_kkt_original();
+}
+
+template <class T>
+void Engine::launch_ray(const T* dx, const T* dy, double* r, double* d, int drift) {
+  const int m = M_.m, n = M_.n;
+  const long long L = static_cast<long long>(m) + n;
+  double* T0 = rayt_.get();
+  const int s_rmax = drift ? kMaxRmax2 : kMaxRmax, s_dabs = drift ? kMaxDabs2 : kMaxDabs;
+  const int s_dviol = drift ? kMaxDviol2 : kMaxDviol, s_pviol = drift ? kMaxPviol2 : kMaxPviol;
+  k_ray_r<T><<<grid_for(m), kBlock, 0, st_>>>(m, dy, sp_.row_scale.get(), sp_.obj_scale, M_.row_lower,
+                                              M_.row_upper, r, res_.get(), s_rmax);
+  k_ray_d<T><<<grid_for(n), kBlock, 0, st_>>>(n, dx, sp_.col_scale.get(), sp_.bound_scale, M_.col_lower,
+                                              M_.col_upper, d, res_.get(), s_dabs);
+  k_ray_cols<<<grid_for(n), kBlock, 0, st_>>>(n, m, M_.col_start, M_.row_index, M_.value, r, d, M_.c,
+                                              static_cast<double>(M_.sense), M_.col_lower, M_.col_upper, T0,
+                                              T0 + L, T0 + 2 * L, T0 + 2 * L + n, res_.get(), s_dviol);
+  B200_LAUNCH_CHECK();
+  EpiRayRows er{{}, r, M_.row_lower, M_.row_upper, T0, T0 + L, res_.get(), s_pviol};
+  launch_slab<double>(m, sp_.a_rp.get(), sp_.a_col.get(), sp_.a_v0.get(), d, er, st_);
+  SumPlan& p = drift ? plan_ray2_ : plan_ray1_;
+  p.launch(st_);
+  B200_COUNT(4 + p.kernel_count());
+}
+
+template <class T>
+void Engine::capture_epoch() {
+  const int idx = std::is_same<T, float>::value ? 1 : 0;
+  if (g_epoch_[idx]) return;
+  IterVecs<T>& v = vecs<T>();
+  const int m = M_.m, n = M_.n, K = o_.check_every;
+  const StepParams* P = params_.get();
+  const int* r0_skip = skip_r0_flag(P);
+  cudaGraph_t g;
+  capturing_ = true;
+  capture_count_ = 0;
+  B200_CHECK(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
+  auto step = [&](int s) {
+    EpiPrimal<T> ep{v.x.get(), v.xh.get(), v.xb.get(), v.x0.get(), sp_.c<T>(), sp_.l<T>(), sp_.u<T>(), P, s, 0, 0, 0};
+    launch_slab<T>(n, M_.col_start, sp_.t_ri.get(), sp_.At_val<T>(), v.y.get(), ep, st_);
+    EpiDual<T> ed{v.y.get(), v.yh.get(), v.yb.get(), v.y0.get(), sp_.rl<T>(), sp_.ru<T>(), P, s, 0, 0, 0, 0};
+    launch_slab<T>(m, sp_.a_rp.get(), sp_.a_col.get(), sp_.A_val<T>(), v.xb.get(), ed, st_);
+    capture_count_ += 2;
+  };
+  B200_CHECK(cudaEventRecordWithFlags(ev_[0], st_, cudaEventRecordExternal));
+  step(0);
+  B200_CHECK(cudaEventRecordWithFlags(ev_[1], st_, cudaEventRecordExternal));
+  launch_residual<T>(false, r0_skip, plan_r0_);  // r⁰ after the first step of a Halpern cycle
+  B200_CHECK(cudaEventRecordWithFlags(ev_[2], st_, cudaEventRecordExternal));
+  for (int s = 1; s < K; ++s) step(s);
+  B200_CHECK(cudaEventRecordWithFlags(ev_[3], st_, cudaEventRecordExternal));
+  const cudaError_t e = cudaStreamEndCapture(st_, &g);
+  capturing_ = false;
+  B200_CHECK(e);
+  B200_CHECK(cudaGraphInstantiate(&g_epoch_[idx], g, 0));
+  cudaGraphDestroy(g);
+  epoch_kernels_[idx] = capture_count_;
+}
+
+template <class T>
+void Engine::capture_check(int variant) {
+  const int idx = std::is_same<T, float>::value ? 1 : 0;
+  if (g_check_[idx][variant]) return;
+  IterVecs<T>& v = vecs<T>();
+  cudaGraph_t g;
+  capturing_ = true;
+  capture_count_ = 0;
+  B200_CHECK(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
+  clear_maxima();
+  launch_residual<T>(true, nullptr, plan_res_);
+  launch_kkt_scaled<T>(v.xh.get(), v.yh.get());
+  if (variant >= 1) launch_ray<T>(v.dx.get(), v.dy.get(), r1_.get(), d1_.get(), 0);
+  if (variant == 2) {
+    k_diff<T><<<grid_for(M_.n), kBlock, 0, st_>>>(M_.n, v.xh.get(), v.x0.get(), v.ddx.get());
+    k_diff<T><<<grid_for(M_.m), kBlock, 0, st_>>>(M_.m, v.yh.get(), v.y0.get(), v.ddy.get());
+    B200_LAUNCH_CHECK();
+    capture_count_ += 2;
+    launch_ray<T>(v.ddx.get(), v.ddy.get(), r2_.get(), d2_.get(), 1);
+  }
+  B200_CHECK(cudaMemcpyAsync(hres_.get(), res_.get(), kNumSlots * sizeof(double), cudaMemcpyDeviceToHost, st_));
+  const cudaError_t e = cudaStreamEndCapture(st_, &g);
+  capturing_ = false;
+  B200_CHECK(e);
+  B200_CHECK(cudaGraphInstantiate(&g_check_[idx][variant], g, 0));
+  cudaGraphDestroy(g);
+  check_kernels_[idx][variant] = capture_count_;
+}
+
+Kkt Engine::read_kkt(const double* h) const {
+  Kkt k;
+  k.primal_residual = std::sqrt(h[kRp2]);
+  k.dual_residual = std::sqrt(h[kRd2]);
+  k.primal_obj = h[kP];
+  k.dual_obj = h[kD];
+  k.b_norm = sp_.b_norm;
+  k.c_norm = sp_.c_norm;
+  k.primal_max_rel = slot_max(h, kMaxPmax);
+  k.dual_max_rel = slot_max(h, kMaxDmax) / (1.0 + sp_.c_inf);
+  // EngineContext::adjust (engine.h:121-126)
+  if (o_.kkt_b_norm >= 0) k.b_norm = o_.kkt_b_norm;
+  if (o_.kkt_c_norm >= 0) k.c_norm = o_.kkt_c_norm;
+  k.obj_shift = o_.kkt_obj_shift;
+  return k;
+}
+
+template <class T>
+void Engine::init_iterates() {
+  IterVecs<T>& v = vecs<T>();
+  const int m = M_.m, n = M_.n;
+  k_init_x<T><<<grid_for(n), kBlock, 0, st_>>>(n, sp_.c<T>(), sp_.l<T>(), sp_.u<T>(), v.x.get());
+  k_fill<T><<<grid_for(m), kBlock, 0, st_>>>(m, v.y.get(), static_cast<T>(0.0));
+  B200_LAUNCH_CHECK();
+  kernels_ += 2;
+}
+
+template <class T>
+void Engine::restart() {
+  IterVecs<T>& v = vecs<T>();
+  const int m = M_.m, n = M_.n;
+  k_restart<T><<<grid_for(std::max(m, n)), kBlock, 0, st_>>>(n, m, v.xh.get(), v.x.get(), v.x0.get(), v.yh.get(),
+                                                               v.y.get(), v.y0.get());
+  B200_LAUNCH_CHECK();
+  ++kernels_;
+}
+
+// set_precision(Fp64): every iterate converted float -> double (cuda_backend.cu:474-483)
+void Engine::promote() {
+  const long long m = M_.m, n = M_.n;
+  DevBuf<float>* fs[] = {&vf_.x, &vf_.x0, &vf_.xh, &vf_.xb, &vf_.y, &vf_.y0, &vf_.yh, &vf_.yb};
+  DevBuf<double>* ds[] = {&vd_.x, &vd_.x0, &vd_.xh, &vd_.xb, &vd_.y, &vd_.y0, &vd_.yh, &vd_.yb};
+  for (int q = 0; q < 8; ++q) {
+    const long long len = q < 4 ? n : m;
+    k_convert<double, float><<<grid_for(len), kBlock, 0, st_>>>(len, fs[q]->get(), ds[q]->get());
+  }
+  B200_LAUNCH_CHECK();
+  kernels_ += 8;
+  mixed_now_ = false;
+}
+
+double Engine::initial_primal_weight() {  // engine.cpp:207-218
+  if (o_.warm_primal_weight > 0) return o_.warm_primal_weight;
+  if (o_.scaling.bound_objective_rescaling) return 1.0;
+  const int m = M_.m, n = M_.n;
+  DevBuf<double> tm(m), tn(n), s(2);
+  k_b2_terms<<<grid_for(m), kBlock, 0, st_>>>(m, sp_.srl.get(), sp_.sru.get(), tm.get());
+  k_sq_terms<<<grid_for(n), kBlock, 0, st_>>>(n, sp_.sc.get(), tn.get());
+  B200_LAUNCH_CHECK();
+  SumPlan p;
+  p.add(tm.get(), 0, m, 0.0, SumOrder::kSeq, s.get());
+  p.add(tn.get(), 0, n, 0.0, SumOrder::kSeq, s.get() + 1);
+  p.build(o_.exact, nullptr);
+  p.launch(st_);
+  double h[2];
+  B200_CHECK(cudaMemcpyAsync(h, s.get(), sizeof h, cudaMemcpyDeviceToHost, st_));
+  B200_CHECK(cudaStreamSynchronize(st_));
+  return (std::sqrt(h[1]) + 1.0) / (std::sqrt(h[0]) + 1.0);
+}
+
+// EngineContext::apply_warm_start (engine.cpp:237-266). Returns true if applied.
+bool Engine::apply_warm_start() {
+  if (o_.warm_x.empty() && o_.warm_y.empty()) return false;
+  const int m = M_.m, n = M_.n;
+  std::vector<double> lo(n), up(n), rl(m), ru(m), cs(n), rs(m);
+  B200_CHECK(cudaMemcpyAsync(lo.data(), M_.col_lower, n * sizeof(double), cudaMemcpyDeviceToHost, st_));
+  B200_CHECK(cudaMemcpyAsync(up.data(), M_.col_upper, n * sizeof(double), cudaMemcpyDeviceToHost, st_));
+  B200_CHECK(cudaMemcpyAsync(rl.data(), M_.row_lower, m * sizeof(double), cudaMemcpyDeviceToHost, st_));
+  B200_CHECK(cudaMemcpyAsync(ru.data(), M_.row_upper, m * sizeof(double), cudaMemcpyDeviceToHost, st_));
+  B200_CHECK(cudaMemcpyAsync(cs.data(), sp_.col_scale.get(), n * sizeof(double), cudaMemcpyDeviceToHost, st_));
+  B200_CHECK(cudaMemcpyAsync(rs.data(), sp_.row_scale.get(), m * sizeof(double), cudaMemcpyDeviceToHost, st_));
+  std::vector<double> xo(n), yo(m, 0.0);
+  if (!o_.warm_x.empty()) {
+    B200_CHECK(cudaStreamSynchronize(st_));
+    for (int j = 0; j < n; ++j) xo[j] = std_min(std_max(o_.warm_x[j], lo[j]), up[j]);
+  } else {  // the engine's cold x, unscaled
+    std::vector<double> xs(n);
+    if (mixed_now_) {
+      std::vector<float> xf(n);
+      B200_CHECK(cudaMemcpyAsync(xf.data(), vf_.x.get(), n * sizeof(float), cudaMemcpyDeviceToHost, st_));
+      B200_CHECK(cudaStreamSynchronize(st_));
+      for (int j = 0; j < n; ++j) xs[j] = xf[j];
+    } else {
+      B200_CHECK(cudaMemcpyAsync(xs.data(), vd_.x.get(), n * sizeof(double), cudaMemcpyDeviceToHost, st_));
+      B200_CHECK(cudaStreamSynchronize(st_));
+    }
+    for (int j = 0; j < n; ++j) xo[j] = std_min(std_max(cs[j] * xs[j] / sp_.bound_scale, lo[j]), up[j]);
+  }
+  if (!o_.warm_y.empty()) {
+    for (int i = 0; i < m; ++i) {
+      double v = static_cast<double>(M_.sense) * o_.warm_y[i];
+      if (!std::isfinite(rl[i])) v = std_min(v, 0.0);
+      if (!std::isfinite(ru[i])) v = std_max(v, 0.0);
+      yo[i] = v;
+    }
+  }
+  // decide the working precision before uploading (PrecisionPolicy::on_warm_start)
+  B200_CHECK(cudaMemcpyAsync(xo_.get(), xo.data(), n * sizeof(double), cudaMemcpyHostToDevice, st_));
+  B200_CHECK(cudaMemcpyAsync(yo_.get(), yo.data(), m * sizeof(double), cudaMemcpyHostToDevice, st_));
+  clear_maxima();
+  launch_kkt_original();
+  sync_results();
+  const double wr = read_kkt(hres_.get()).rel_kkt();
+  if (o_.mixed && mixed_now_ && wr <= kMixedPrecisionSwitch && o_.tolerance < kMixedPrecisionSwitch) {
+    mixed_now_ = false;
+    switch_it_ = 0;
+  }
+  std::vector<double> xs(n), ys(m);
+  for (int j = 0; j < n; ++j) xs[j] = sp_.bound_scale * xo[j] / cs[j];
+  for (int i = 0; i < m; ++i) ys[i] = sp_.obj_scale * yo[i] / rs[i];
+  if (mixed_now_) {
+    std::vector<float> xf(xs.begin(), xs.end()), yf(ys.begin(), ys.end());
+    B200_CHECK(cudaMemcpyAsync(vf_.x.get(), xf.data(), n * sizeof(float), cudaMemcpyHostToDevice, st_));
+    B200_CHECK(cudaMemcpyAsync(vf_.y.get(), yf.data(), m * sizeof(float), cudaMemcpyHostToDevice, st_));
+    B200_CHECK(cudaStreamSynchronize(st_));
+  } else {
+    B200_CHECK(cudaMemcpyAsync(vd_.x.get(), xs.data(), n * sizeof(double), cudaMemcpyHostToDevice, st_));
+    B200_CHECK(cudaMemcpyAsync(vd_.y.get(), ys.data(), m * sizeof(double), cudaMemcpyHostToDevice, st_));
+    B200_CHECK(cudaStreamSynchronize(st_));
+  }
+  return true;
+}
+
+void Engine::finish(EngineResult& R, Status st, bool use_hat, long long it, const std::string& msg,
+                    const DeviceOutputs& out, int ray_test) {
+  if (mixed_now_) finish_t<float>(R, st, use_hat, it, msg, out, ray_test);
+  else finish_t<double>(R, st, use_hat, it, msg, out, ray_test);
+}
+
+// EngineContext::finish (engine.cpp:268-307) plus the device-side in-process check.
+template <class T>
+void Engine::finish_t(EngineResult& R, Status status, bool use_hat, long long it, const std::string& msg,
+                      const DeviceOutputs& out, int ray_test) {
+  const auto tf = clock::now();
+  IterVecs<T>& v = vecs<T>();
+  const int m = M_.m, n = M_.n;
+  clear_maxima();
+  launch_kkt_scaled<T>(use_hat ? v.xh.get() : v.x.get(), use_hat ? v.yh.get() : v.y.get());
+  // objective = offset + Σ c_j x_j (Model::objective_value)
+  k_obj_terms<<<grid_for(n), kBlock, 0, st_>>>(n, M_.c, xo_.get(), objt_.get());
+  B200_LAUNCH_CHECK();
+  plan_obj_.launch(st_);
+  // in-process check (solution_checker.cpp:61-133) on xo and y_min = yo
+  double c_scale = std_max(1.0, sp_.c_inf);
+  EpiCheckRows cr{{}, yo_.get(), M_.row_lower, M_.row_upper, c_scale, objt_.get() + n, res_.get()};
+  launch_slab<double>(m, sp_.a_rp.get(), sp_.a_col.get(), sp_.a_v0.get(), xo_.get(), cr, st_);
+  // t_primal lands in objt_[0, n): the objective terms were consumed by plan_obj_ above
+  EpiCheckCols cc{{}, xo_.get(), M_.c, M_.col_lower, M_.col_upper, static_cast<double>(M_.sense), c_scale, m,
+                  objt_.get() + n, objt_.get(), res_.get()};
+  launch_slab<double>(n, M_.col_start, M_.row_index, M_.value, yo_.get(), cc, st_);
+  plan_chk_.launch(st_);
+  kernels_ += 3 + plan_obj_.kernel_count() + plan_chk_.kernel_count();
+  // outputs
+  if (out.x) B200_CHECK(cudaMemcpyAsync(out.x, xo_.get(), n * sizeof(double), cudaMemcpyDeviceToDevice, st_));
+  if (out.y || out.z) {
+    DevBuf<double> ytmp;
+    double* y = out.y;
+    if (!y) {
+      ytmp.alloc(m);
+      y = ytmp.get();
+    }
+    k_dual_out<<<grid_for(m), kBlock, 0, st_>>>(m, static_cast<double>(M_.sense), yo_.get(), y);
+    if (out.z) k_reduced_costs<<<grid_for(n), kBlock, 0, st_>>>(n, M_.col_start, M_.row_index, M_.value, M_.c, y, out.z);
+    B200_LAUNCH_CHECK();
+    kernels_ += 2;
+    if (ytmp.get()) B200_CHECK(cudaStreamSynchronize(st_));
+  }
+  if (status == Status::Infeasible && out.dual_ray)
+    B200_CHECK(cudaMemcpyAsync(out.dual_ray, ray_test == 2 ? r2_.get() : r1_.get(), m * sizeof(double),
+                               cudaMemcpyDeviceToDevice, st_));
+  if (status == Status::Unbounded && out.primal_ray)
+    B200_CHECK(cudaMemcpyAsync(out.primal_ray, ray_test == 2 ? d2_.get() : d1_.get(), n * sizeof(double),
+                               cudaMemcpyDeviceToDevice, st_));
+  sync_results();
+  const double* h = hres_.get();
+  const Kkt k = read_kkt(h);
+  if (!k.finite()) status = Status::NumericalError;
+  if (status == Status::Optimal && !k.converged(o_.tolerance)) status = Status::NumericalError;  // never over-claim
+  const double sense = M_.sense;
+  R.status = status;
+  R.iterations = it;
+  R.message = msg;
+  R.objective = h[kObjective];
+  R.dual_objective = sense * k.dual_obj + M_.offset;
+  R.primal_residual = k.rel_primal();
+  R.dual_residual = k.rel_dual();
+  R.gap = k.rel_gap();
+  R.iterations_to_fast = fast_it_;
+  R.switch_iteration = switch_it_;
+  R.primal_weight = primal_weight_;
+  R.eta = eta_;
+  R.have_dual_ray = status == Status::Infeasible;
+  R.have_primal_ray = status == Status::Unbounded;
+  if (status == Status::Infeasible || status == Status::Unbounded)
+    R.objective = R.dual_objective = std::numeric_limits<double>::quiet_NaN();
+  // check report (solution_checker.cpp:111-131)
+  const double pobj = sense * h[kChkPrimal] + M_.offset, dobj = sense * h[kChkDual] + M_.offset;
+  R.check_primal = slot_max(h, kMaxChkPrimal);
+  R.check_dual = slot_max(h, kMaxChkDual);
+  R.check_gap = std::fabs(pobj - dobj) / (1.0 + std::fabs(pobj) + std::fabs(dobj));
+  const bool finite_pt = std::isfinite(pobj) && std::isfinite(dobj) && std::isfinite(R.check_primal);
+  R.check = finite_pt && R.check_primal <= kVerifyPrimal && R.check_dual <= kVerifyDual && R.check_gap <= kVerifyGap;
+  R.finish_seconds = std::chrono::duration<double>(clock::now() - tf).count();
+}
+
+EngineResult Engine::run(const DeviceOutputs& out) {
+  t0_ = clock::now();
+  EngineResult R;
+  setup();
+  mixed_now_ = o_.mixed;
+  const double rho = o_.reflection;
+  double omega = initial_primal_weight();
+  if (mixed_now_) init_iterates<float>();
+  else init_iterates<double>();
+  const bool warm = apply_warm_start();
+  primal_weight_ = omega;
+  std::string msg = warm ? "warm start" : "";
+  const int K = o_.check_every;
+  R.setup_seconds = elapsed();
+  auto done = [&](Status s, bool hat, long long it, const std::string& m, int ray) {
+    R.loop_seconds = elapsed() - R.setup_seconds;
+    finish(R, s, hat, it, m, out, ray);
+    R.kernel_launches = kernels_;
+    R.iter_kernel_ms = iter_ms_;
+    R.iter_kernel_launches = iter_launches_;
+    R.seconds = elapsed();
+    return R;
+  };
+  if (warm) {  // the warm point may already be good enough (r2hpdhg.cpp:37-40)
+    clear_maxima();
+    if (mixed_now_) launch_kkt_scaled<float>(vf_.x.get(), vf_.y.get());
+    else launch_kkt_scaled<double>(vd_.x.get(), vd_.y.get());
+    sync_results();
+    const Kkt kw = read_kkt(hres_.get());
+    if (fast_it_ < 0 && kw.rel_kkt() <= kFirstOrderFast) fast_it_ = 0;
+    if (kw.finite() && kw.converged(o_.tolerance)) return done(Status::Optimal, false, 0, "warm start already optimal", 0);
+  }
+  {
+    const long long m = M_.m, n = M_.n;
+    if (mixed_now_) {
+      B200_CHECK(cudaMemcpyAsync(vf_.x0.get(), vf_.x.get(), n * sizeof(float), cudaMemcpyDeviceToDevice, st_));
+      B200_CHECK(cudaMemcpyAsync(vf_.xh.get(), vf_.x.get(), n * sizeof(float), cudaMemcpyDeviceToDevice, st_));
+      B200_CHECK(cudaMemcpyAsync(vf_.y0.get(), vf_.y.get(), m * sizeof(float), cudaMemcpyDeviceToDevice, st_));
+      B200_CHECK(cudaMemcpyAsync(vf_.yh.get(), vf_.y.get(), m * sizeof(float), cudaMemcpyDeviceToDevice, st_));
+    } else {
+      B200_CHECK(cudaMemcpyAsync(vd_.x0.get(), vd_.x.get(), n * sizeof(double), cudaMemcpyDeviceToDevice, st_));
+      B200_CHECK(cudaMemcpyAsync(vd_.xh.get(), vd_.x.get(), n * sizeof(double), cudaMemcpyDeviceToDevice, st_));
+      B200_CHECK(cudaMemcpyAsync(vd_.y0.get(), vd_.y.get(), m * sizeof(double), cudaMemcpyDeviceToDevice, st_));
+      B200_CHECK(cudaMemcpyAsync(vd_.yh.get(), vd_.y.get(), m * sizeof(double), cudaMemcpyDeviceToDevice, st_));
+    }
+  }
+  double pid_integral = 0.0, pid_last = 0.0, best_omega = omega, best_balance = 1e300;
+  long long it = 0, inner = 0;
+  double r0 = -1.0, r_last = std::numeric_limits<double>::infinity();
+  StepParams& hp = *hparams_.get();
+  for (;;) {
+    const double tau = eta_ / omega, sigma = eta_ * omega;
+    hp.tau = tau;
+    hp.sigma = sigma;
+    hp.rho = rho;
+    hp.inner0 = inner;
+    hp.K = K;
+    hp.done = 0;
+    hp.skip_r0 = inner != 0 ? 1 : 0;
+    B200_CHECK(cudaMemcpyAsync(params_.get(), &hp, sizeof(StepParams), cudaMemcpyHostToDevice, st_));
+    const bool fresh = inner == 0;
+    const int pidx = mixed_now_ ? 1 : 0;
+    if (mixed_now_) capture_epoch<float>();
+    else capture_epoch<double>();
+    B200_CHECK(cudaGraphLaunch(g_epoch_[pidx], st_));
+    kernels_ += epoch_kernels_[pidx];
+    it += K;
+    inner += K;
+    const int variant = it >= 4LL * K ? (((it / K) % 4 == 0) ? 2 : 1) : 0;
+    if (mixed_now_) capture_check<float>(variant);
+    else capture_check<double>(variant);
+    B200_CHECK(cudaGraphLaunch(g_check_[pidx][variant], st_));
+    kernels_ += check_kernels_[pidx][variant];
+    B200_CHECK(cudaStreamSynchronize(st_));
+    ++R.checks;
+    {
+      float a = 0, b = 0;
+      B200_CHECK(cudaEventElapsedTime(&a, ev_[0], ev_[1]));
+      B200_CHECK(cudaEventElapsedTime(&b, ev_[2], ev_[3]));
+      iter_ms_ += a + b;
+      iter_launches_ += 2LL * K;
+    }
+    const double* h = hres_.get();
+    if (fresh) r0 = std::sqrt(std_max(omega * h[kPx0] + h[kPy0] / omega + 2.0 * eta_ * h[kCross0], 0.0));
+    const double r = std::sqrt(std_max(omega * h[kPx] + h[kPy] / omega + 2.0 * eta_ * h[kCross], 0.0));
+    const Kkt k = read_kkt(h);
+    if (o_.verbosity >= 2)
+      std::fprintf(stderr, "r2hpdhg-b200 it %8lld  t %7.2fs  pobj %+.10e  dobj %+.10e  rp %.2e  rd %.2e  gap %.2e  %s\n",
+                   it, elapsed(), k.primal_obj, k.dual_obj, k.rel_primal(), k.rel_dual(), k.rel_gap(),
+                   mixed_now_ ? "fp32" : "fp64");
+    if (!k.finite() || !std::isfinite(r)) return done(Status::NumericalError, true, it, "non-finite iterate", 0);
+    if (fast_it_ < 0 && k.rel_kkt() <= kFirstOrderFast) fast_it_ = it;
+    if (k.converged(o_.tolerance)) return done(Status::Optimal, true, it, msg, 0);
+    if (it >= o_.iteration_limit) return done(Status::IterationLimit, true, it, msg, 0);
+    if (elapsed() > o_.time_limit) return done(Status::TimeLimit, true, it, msg, 0);
+    if (variant >= 1) {  // EngineContext::check_infeasibility + ray_test (engine.cpp:82-184)
+      auto test = [&](int which, std::string& why) {
+        const int s_rmax = which == 2 ? kMaxRmax2 : kMaxRmax, s_dabs = which == 2 ? kMaxDabs2 : kMaxDabs;
+        const int s_dviol = which == 2 ? kMaxDviol2 : kMaxDviol, s_pviol = which == 2 ? kMaxPviol2 : kMaxPviol;
+        const double obj = h[which == 2 ? kRayObj2 : kRayObj], mag = h[which == 2 ? kRayMag2 : kRayMag];
+        const double cd = h[which == 2 ? kRayCd2 : kRayCd], cmag = h[which == 2 ? kRayCmag2 : kRayCmag];
+        const double rmax = slot_max(h, s_rmax), dmax = slot_max(h, s_dabs);
+        bool pinf = false, dinf = false;
+        double dro = 0, drv = 0, pro = 0, prv = 0;
+        if (rmax > 0) {
+          const double viol = slot_max(h, s_dviol), scale = std_max(rmax, viol);
+          dro = obj / scale, drv = viol / scale;
+          pinf = dro > 0 && obj > kFirstOrderInfeasible * mag && drv <= kFirstOrderInfeasible * dro;
+        }
+        if (dmax > 0) {
+          const double viol = slot_max(h, s_pviol), scale = std_max(dmax, viol);
+          pro = cd / scale, prv = viol / scale;
+          dinf = pro < 0 && -cd > kFirstOrderInfeasible * cmag && prv <= kFirstOrderInfeasible * -pro;
+        }
+        char buf[200];
+        if (pinf) {
+          std::snprintf(buf, sizeof buf, "primal infeasible: dual ray certificate (objective %f, violation %f)", dro, drv);
+          why = buf;
+          return Status::Infeasible;
+        }
+        if (dinf) {
+          const bool feasible = k.rel_primal() <= kVerifyPrimal && k.primal_max_rel <= kVerifyPrimal;
+          std::snprintf(buf, sizeof buf, "unbounded: primal ray certificate (c'd %f, violation %f)%s", pro, prv,
+                        feasible ? " at a primal-feasible iterate" : "; iterate not primal-feasible yet");
+          why = buf;
+          return Status::Unbounded;
+        }
+        return Status::NotSolved;
+      };
+      std::string why;
+      int which = 1;
+      Status s = test(1, why);
+      if (s == Status::NotSolved && variant == 2) {
+        which = 2;
+        s = test(2, why);
+        if (s != Status::NotSolved) why += " (drift since the restart anchor)";
+      }
+      if (s != Status::NotSolved) return done(s, true, it, why, which);
+    }
+    // PrecisionPolicy::on_check (engine.cpp:61-79)
+    bool promoted = false;
+    if (o_.mixed && mixed_now_) {
+      const double rk = k.rel_kkt();
+      if (rk < 0.9 * pol_best_) pol_best_ = rk, pol_since_best_ = 0;
+      else ++pol_since_best_;
+      const bool reached = rk <= kMixedPrecisionSwitch && o_.tolerance < kMixedPrecisionSwitch;
+      if (reached || pol_since_best_ >= 10) {
+        promote();
+        switch_it_ = it;
+        promoted = true;
+        msg += std::string(msg.empty() ? "" : "; ") + "fp32 -> fp64 at iteration " + std::to_string(it);
+      }
+    }
+    const bool ratios_ok = r0 > 0 && std::isfinite(r0) && r > 0;
+    const bool restart_now = promoted ||
+                             (ratios_ok && (r <= o_.restart_sufficient * r0 ||
+                                            (r <= o_.restart_necessary * r0 && r > r_last))) ||
+                             static_cast<double>(inner) >= o_.restart_artificial * static_cast<double>(it);
+    r_last = r;
+    if (!restart_now) continue;
+    // PID primal weight (r2hpdhg.cpp:126-148)
+    const double dxn = std::sqrt(h[kDxn2]), dyn = std::sqrt(h[kDyn2]);
+    const bool both_pos = k.rel_dual() > 0 && k.rel_primal() > 0;
+    const double ratio = both_pos ? k.rel_dual() / k.rel_primal() : 1.0;
+    if (dxn > 1e-16 && dyn > 1e-16 && dxn < 1e12 && dyn < 1e12 && ratio > 1e-8 && ratio < 1e8) {
+      const double e = std::log(dyn) - std::log(dxn) - std::log(omega);
+      pid_integral = o_.pid_integral_decay * pid_integral + e;
+      const double step = o_.pid_kp * e + o_.pid_ki * pid_integral + o_.pid_kd * (e - pid_last);
+      omega *= std::exp(std::clamp(step, -o_.pid_max_log_step, o_.pid_max_log_step));
+      pid_last = e;
+    } else {
+      omega = best_omega;
+      pid_integral = pid_last = 0.0;
+    }
+    const double balance = std::fabs(std::log10(ratio));
+    if (both_pos && balance < best_balance) {
+      best_balance = balance;
+      best_omega = omega;
+    }
+    primal_weight_ = omega;
+    ++R.restarts;
+    if (o_.verbosity >= 2)
+      std::fprintf(stderr, "  restart at %lld: r/r0 %.3f  omega %.4e  dx %.3e dy %.3e\n", it, r / r0, omega, dxn, dyn);
+    if (mixed_now_) restart<float>();
+    else restart<double>();
+    inner = 0;
+    r_last = std::numeric_limits<double>::infinity();
+  }
+}
+
+}  // namespace
+
+EngineResult run_engine(const DeviceModel& M, const EngineOptions& opt, const DeviceOutputs& out, void* stream) {
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  bool own = false;
+  if (!st) {
+    // The caller's inputs may still be in flight on the legacy default stream: finish them,
+    // then run on a stream of our own (capturable, unlike the legacy stream).
+    B200_CHECK(cudaDeviceSynchronize());
+    B200_CHECK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    own = true;
+  }
+  struct StreamGuard {
+    cudaStream_t s;
+    bool own;
+    ~StreamGuard() {
+      if (own) cudaStreamDestroy(s);
+    }
+  } guard{st, own};
+  Engine e(M, opt, st);
+  return e.run(out);
+}
+
+EngineResult run_engine_host(const HostModelView& H, const EngineOptions& opt, HostOutputs& out) {
+  cudaStream_t st;
+  B200_CHECK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  struct StreamGuard {
+    cudaStream_t s;
+    ~StreamGuard() { cudaStreamDestroy(s); }
+  } guard{st};
+  const int m = H.m, n = H.n;
+  const long long nnz = H.col_start[n];
+  DevBuf<double> c, cl, cu, rl, ru, v, x, y, z, dr, pr;
+  DevBuf<int> cs, ri;
+  c.upload(H.c, n, st), cl.upload(H.col_lower, n, st), cu.upload(H.col_upper, n, st);
+  rl.upload(H.row_lower, m, st), ru.upload(H.row_upper, m, st);
+  cs.upload(H.col_start, static_cast<std::size_t>(n) + 1, st);
+  ri.upload(H.row_index, static_cast<std::size_t>(nnz), st);
+  v.upload(H.value, static_cast<std::size_t>(nnz), st);
+  x.alloc(n), z.alloc(n), pr.alloc(n), y.alloc(m), dr.alloc(m);
+  DeviceModel M;
+  M.m = m, M.n = n, M.sense = H.sense, M.offset = H.offset, M.nnz = nnz;
+  M.c = c.get(), M.col_lower = cl.get(), M.col_upper = cu.get(), M.row_lower = rl.get(), M.row_upper = ru.get();
+  M.col_start = cs.get(), M.row_index = ri.get(), M.value = v.get();
+  DeviceOutputs o{x.get(), y.get(), z.get(), dr.get(), pr.get()};
+  EngineResult R = run_engine(M, opt, o, st);
+  out.x.resize(n), out.y.resize(m), out.z.resize(n);
+  x.download(out.x.data(), n, st);
+  y.download(out.y.data(), m, st);
+  z.download(out.z.data(), n, st);
+  if (R.have_dual_ray) out.dual_ray.resize(m), dr.download(out.dual_ray.data(), m, st);
+  if (R.have_primal_ray) out.primal_ray.resize(n), pr.download(out.primal_ray.data(), n, st);
+  B200_CHECK(cudaStreamSynchronize(st));
+  return R;
+}
+
+}  // namespace b200

@@ -1,0 +1,756 @@
+// solver.cpp — model contract, presolve/postsolve, in-process check and the solve()
+// dispatcher around the GPU engine. Each function follows the reference function named in
+// its comment (file:line in the reference project); the engine itself runs on the GPU.
+#include "solver.hpp"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <sstream>
+#include <stdexcept>
+
+namespace b200 {
+
+// ============================================================ Model (model.cpp)
+std::string Model::validate() const {  // model.cpp:93-151
+  std::ostringstream err;
+  const auto n = static_cast<std::size_t>(num_cols);
+  const auto m = static_cast<std::size_t>(num_rows);
+  if (num_rows < 0 || num_cols < 0) return "negative dimension";
+  if (sense != 1 && sense != -1) return "sense must be +1 or -1";
+  if (!std::isfinite(obj_offset)) return "obj_offset is not finite";
+  if (obj.size() != n) return "obj has wrong size";
+  if (col_lower.size() != n || col_upper.size() != n) return "column bounds have wrong size";
+  if (row_lower.size() != m || row_upper.size() != m) return "row bounds have wrong size";
+  if (col_start.size() != n + 1) return "col_start must have num_cols+1 entries";
+  if (col_start[0] != 0) return "col_start[0] must be 0";
+  if (row_index.size() != value.size()) return "row_index and value differ in size";
+  if (static_cast<std::size_t>(col_start[n]) != value.size()) return "col_start[n] != nnz";
+  std::vector<int> seen(m, -1);
+  for (std::size_t j = 0; j < n; ++j) {
+    if (col_start[j + 1] < col_start[j]) {
+      err << "col_start not monotone at column " << j;
+      return err.str();
+    }
+    if (!std::isfinite(obj[j])) {
+      err << "objective coefficient of column " << j << " is not finite";
+      return err.str();
+    }
+    for (int k = col_start[j]; k < col_start[j + 1]; ++k) {
+      const int i = row_index[k];
+      if (i < 0 || static_cast<std::size_t>(i) >= m) {
+        err << "row index out of range in column " << j;
+        return err.str();
+      }
+      if (seen[i] == static_cast<int>(j)) {
+        err << "duplicate entry (" << i << "," << j << ")";
+        return err.str();
+      }
+      seen[i] = static_cast<int>(j);
+      if (!std::isfinite(value[k])) {
+        err << "matrix entry (" << i << "," << j << ") is not finite";
+        return err.str();
+      }
+    }
+  }
+  auto check_bounds = [&](const std::vector<double>& lo, const std::vector<double>& up, const char* what) {
+    for (std::size_t k = 0; k < lo.size(); ++k) {
+      std::ostringstream e;
+      if (std::isnan(lo[k]) || std::isnan(up[k])) e << what << " bound " << k << " is NaN";
+      else if (lo[k] == kInf) e << what << " lower bound " << k << " is +inf";
+      else if (up[k] == -kInf) e << what << " upper bound " << k << " is -inf";
+      if (!e.str().empty()) return e.str();
+    }
+    return std::string();
+  };
+  if (auto s = check_bounds(col_lower, col_upper, "column"); !s.empty()) return s;
+  return check_bounds(row_lower, row_upper, "row");
+}
+
+std::string Model::crossed_bounds() const {  // model.cpp:153-167
+  auto first = [](const std::vector<double>& lo, const std::vector<double>& up, const char* what) {
+    for (std::size_t k = 0; k < lo.size() && k < up.size(); ++k)
+      if (lo[k] > up[k]) {
+        std::ostringstream e;
+        e << what << " " << k << " has lower bound " << lo[k] << " > upper bound " << up[k];
+        return e.str();
+      }
+    return std::string();
+  };
+  if (auto s = first(col_lower, col_upper, "column"); !s.empty()) return s;
+  return first(row_lower, row_upper, "row");
+}
+
+double Model::objective_value(const std::vector<double>& x) const {  // model.cpp:169-173
+  double v = obj_offset;
+  for (int j = 0; j < num_cols; ++j) v += obj[j] * x[j];
+  return v;
+}
+
+std::vector<double> Model::row_activity(const std::vector<double>& x) const {  // model.cpp:175-180
+  std::vector<double> ax(num_rows, 0.0);
+  for (int j = 0; j < num_cols; ++j)
+    for (int k = col_start[j]; k < col_start[j + 1]; ++k) ax[row_index[k]] += value[k] * x[j];
+  return ax;
+}
+
+std::uint64_t Model::fingerprint() const {  // model.cpp:20-85: FNV-1a over the canonical numbers
+  std::uint64_t h = 0xcbf29ce484222325ULL;
+  auto bytes = [&](const void* p, std::size_t n) {
+    const auto* b = static_cast<const unsigned char*>(p);
+    for (std::size_t i = 0; i < n; ++i) h ^= b[i], h *= 0x100000001b3ULL;
+  };
+  auto u64 = [&](std::uint64_t v) { bytes(&v, sizeof v); };
+  auto i64 = [&](std::int64_t v) { bytes(&v, sizeof v); };
+  auto f64 = [&](double v) {
+    if (v == 0.0) v = 0.0;
+    std::uint64_t bits;
+    if (std::isnan(v)) bits = 0x7ff8000000000000ULL;
+    else std::memcpy(&bits, &v, sizeof bits);
+    u64(bits);
+  };
+  auto f64s = [&](const std::vector<double>& v) {
+    u64(v.size());
+    for (double d : v) f64(d);
+  };
+  i64(num_rows), i64(num_cols), i64(sense), f64(obj_offset);
+  f64s(obj), f64s(col_lower), f64s(col_upper), f64s(row_lower), f64s(row_upper);
+  u64(value.size());
+  std::vector<std::pair<int, double>> col;
+  for (int j = 0; j < num_cols; ++j) {
+    col.clear();
+    for (int k = col_start[j]; k < col_start[j + 1]; ++k) col.emplace_back(row_index[k], value[k]);
+    std::sort(col.begin(), col.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+    i64(static_cast<std::int64_t>(col.size()));
+    for (const auto& [i, v] : col) i64(i), f64(v);
+  }
+  for (int j = 0; j < num_cols; ++j) i64(0);
+  return h;
+}
+
+HostModelView Model::view() const {
+  HostModelView v;
+  v.m = num_rows, v.n = num_cols, v.sense = sense, v.offset = obj_offset;
+  v.c = obj.data(), v.col_lower = col_lower.data(), v.col_upper = col_upper.data();
+  v.row_lower = row_lower.data(), v.row_upper = row_upper.data();
+  v.col_start = col_start.data(), v.row_index = row_index.data(), v.value = value.data();
+  return v;
+}
+
+// ============================================================ check (solution_checker.cpp)
+namespace {
+struct DualTerm {
+  double violation, contribution, complementarity;
+};
+DualTerm evaluate_multiplier(double mult, double lo, double up, double val) {  // solution_checker.cpp:30-48
+  DualTerm t{0.0, 0.0, 0.0};
+  if (mult > 0.0) {
+    if (lo == -kInf) t.violation = mult;
+    else t.contribution = mult * lo, t.complementarity = mult * std::fabs(val - lo);
+  } else if (mult < 0.0) {
+    if (up == kInf) t.violation = -mult;
+    else t.contribution = mult * up, t.complementarity = -mult * std::fabs(up - val);
+  }
+  return t;
+}
+double bound_violation(double val, double lo, double up) {
+  double v = 0.0;
+  if (lo != -kInf) v = std::max(v, (lo - val) / (1.0 + std::fabs(lo)));
+  if (up != kInf) v = std::max(v, (val - up) / (1.0 + std::fabs(up)));
+  return v;
+}
+}  // namespace
+
+CheckReport check_solution(const Model& lp, const std::vector<double>& x, const std::vector<double>& row_dual) {
+  CheckReport rep;
+  const int m = lp.num_rows, n = lp.num_cols;
+  const double sense = lp.sense;
+  auto reject = [&rep]() {
+    rep.max_primal_violation = rep.max_dual_violation = rep.relative_gap = kInf;
+    rep.primal_ok = rep.dual_ok = rep.gap_ok = false;
+    return rep;
+  };
+  if (static_cast<int>(x.size()) != n || static_cast<int>(row_dual.size()) != m) return reject();
+  for (double v : x)
+    if (!std::isfinite(v)) return reject();
+  for (double v : row_dual)
+    if (!std::isfinite(v)) return reject();
+  const std::vector<double> ax = lp.row_activity(x);
+  for (int i = 0; i < m; ++i)
+    rep.max_primal_violation = std::max(rep.max_primal_violation, bound_violation(ax[i], lp.row_lower[i], lp.row_upper[i]));
+  for (int j = 0; j < n; ++j)
+    rep.max_primal_violation = std::max(rep.max_primal_violation, bound_violation(x[j], lp.col_lower[j], lp.col_upper[j]));
+  std::vector<double> y(m);
+  for (int i = 0; i < m; ++i) y[i] = sense * row_dual[i];
+  std::vector<double> aty(n, 0.0);
+  for (int j = 0; j < n; ++j)
+    for (int k = lp.col_start[j]; k < lp.col_start[j + 1]; ++k) aty[j] += lp.value[k] * y[lp.row_index[k]];
+  double dual_obj_min = 0.0, primal_obj_min = 0.0, c_scale = 1.0;
+  for (int j = 0; j < n; ++j) c_scale = std::max(c_scale, std::fabs(lp.obj[j]));
+  for (int i = 0; i < m; ++i) {
+    const DualTerm t = evaluate_multiplier(y[i], lp.row_lower[i], lp.row_upper[i], ax[i]);
+    rep.max_dual_violation = std::max(rep.max_dual_violation, t.violation / c_scale);
+    rep.max_complementarity = std::max(rep.max_complementarity, t.complementarity);
+    dual_obj_min += t.contribution;
+  }
+  for (int j = 0; j < n; ++j) {
+    const double c = sense * lp.obj[j];
+    const double d = c - aty[j];
+    const DualTerm t = evaluate_multiplier(d, lp.col_lower[j], lp.col_upper[j], x[j]);
+    rep.max_dual_violation = std::max(rep.max_dual_violation, t.violation / c_scale);
+    rep.max_complementarity = std::max(rep.max_complementarity, t.complementarity);
+    dual_obj_min += t.contribution;
+    primal_obj_min += c * x[j];
+  }
+  rep.primal_objective = sense * primal_obj_min + lp.obj_offset;
+  rep.dual_objective = sense * dual_obj_min + lp.obj_offset;
+  rep.relative_gap = std::fabs(rep.primal_objective - rep.dual_objective) /
+                     (1.0 + std::fabs(rep.primal_objective) + std::fabs(rep.dual_objective));
+  if (!std::isfinite(rep.primal_objective) || !std::isfinite(rep.dual_objective)) return reject();
+  rep.primal_ok = rep.max_primal_violation <= 1e-6;
+  rep.dual_ok = rep.max_dual_violation <= 1e-6;
+  rep.gap_ok = rep.relative_gap <= 1e-6;
+  return rep;
+}
+
+std::string CheckReport::summary() const {
+  char buf[256];
+  std::snprintf(buf, sizeof buf, "primal viol %.1e  dual viol %.1e  compl %.1e  gap %.1e  => %s", max_primal_violation,
+                max_dual_violation, max_complementarity, relative_gap, passed() ? "PASS" : "FAIL");
+  return buf;
+}
+
+// ============================================================ presolve (presolve.cpp)
+namespace {
+constexpr double kFeasTol = 1e-9;
+bool within(double v, double lo, double up) {
+  return v >= lo - kFeasTol * (1 + std::fabs(lo)) && v <= up + kFeasTol * (1 + std::fabs(up));
+}
+}  // namespace
+
+PresolveResult presolve(const Model& M) {  // presolve.cpp:22-156 (LP: no integer columns here)
+  PresolveResult r;
+  const int m = M.num_rows, n = M.num_cols;
+  // row access: CSR of A, columns in increasing order inside each row (la::csr_from_model)
+  std::vector<int> rp(static_cast<std::size_t>(m) + 1, 0), rc(M.nnz());
+  std::vector<double> rv(M.nnz());
+  for (std::size_t k = 0; k < M.nnz(); ++k) ++rp[M.row_index[k] + 1];
+  for (int i = 0; i < m; ++i) rp[i + 1] += rp[i];
+  {
+    std::vector<int> next(rp.begin(), rp.end() - 1);
+    for (int j = 0; j < n; ++j)
+      for (int k = M.col_start[j]; k < M.col_start[j + 1]; ++k) {
+        const int p = next[M.row_index[k]]++;
+        rc[p] = j;
+        rv[p] = M.value[k];
+      }
+  }
+  std::vector<double> rl = M.row_lower, ru = M.row_upper, cl = M.col_lower, cu = M.col_upper;
+  std::vector<char> row_alive(m, 1), col_alive(n, 1);
+  std::vector<int> row_cnt(m), col_cnt(n);
+  for (int i = 0; i < m; ++i) row_cnt[i] = rp[i + 1] - rp[i];
+  for (int j = 0; j < n; ++j) col_cnt[j] = M.col_start[j + 1] - M.col_start[j];
+  r.fixed_value.assign(n, kNaN);
+  double offset = M.obj_offset;
+  auto infeasible = [&](const std::string& why) {
+    r.outcome = PresolveResult::Outcome::Infeasible;
+    r.message = why;
+    return r;
+  };
+  bool changed = true;
+  while (changed) {
+    changed = false;
+    for (int i = 0; i < m; ++i) {  // rows: empty (R1) and singleton (R4)
+      if (!row_alive[i]) continue;
+      if (row_cnt[i] == 0) {
+        if (!within(0.0, rl[i], ru[i])) return infeasible("empty row " + std::to_string(i) + " excludes 0");
+        row_alive[i] = 0;
+        ++r.removed_rows;
+        changed = true;
+      } else if (row_cnt[i] == 1) {
+        int j = -1;
+        double a = 0;
+        for (int p = rp[i]; p < rp[i + 1]; ++p)
+          if (col_alive[rc[p]]) j = rc[p], a = rv[p];
+        if (j < 0 || a == 0.0) continue;
+        const double lo = a > 0 ? rl[i] / a : ru[i] / a;
+        const double hi = a > 0 ? ru[i] / a : rl[i] / a;
+        const bool set_lower = lo > cl[j], set_upper = hi < cu[j];
+        double nl = set_lower ? lo : cl[j], nu = set_upper ? hi : cu[j];
+        if (nl > nu) {
+          if (nl - nu > kFeasTol * (1 + std::fabs(nl)))
+            return infeasible("singleton row " + std::to_string(i) + " conflicts with the bounds of its column");
+          nl = nu = 0.5 * (nl + nu);
+        }
+        cl[j] = nl;
+        cu[j] = nu;
+        r.singletons.push_back({i, j, a, set_lower, set_upper});
+        r.tightened_bounds += set_lower + set_upper;
+        row_alive[i] = 0;
+        --col_cnt[j];
+        ++r.removed_rows;
+        changed = true;
+      }
+    }
+    for (int j = 0; j < n; ++j) {  // columns: fixed (R2) and empty (R3)
+      if (!col_alive[j]) continue;
+      double v;
+      if (cl[j] == cu[j]) {
+        v = cl[j];
+      } else if (col_cnt[j] == 0) {
+        const double c = M.sense * M.obj[j];
+        v = c > 0 ? cl[j] : (c < 0 ? cu[j] : std::min(std::max(0.0, cl[j]), cu[j]));
+        if (!std::isfinite(v)) continue;
+      } else {
+        continue;
+      }
+      for (int p = M.col_start[j]; p < M.col_start[j + 1]; ++p) {
+        const int i = M.row_index[p];
+        if (!row_alive[i]) continue;
+        const double t = M.value[p] * v;
+        if (std::isfinite(rl[i])) rl[i] -= t;
+        if (std::isfinite(ru[i])) ru[i] -= t;
+        --row_cnt[i];
+      }
+      offset += M.obj[j] * v;
+      r.fixed_value[j] = v;
+      col_alive[j] = 0;
+      ++r.removed_cols;
+      changed = true;
+    }
+  }
+  if (r.removed_rows == 0 && r.removed_cols == 0) {
+    r.outcome = PresolveResult::Outcome::Unchanged;
+    return r;
+  }
+  Model& R = r.reduced;
+  std::vector<int> new_row(m, -1);
+  for (int i = 0; i < m; ++i)
+    if (row_alive[i]) new_row[i] = static_cast<int>(r.row_map.size()), r.row_map.push_back(i);
+  for (int j = 0; j < n; ++j)
+    if (col_alive[j]) r.col_map.push_back(j);
+  R.sense = M.sense;
+  R.obj_offset = offset;
+  R.num_rows = static_cast<int>(r.row_map.size());
+  R.num_cols = static_cast<int>(r.col_map.size());
+  R.col_start.push_back(0);
+  for (int j : r.col_map) {
+    R.obj.push_back(M.obj[j]);
+    R.col_lower.push_back(cl[j]);
+    R.col_upper.push_back(cu[j]);
+    for (int p = M.col_start[j]; p < M.col_start[j + 1]; ++p) {
+      const int i = M.row_index[p];
+      if (new_row[i] >= 0) R.row_index.push_back(new_row[i]), R.value.push_back(M.value[p]);
+    }
+    R.col_start.push_back(static_cast<int>(R.value.size()));
+  }
+  for (int i : r.row_map) {
+    R.row_lower.push_back(rl[i]);
+    R.row_upper.push_back(ru[i]);
+  }
+  r.outcome = PresolveResult::Outcome::Reduced;
+  return r;
+}
+
+Solution postsolve(const Model& M, const PresolveResult& r, const Solution& red) {  // presolve.cpp:158-193
+  Solution s = red;
+  const int m = M.num_rows, n = M.num_cols;
+  s.x.assign(n, 0.0);
+  s.y.assign(m, 0.0);
+  const bool have_x = red.x.size() == r.col_map.size();
+  const bool have_y = red.y.size() == r.row_map.size();
+  for (int j = 0; j < n; ++j)
+    if (!std::isnan(r.fixed_value[j])) s.x[j] = r.fixed_value[j];
+  if (have_x)
+    for (std::size_t c = 0; c < r.col_map.size(); ++c) s.x[r.col_map[c]] = red.x[c];
+  if (have_y)
+    for (std::size_t q = 0; q < r.row_map.size(); ++q) s.y[r.row_map[q]] = red.y[q];
+  for (auto it = r.singletons.rbegin(); it != r.singletons.rend(); ++it) {
+    const int j = it->col;
+    double z = M.obj[j];
+    for (int p = M.col_start[j]; p < M.col_start[j + 1]; ++p) z -= M.value[p] * s.y[M.row_index[p]];
+    const double zm = M.sense * z;
+    if ((zm > 0 && it->set_lower) || (zm < 0 && it->set_upper)) s.y[it->row] = z / it->a;
+  }
+  s.z = M.obj;
+  for (int j = 0; j < n; ++j)
+    for (int p = M.col_start[j]; p < M.col_start[j + 1]; ++p) s.z[j] -= M.value[p] * s.y[M.row_index[p]];
+  s.objective = M.objective_value(s.x);
+  if (!have_x) {
+    s.x.clear();
+    s.objective = kNaN;
+  }
+  if (!have_y) s.y.clear(), s.z.clear();
+  return s;
+}
+
+// ============================================================ dispatcher (solve.cpp)
+namespace {
+
+using clock_t_ = std::chrono::steady_clock;
+double since(clock_t_::time_point t0) { return std::chrono::duration<double>(clock_t_::now() - t0).count(); }
+
+const char* alg_name(Algorithm a) {
+  switch (a) {
+    case Algorithm::Auto: return "auto";
+    case Algorithm::Oracle: return "oracle";
+    case Algorithm::Pdlp: return "pdlp";
+    case Algorithm::R2hpdhg: return "r2hpdhg";
+    default: return "simplex";
+  }
+}
+
+void note(Solution& s, const std::string& t) { s.message += std::string(s.message.empty() ? "" : "; ") + t; }
+
+EngineOptions engine_options(const Options& o) {  // engine.cpp:168-186
+  EngineOptions e;
+  e.tolerance = o.tolerance;
+  e.time_limit = o.time_limit;
+  e.iteration_limit = o.iteration_limit;
+  e.check_every = o.check_every > 0 ? o.check_every : 64;
+  e.mixed = o.precision == Precision::Mixed;
+  e.exact = o.exact;
+  e.scaling = o.scaling;
+  e.reflection = o.reflection;
+  e.warm_x = o.warm_x;
+  e.warm_y = o.warm_y;
+  e.warm_primal_weight = o.warm_primal_weight;
+  e.kkt_b_norm = o.kkt_b_norm;
+  e.kkt_c_norm = o.kkt_c_norm;
+  e.kkt_obj_shift = o.kkt_obj_shift;
+  e.verbosity = o.verbosity;
+  return e;
+}
+
+Solution trivially_infeasible(const Options& options, const std::string& why) {
+  Solution s;
+  s.status = Status::Infeasible;
+  s.precision = options.precision == Precision::Mixed ? "mixed" : "fp64";
+  s.message = "bounds cross: " + why;
+  return s;
+}
+
+// The first-order engine on the GPU for one model (solve.cpp:469-609, LP part).
+Solution solve_direct(const Model& model, const Options& options) {
+  const auto t0 = clock_t_::now();
+  Solution sol;
+  sol.precision = options.precision == Precision::Mixed ? "mixed" : "fp64";
+  if (auto err = model.validate(); !err.empty()) {
+    sol.status = Status::NotSolved;
+    sol.message = "invalid model: " + err;
+    return sol;
+  }
+  if ((!options.warm_x.empty() && static_cast<int>(options.warm_x.size()) != model.num_cols) ||
+      (!options.warm_y.empty() && static_cast<int>(options.warm_y.size()) != model.num_rows)) {
+    sol.status = Status::NotSolved;
+    sol.message = "warm start vectors have the wrong size";
+    return sol;
+  }
+  auto finite = [](const std::vector<double>& v) { return std::all_of(v.begin(), v.end(), [](double a) { return std::isfinite(a); }); };
+  if (!finite(options.warm_x) || !finite(options.warm_y) ||
+      !(options.warm_primal_weight >= 0 && std::isfinite(options.warm_primal_weight))) {
+    sol.status = Status::NotSolved;
+    sol.message = "warm start contains non-finite values";
+    return sol;
+  }
+  if (auto why = model.crossed_bounds(); !why.empty()) return trivially_infeasible(options, why);
+  try {
+    HostOutputs out;
+    const EngineResult R = run_engine_host(model.view(), engine_options(options), out);
+    sol.status = R.status;
+    sol.iterations = R.iterations;
+    sol.objective = R.objective;
+    sol.dual_objective = R.dual_objective;
+    sol.primal_residual = R.primal_residual;
+    sol.dual_residual = R.dual_residual;
+    sol.gap = R.gap;
+    sol.primal_weight = R.primal_weight;
+    sol.setup_seconds = R.setup_seconds;
+    sol.message = R.message;
+    sol.engine_result = R;
+    sol.x = std::move(out.x);
+    sol.y = std::move(out.y);
+    sol.z = std::move(out.z);
+    if (R.have_dual_ray) sol.dual_ray = std::move(out.dual_ray);
+    if (R.have_primal_ray) sol.primal_ray = std::move(out.primal_ray);
+  } catch (const std::bad_alloc&) {
+    sol = Solution{};
+    sol.status = Status::NotSolved;
+    sol.message = "out of memory";
+  } catch (const std::exception& e) {
+    sol = Solution{};
+    sol.status = Status::NumericalError;
+    sol.message = e.what();
+  }
+  sol.seconds = since(t0);
+  return sol;
+}
+
+// Presolve wrapper (solve.cpp:266-467, LP part).
+Solution solve_impl(const Model& model, const Options& options) {
+  const bool bad_warm = (!options.warm_x.empty() && static_cast<int>(options.warm_x.size()) != model.num_cols) ||
+                        (!options.warm_y.empty() && static_cast<int>(options.warm_y.size()) != model.num_rows);
+  auto finite = [](const std::vector<double>& v) { return std::all_of(v.begin(), v.end(), [](double a) { return std::isfinite(a); }); };
+  const bool bad_warm_values = !finite(options.warm_x) || !finite(options.warm_y);
+  if (!options.presolve || bad_warm || bad_warm_values || !model.validate().empty()) return solve_direct(model, options);
+  if (auto why = model.crossed_bounds(); !why.empty()) return trivially_infeasible(options, why);
+  const auto t0 = clock_t_::now();
+  PresolveResult pr = presolve(model);
+  const double presolve_s = since(t0);
+  if (pr.outcome == PresolveResult::Outcome::Unchanged) {
+    Solution s = solve_direct(model, options);
+    s.presolve_seconds = presolve_s;
+    return s;
+  }
+  Options inner = options;
+  inner.presolve = false;
+  {
+    double b2 = 0, c2 = 0;
+    for (int i = 0; i < model.num_rows; ++i) {
+      const double lo = std::isfinite(model.row_lower[i]) ? std::fabs(model.row_lower[i]) : 0.0;
+      const double up = std::isfinite(model.row_upper[i]) ? std::fabs(model.row_upper[i]) : 0.0;
+      b2 += std::max(lo, up) * std::max(lo, up);
+    }
+    for (double c : model.obj) c2 += c * c;
+    inner.kkt_b_norm = std::sqrt(b2);
+    inner.kkt_c_norm = std::sqrt(c2);
+    inner.kkt_obj_shift = model.sense * (pr.reduced.obj_offset - model.obj_offset);
+  }
+  auto budget = [&](Options o, long long used) {
+    o.time_limit = std::max(0.0, options.time_limit - since(t0));
+    o.iteration_limit = std::max<long long>(0, options.iteration_limit - used);
+    return o;
+  };
+  auto on_original = [&](const Solution& why, const std::string& what) {
+    Options direct = budget(options, why.iterations);
+    direct.presolve = false;
+    Solution d = solve_direct(model, direct);
+    d.iterations += why.iterations;
+    d.seconds = since(t0);
+    note(d, "presolve: " + what + "; re-solved the original model for an original-space certificate");
+    return d;
+  };
+  if (pr.outcome == PresolveResult::Outcome::Infeasible) {
+    Solution none;
+    return on_original(none, "reduction found infeasibility (" + pr.message + ")");
+  }
+  if (!options.warm_x.empty()) {
+    inner.warm_x.clear();
+    for (int j : pr.col_map) inner.warm_x.push_back(options.warm_x[j]);
+  }
+  if (!options.warm_y.empty()) {
+    inner.warm_y.clear();
+    for (int i : pr.row_map) inner.warm_y.push_back(options.warm_y[i]);
+  }
+  Solution red;
+  if (pr.reduced.num_cols == 0 && pr.reduced.num_rows == 0) {
+    red.status = Status::Optimal;
+    red.engine = "presolve";
+  } else {
+    red = solve_direct(pr.reduced, budget(inner, 0));
+  }
+  if (red.status == Status::Infeasible || red.status == Status::Unbounded)
+    return on_original(red, std::string("reduced model ") + status_name(red.status));
+  Solution post = postsolve(model, pr, red);
+  const std::string pnote = "presolve removed " + std::to_string(pr.removed_rows) + " rows, " +
+                            std::to_string(pr.removed_cols) + " cols";
+  post.message = post.message.empty() ? pnote : post.message + "; " + pnote;
+  auto passes = [&](const Solution& s) {
+    if (static_cast<int>(s.x.size()) != model.num_cols || static_cast<int>(s.y.size()) != model.num_rows) return false;
+    // original_kkt(model, s).converged(tol) (solve.cpp:77-84): KKT of (x, sense·y) on the original
+    // model with its own norms. check_solution's measures are not the same test, so the KKT
+    // statistics are recomputed here exactly as kkt_general defines them.
+    const int m = model.num_rows, n = model.num_cols;
+    std::vector<double> ax = std::vector<double>(m, 0.0), aty(n, 0.0), ymin(s.y);
+    for (double& v : ymin) v *= model.sense;
+    {  // A·x row-sequential in column order (CSR of A)
+      std::vector<int> rp(static_cast<std::size_t>(m) + 1, 0);
+      for (std::size_t k = 0; k < model.nnz(); ++k) ++rp[model.row_index[k] + 1];
+      for (int i = 0; i < m; ++i) rp[i + 1] += rp[i];
+      std::vector<int> next(rp.begin(), rp.end() - 1), cc(model.nnz());
+      std::vector<double> vv(model.nnz());
+      for (int j = 0; j < n; ++j)
+        for (int k = model.col_start[j]; k < model.col_start[j + 1]; ++k) {
+          const int p = next[model.row_index[k]]++;
+          cc[p] = j, vv[p] = model.value[k];
+        }
+      for (int i = 0; i < m; ++i) {
+        double acc = 0;
+        for (int p = rp[i]; p < rp[i + 1]; ++p) acc += vv[p] * s.x[cc[p]];
+        ax[i] = acc;
+      }
+    }
+    for (int j = 0; j < n; ++j) {
+      double acc = 0;
+      for (int k = model.col_start[j]; k < model.col_start[j + 1]; ++k) acc += model.value[k] * ymin[model.row_index[k]];
+      aty[j] = acc;
+    }
+    double rp2 = 0, rd2 = 0, b2 = 0, c2 = 0, p = 0, d = 0, cinf = 0, pmax = 0, dmax = 0;
+    auto ev = [](double v, double lo, double up) {
+      if (v < lo) return (lo - v) / (1.0 + std::fabs(lo));
+      if (v > up) return (v - up) / (1.0 + std::fabs(up));
+      return 0.0;
+    };
+    for (int i = 0; i < m; ++i) {
+      const double lo = model.row_lower[i], up = model.row_upper[i];
+      const double viol = ax[i] < lo ? lo - ax[i] : (ax[i] > up ? ax[i] - up : 0.0);
+      rp2 += viol * viol;
+      pmax = std::max(pmax, ev(ax[i], lo, up));
+      const double bl = std::isfinite(lo) ? std::fabs(lo) : 0.0, bu = std::isfinite(up) ? std::fabs(up) : 0.0;
+      b2 += std::max(bl, bu) * std::max(bl, bu);
+      const double y = ymin[i];
+      if (y > 0) {
+        if (std::isfinite(lo)) d += y * lo;
+        else rd2 += y * y, dmax = std::max(dmax, y);
+      } else if (y < 0) {
+        if (std::isfinite(up)) d += y * up;
+        else rd2 += y * y, dmax = std::max(dmax, -y);
+      }
+    }
+    for (int j = 0; j < n; ++j) {
+      const double cj = model.sense * model.obj[j];
+      c2 += cj * cj;
+      cinf = std::max(cinf, std::fabs(cj));
+      p += cj * s.x[j];
+      pmax = std::max(pmax, ev(s.x[j], model.col_lower[j], model.col_upper[j]));
+      const double lam = cj - aty[j], lo = model.col_lower[j], up = model.col_upper[j];
+      double z;
+      if (std::isfinite(lo) && std::isfinite(up)) z = lam;
+      else if (std::isfinite(lo)) z = std::max(lam, 0.0);
+      else if (std::isfinite(up)) z = std::min(lam, 0.0);
+      else z = 0.0;
+      rd2 += (lam - z) * (lam - z);
+      dmax = std::max(dmax, std::fabs(lam - z));
+      if (z > 0) d += z * lo;
+      else if (z < 0) d += z * up;
+    }
+    const double rprim = std::sqrt(rp2) / (1.0 + std::sqrt(b2)), rdual = std::sqrt(rd2) / (1.0 + std::sqrt(c2));
+    const double gap = std::fabs(p - d) / (1.0 + std::fabs(p) + std::fabs(d));
+    const double rk = std::max({rprim, rdual, gap});
+    if (rk > options.tolerance) return false;
+    if (options.tolerance >= 1e-6) return true;
+    return pmax <= 1e-6 && dmax / (1.0 + cinf) <= 1e-6 && gap <= 1e-6;
+  };
+  if (post.status == Status::Optimal && !passes(post)) {  // solve.cpp:414-450
+    Options tight = inner;
+    tight.tolerance = std::max(options.tolerance * 1e-2, 1e-13);
+    tight.warm_x = red.x;
+    tight.warm_y = red.y;
+    const Solution red2 = solve_direct(pr.reduced, budget(tight, red.iterations));
+    Solution post2 = postsolve(model, pr, red2);
+    post2.iterations += red.iterations;
+    if (post2.status == Status::Optimal && passes(post2)) {
+      char buf[64];
+      std::snprintf(buf, sizeof buf, "%.0e", tight.tolerance);
+      post2.message = pnote + "; reduced model re-solved to " + buf + " to pass on the original";
+      post = post2;
+    } else {
+      Solution cold = solve_direct(model, budget(inner, red.iterations + red2.iterations));
+      cold.iterations += red.iterations + red2.iterations;
+      note(cold, pnote + "; postsolved point missed the tolerance, fell back to solving the original");
+      post = cold;
+    }
+  } else if (post.status == Status::Optimal && static_cast<int>(post.x.size()) != model.num_cols) {
+    post.status = Status::NumericalError;
+  }
+  post.presolve_seconds = presolve_s;
+  post.seconds = since(t0);
+  return post;
+}
+
+// The verification gate (solve.cpp:119-185, LP part).
+void gate(const Model& model, const Options& options, Solution& s) {
+  if (s.status == Status::Infeasible || s.status == Status::Unbounded) {
+    s.objective = s.dual_objective = kNaN;
+    if (s.status == Status::Infeasible && !model.crossed_bounds().empty()) {
+      s.check = "PASS";
+      return;
+    }
+    s.check.clear();
+    note(s, "not certified (certificate verification is not part of this library)");
+    return;
+  }
+  if (s.status != Status::Optimal) return;
+  if (static_cast<int>(s.x.size()) != model.num_cols || static_cast<int>(s.y.size()) != model.num_rows) {
+    s.status = Status::NumericalError;
+    note(s, "engine reported Optimal without primal and dual vectors");
+    return;
+  }
+  const CheckReport rep = check_solution(model, s.x, s.y);
+  s.check = rep.passed() ? "PASS" : "FAIL";
+  s.check_primal = rep.max_primal_violation;
+  s.check_dual = rep.max_dual_violation;
+  s.check_gap = rep.relative_gap;
+  if (std::isnan(s.dual_objective)) s.dual_objective = rep.dual_objective;
+  if (rep.passed()) return;
+  const bool claims_verifier_grade = options.tolerance < 1e-6;
+  const std::string what = "in-process check on the original model: " + rep.summary();
+  if (claims_verifier_grade) {
+    s.status = Status::NumericalError;
+    note(s, "Optimal withdrawn, " + what);
+  } else {
+    note(s, what + " (requested tolerance is looser than the verifier's)");
+  }
+}
+
+Solution solve_unguarded(const Model& model, const Options& options) {  // solve.cpp:213-259
+  Options resolved = options;
+  std::string prefix;
+  if (options.algorithm == Algorithm::Auto) {
+    const double work = static_cast<double>(std::max(model.num_rows, 1)) * static_cast<double>(model.nnz());
+    bool first_order_request = options.use_gpu || !options.warm_x.empty() || !options.warm_y.empty() ||
+                               options.warm_primal_weight > 0;
+    resolved.algorithm = !first_order_request && work <= 2e8 ? Algorithm::Simplex : Algorithm::R2hpdhg;
+    char buf[96];
+    std::snprintf(buf, sizeof buf, "auto: %s (rows*nnz = %.2g)", alg_name(resolved.algorithm), work);
+    prefix = buf;
+  }
+  Solution s;
+  if (resolved.algorithm != Algorithm::R2hpdhg) {
+    s.status = Status::NotSolved;
+    s.engine = alg_name(resolved.algorithm);
+    s.message = std::string("algorithm '") + alg_name(resolved.algorithm) +
+                "' is not provided by this library: it runs r2hpdhg on the GPU (use_gpu = 1)";
+  } else if (!options.use_gpu) {
+    s.status = Status::NotSolved;
+    s.message = "this library runs r2hpdhg on the GPU only: set use_gpu = 1 (there is no CPU fallback)";
+  } else {
+    bool device = true;
+    try {
+      require_device();
+    } catch (const std::runtime_error& e) {  // cpu_backend.cpp:300-305
+      device = false;
+      s.status = Status::NotSolved;
+      s.message = std::string("CUDA backend unavailable: ") + e.what();
+    }
+    if (device) {
+      s = solve_impl(model, resolved);
+      gate(model, resolved, s);
+    }
+  }
+  if (!prefix.empty()) s.message = s.message.empty() ? prefix : prefix + "; " + s.message;
+  return s;
+}
+
+}  // namespace
+
+Solution solve(const Model& model, const Options& options) {  // solve.cpp:194-210
+  try {
+    return solve_unguarded(model, options);
+  } catch (const std::bad_alloc&) {
+    Solution s;
+    s.status = Status::NotSolved;
+    s.message = "out of memory";
+    return s;
+  } catch (const std::exception& e) {
+    Solution s;
+    s.status = Status::NumericalError;
+    s.message = std::string("internal error: ") + e.what();
+    return s;
+  }
+}
+
+}  // namespace b200

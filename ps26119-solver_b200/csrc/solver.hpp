@@ -1,0 +1,107 @@
+// solver.hpp — host-side model, options, solution and the solve() dispatcher around the
+// GPU engine. Mirrors the reference's contracts:
+//   Model     include/ps26119/model.h:18-70      (CSC, validate, fingerprint, row_activity)
+//   Options   include/ps26119/options.h:37-82    (the fields this library honours)
+//   Solution  include/ps26119/solution.h:21-86
+//   solve()   src/core/solve.cpp:194-609          (presolve wrapper, direct solve, gate)
+//   presolve  src/core/presolve.{h,cpp}            (R1-R4 + primal/dual postsolve)
+//   checker   src/core/solution_checker.{h,cpp}
+#pragma once
+
+#include <cstdint>
+#include <limits>
+#include <string>
+#include <vector>
+
+#include "engine.hpp"
+
+namespace b200 {
+
+constexpr double kInf = std::numeric_limits<double>::infinity();
+constexpr double kNaN = std::numeric_limits<double>::quiet_NaN();
+
+struct Model {
+  int num_rows = 0, num_cols = 0, sense = 1;
+  double obj_offset = 0.0;
+  std::vector<double> obj, col_lower, col_upper, row_lower, row_upper;
+  std::vector<int> col_start, row_index;
+  std::vector<double> value;
+
+  std::size_t nnz() const { return value.size(); }
+  std::string validate() const;        // model.cpp:93-160
+  std::string crossed_bounds() const;  // model.cpp:162-167
+  double objective_value(const std::vector<double>& x) const;
+  std::vector<double> row_activity(const std::vector<double>& x) const;
+  std::uint64_t fingerprint() const;   // model.cpp:53-85 (FNV-1a)
+  HostModelView view() const;
+};
+
+enum class Algorithm { Auto, Oracle, Pdlp, R2hpdhg, Simplex };
+enum class Precision { Fp64, Mixed };
+
+struct Options {
+  Algorithm algorithm = Algorithm::Auto;
+  Precision precision = Precision::Fp64;
+  bool use_gpu = false;
+  double tolerance = 1e-8;
+  double time_limit = 3600.0;
+  long long iteration_limit = 100000000LL;
+  int verbosity = 0;
+  int threads = 1;
+  bool presolve = true;
+  int check_every = 64;
+  bool exact = false;
+  ScalingOptions scaling;
+  double reflection = 1.0;
+  std::vector<double> warm_x, warm_y;
+  double warm_primal_weight = 0.0;
+  double kkt_b_norm = -1, kkt_c_norm = -1, kkt_obj_shift = 0;
+};
+
+struct Solution {
+  Status status = Status::NotSolved;
+  std::vector<double> x, y, z, dual_ray, primal_ray;
+  double objective = kNaN, dual_objective = kNaN, primal_residual = kNaN, dual_residual = kNaN, gap = kNaN;
+  long long iterations = 0;
+  double seconds = 0, setup_seconds = 0;
+  double certified_bound = kNaN;
+  double primal_weight = kNaN;
+  std::string check;  // "PASS" / "FAIL" / "" (not applicable / not certified)
+  double check_primal = kNaN, check_dual = kNaN, check_gap = kNaN;
+  std::string engine = "r2hpdhg-b200", precision = "fp64", message;
+  EngineResult engine_result;  // statistics of the last engine run
+  double presolve_seconds = 0;
+};
+
+// The in-process optimality check (solution_checker.cpp:61-133).
+struct CheckReport {
+  double max_primal_violation = 0, max_dual_violation = 0, max_complementarity = 0;
+  double primal_objective = 0, dual_objective = 0, relative_gap = 0;
+  bool primal_ok = false, dual_ok = false, gap_ok = false;
+  bool passed() const { return primal_ok && dual_ok && gap_ok; }
+  std::string summary() const;
+};
+CheckReport check_solution(const Model& lp, const std::vector<double>& x, const std::vector<double>& row_dual);
+
+// Presolve R1-R4 with postsolve (presolve.h:22-65).
+struct PresolveResult {
+  enum class Outcome { Reduced, Infeasible, Unchanged } outcome = Outcome::Unchanged;
+  Model reduced;
+  std::string message;
+  int removed_rows = 0, removed_cols = 0, tightened_bounds = 0;
+  std::vector<int> row_map, col_map;
+  std::vector<double> fixed_value;
+  struct Singleton {
+    int row, col;
+    double a;
+    bool set_lower, set_upper;
+  };
+  std::vector<Singleton> singletons;
+};
+PresolveResult presolve(const Model& model);
+Solution postsolve(const Model& original, const PresolveResult& r, const Solution& reduced);
+
+// The library entry point: never throws (solve.cpp:194-210).
+Solution solve(const Model& model, const Options& options);
+
+}  // namespace b200
