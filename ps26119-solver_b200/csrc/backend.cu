@@ -111,12 +111,12 @@ class GpuBackendImpl final : public GpuBackend {
     B200_LAUNCH_CHECK();
   }
   void spmv(int x, int out) override {
-    if (mixed_) launch_slab<float>(m_, sp_.a_rp.get(), sp_.a_col.get(), sp_.saf.get(), f_[x].get(), EpiStore<float>{{}, f_[out].get()}, st_);
-    else launch_slab<double>(m_, sp_.a_rp.get(), sp_.a_col.get(), sp_.sa.get(), d_[x].get(), EpiStore<double>{{}, d_[out].get()}, st_);
+    if (mixed_) launch_slab_tma<float>(m_, sp_.a_rp.get(), sp_.a_col.get(), sp_.saf.get(), f_[x].get(), EpiStore<float>{{}, f_[out].get()}, st_);
+    else launch_slab_tma<double>(m_, sp_.a_rp.get(), sp_.a_col.get(), sp_.sa.get(), d_[x].get(), EpiStore<double>{{}, d_[out].get()}, st_);
   }
   void spmv_t(int y, int out) override {
-    if (mixed_) launch_slab<float>(n_, cs_.get(), sp_.t_ri.get(), sp_.satf.get(), f_[y].get(), EpiStore<float>{{}, f_[out].get()}, st_);
-    else launch_slab<double>(n_, cs_.get(), sp_.t_ri.get(), sp_.sat.get(), d_[y].get(), EpiStore<double>{{}, d_[out].get()}, st_);
+    if (mixed_) launch_slab_tma<float>(n_, cs_.get(), sp_.t_ri.get(), sp_.satf.get(), f_[y].get(), EpiStore<float>{{}, f_[out].get()}, st_);
+    else launch_slab_tma<double>(n_, cs_.get(), sp_.t_ri.get(), sp_.sat.get(), d_[y].get(), EpiStore<double>{{}, d_[out].get()}, st_);
   }
   double dot(int a, int b) override { return pair_sum(a, b, false); }
   double norm2(int a) override { return std::sqrt(pair_sum(a, a, false)); }
@@ -154,12 +154,12 @@ class GpuBackendImpl final : public GpuBackend {
     B200_LAUNCH_CHECK();
   }
   void fused_primal(int y, int x, int x0, double tau, double w, double rho, int xh, int xb) override {
-    if (mixed_) launch_slab<float>(n_, cs_.get(), sp_.t_ri.get(), sp_.satf.get(), f_[y].get(), epi_primal<float>(x, x0, tau, w, rho, xh, xb), st_);
-    else launch_slab<double>(n_, cs_.get(), sp_.t_ri.get(), sp_.sat.get(), d_[y].get(), epi_primal<double>(x, x0, tau, w, rho, xh, xb), st_);
+    if (mixed_) launch_slab_tma<float>(n_, cs_.get(), sp_.t_ri.get(), sp_.satf.get(), f_[y].get(), epi_primal<float>(x, x0, tau, w, rho, xh, xb), st_);
+    else launch_slab_tma<double>(n_, cs_.get(), sp_.t_ri.get(), sp_.sat.get(), d_[y].get(), epi_primal<double>(x, x0, tau, w, rho, xh, xb), st_);
   }
   void fused_dual(int xb, int y, int y0, double sigma, double w, double rho, int yh, int yb) override {
-    if (mixed_) launch_slab<float>(m_, sp_.a_rp.get(), sp_.a_col.get(), sp_.saf.get(), f_[xb].get(), epi_dual<float>(y, y0, sigma, w, rho, yh, yb), st_);
-    else launch_slab<double>(m_, sp_.a_rp.get(), sp_.a_col.get(), sp_.sa.get(), d_[xb].get(), epi_dual<double>(y, y0, sigma, w, rho, yh, yb), st_);
+    if (mixed_) launch_slab_tma<float>(m_, sp_.a_rp.get(), sp_.a_col.get(), sp_.saf.get(), f_[xb].get(), epi_dual<float>(y, y0, sigma, w, rho, yh, yb), st_);
+    else launch_slab_tma<double>(m_, sp_.a_rp.get(), sp_.a_col.get(), sp_.sa.get(), d_[xb].get(), epi_dual<double>(y, y0, sigma, w, rho, yh, yb), st_);
   }
 
   // Backend::kkt (cpu_backend.cpp:269-276 + 226-284) on the device.
@@ -177,7 +177,7 @@ class GpuBackendImpl final : public GpuBackend {
     B200_LAUNCH_CHECK();
     double* K0 = terms_.get();
     EpiKktRows er{{}, yo_.get(), M_.row_lower, M_.row_upper, K0, K0 + L, K0 + 2 * L, res_.get()};
-    launch_slab<double>(m_, sp_.a_rp.get(), sp_.a_col.get(), sp_.a_v0.get(), xo_.get(), er, st_);
+    launch_slab_tma<double>(m_, sp_.a_rp.get(), sp_.a_col.get(), sp_.a_v0.get(), xo_.get(), er, st_);
     EpiKktCols ec{{}, xo_.get(), M_.c, M_.col_lower, M_.col_upper, static_cast<double>(M_.sense), m_, K0 + 3 * L, K0 + L, K0 + 2 * L, res_.get()};
     launch_slab<double>(n_, M_.col_start, M_.row_index, M_.value, yo_.get(), ec, st_);
     SumPlan p;

@@ -98,22 +98,29 @@ struct EpiKktRows : AlwaysActive {
   const double *y, *rl, *ru;
   double *t_rp2, *t_d, *t_rd2;
   double* res;
-  __device__ void operator()(int i, double ax) const {
+  struct Acc {
+    double pmax = 0.0, dmax = 0.0;
+  };
+  __device__ void operator()(int i, double ax, Acc& acc) const {
     const double lo = rl[i], up = ru[i];
     const double viol = ax < lo ? lo - ax : (ax > up ? ax - up : 0.0);
     t_rp2[i] = viol * viol;
-    atomic_max_nonneg(max_slot(res, kMaxPmax), elem_viol(ax, lo, up));
+    acc.pmax = elem_viol(ax, lo, up);
     const double yi = y[i];
     double d = 0.0, rd = 0.0;
     if (yi > 0) {
       if (isfinite(lo)) d = yi * lo;
-      else rd = yi * yi, atomic_max_nonneg(max_slot(res, kMaxDmax), yi);
+      else rd = yi * yi, acc.dmax = yi;
     } else if (yi < 0) {
       if (isfinite(up)) d = yi * up;
-      else rd = yi * yi, atomic_max_nonneg(max_slot(res, kMaxDmax), -yi);
+      else rd = yi * yi, acc.dmax = -yi;
     }
     t_d[i] = d;
     t_rd2[i] = rd;
+  }
+  __device__ void flush(const Acc& a) const {
+    warp_max_atomic(max_slot(res, kMaxPmax), a.pmax);
+    warp_max_atomic(max_slot(res, kMaxDmax), a.dmax);
   }
 };
 // Column part after aty = Aᵀ_orig·y (the caller's CSC order).
@@ -123,11 +130,14 @@ struct EpiKktCols : AlwaysActive {
   int m;
   double *t_p, *t_d, *t_rd2;
   double* res;
-  __device__ void operator()(int j, double aty) const {
+  struct Acc {
+    double pmax = 0.0, dmax = 0.0;
+  };
+  __device__ void operator()(int j, double aty, Acc& acc) const {
     const double cj = sense * c[j];
     t_p[m + j] = cj * x[j];
     const double lo = cl[j], up = cu[j];
-    atomic_max_nonneg(max_slot(res, kMaxPmax), elem_viol(x[j], lo, up));
+    acc.pmax = elem_viol(x[j], lo, up);
     const double lam = cj - aty;
     double z;
     if (isfinite(lo) && isfinite(up)) z = lam;
@@ -135,8 +145,12 @@ struct EpiKktCols : AlwaysActive {
     else if (isfinite(up)) z = std_min(lam, 0.0);
     else z = 0.0;
     t_rd2[m + j] = (lam - z) * (lam - z);
-    atomic_max_nonneg(max_slot(res, kMaxDmax), fabs(lam - z));
+    acc.dmax = fabs(lam - z);
     t_d[m + j] = z > 0 ? z * lo : (z < 0 ? z * up : 0.0);
+  }
+  __device__ void flush(const Acc& a) const {
+    warp_max_atomic(max_slot(res, kMaxPmax), a.pmax);
+    warp_max_atomic(max_slot(res, kMaxDmax), a.dmax);
   }
 };
 
@@ -145,30 +159,35 @@ struct EpiKktCols : AlwaysActive {
 template <class T>
 static __global__ void k_ray_r(int m, const T* dy, const double* row_scale, double obj_scale, const double* rl,
                         const double* ru, double* r, double* res, int slot_rmax) {
+  double mx = 0.0;
   B200_FOR(i, m) {
     double v = row_scale[i] * static_cast<double>(dy[i]) / obj_scale;
     if (!isfinite(rl[i])) v = std_min(v, 0.0);
     if (!isfinite(ru[i])) v = std_max(v, 0.0);
     r[i] = v;
-    atomic_max_nonneg(max_slot(res, slot_rmax), fabs(v));
+    mx = std_max(mx, fabs(v));
   }
+  warp_max_atomic(max_slot(res, slot_rmax), mx);
 }
 template <class T>
 static __global__ void k_ray_d(int n, const T* dx, const double* col_scale, double bound_scale, const double* cl,
                         const double* cu, double* d, double* res, int slot_dabs) {
+  double mx = 0.0;
   B200_FOR(j, n) {
     double v = col_scale[j] * static_cast<double>(dx[j]) / bound_scale;
     if (isfinite(cl[j])) v = std_max(v, 0.0);
     if (isfinite(cu[j])) v = std_min(v, 0.0);
     d[j] = v;
-    atomic_max_nonneg(max_slot(res, slot_dabs), fabs(v));
+    mx = std_max(mx, fabs(v));
   }
+  warp_max_atomic(max_slot(res, slot_dabs), mx);
 }
 // Columns: g = Aᵀr and gabs = Σ|a r| (CSC order), λ = −g; objective/magnitude terms and the
 // dual-ray violation; plus the primal-ray terms cᵀd and Σ|c d| (engine.cpp:97-116, 138-139).
 static __global__ void k_ray_cols(int n, int m, const int* cp, const int* ri, const double* v, const double* r,
                            const double* d, const double* c, double sense, const double* cl, const double* cu,
                            double* t_obj, double* t_mag, double* t_cd, double* t_cmag, double* res, int slot_dviol) {
+  double dviol = 0.0;
   B200_FOR(j, n) {
     double g = 0.0, gabs = 0.0;
     for (int k = cp[j]; k < cp[j + 1]; ++k) {
@@ -179,16 +198,17 @@ static __global__ void k_ray_cols(int n, int m, const int* cp, const int* ri, co
     double ob = 0.0, mg = 0.0;
     if (lam > 0) {
       if (isfinite(lo)) ob = lo * lam, mg = gabs * fabs(lo);
-      else atomic_max_nonneg(max_slot(res, slot_dviol), lam);
+      else dviol = std_max(dviol, lam);
     } else if (lam < 0) {
       if (isfinite(up)) ob = up * lam, mg = gabs * fabs(up);
-      else atomic_max_nonneg(max_slot(res, slot_dviol), -lam);
+      else dviol = std_max(dviol, -lam);
     }
     t_obj[m + j] = ob;
     t_mag[m + j] = mg;
     t_cd[j] = sense * c[j] * d[j];
     t_cmag[j] = fabs(c[j] * d[j]);
   }
+  warp_max_atomic(max_slot(res, slot_dviol), dviol);
 }
 // Rows after ad = A_orig·d: primal-ray violation; dual-ray objective/magnitude row terms.
 struct EpiRayRows : AlwaysActive {
@@ -196,14 +216,20 @@ struct EpiRayRows : AlwaysActive {
   double *t_obj, *t_mag;
   double* res;
   int slot_pviol;
-  __device__ void operator()(int i, double ad) const {
-    if (isfinite(rl[i])) atomic_max_nonneg(max_slot(res, slot_pviol), -ad);
-    if (isfinite(ru[i])) atomic_max_nonneg(max_slot(res, slot_pviol), ad);
+  struct Acc {
+    double pviol = 0.0;
+  };
+  __device__ void operator()(int i, double ad, Acc& acc) const {
+    double v = 0.0;
+    if (isfinite(rl[i])) v = std_max(v, -ad);
+    if (isfinite(ru[i])) v = std_max(v, ad);
+    acc.pviol = v;
     const double ri = r[i];
     const double term = ri > 0 ? rl[i] * ri : (ri < 0 ? ru[i] * ri : 0.0);
     t_obj[i] = term;
     t_mag[i] = fabs(term);
   }
+  __device__ void flush(const Acc& a) const { warp_max_atomic(max_slot(res, slot_pviol), a.pviol); }
 };
 
 // ---------------------------------------------------------------------- finish
@@ -245,12 +271,19 @@ struct EpiCheckRows : AlwaysActive {  // after ax = A·x; y = min-form duals (se
   double c_scale;
   double* t_dual;  // [0, m) rows, [m, m+n) cols
   double* res;
-  __device__ void operator()(int i, double ax) const {
-    atomic_max_nonneg(max_slot(res, kMaxChkPrimal), bound_violation(ax, rl[i], ru[i]));
+  struct Acc {
+    double primal = 0.0, dual = 0.0;
+  };
+  __device__ void operator()(int i, double ax, Acc& acc) const {
+    acc.primal = bound_violation(ax, rl[i], ru[i]);
     double viol, contrib;
     multiplier(y[i], rl[i], ru[i], viol, contrib);
-    atomic_max_nonneg(max_slot(res, kMaxChkDual), viol / c_scale);
+    acc.dual = viol / c_scale;
     t_dual[i] = contrib;
+  }
+  __device__ void flush(const Acc& a) const {
+    warp_max_atomic(max_slot(res, kMaxChkPrimal), a.primal);
+    warp_max_atomic(max_slot(res, kMaxChkDual), a.dual);
   }
 };
 struct EpiCheckCols : AlwaysActive {  // after aty = Aᵀ·y_min (CSC order)
@@ -259,15 +292,22 @@ struct EpiCheckCols : AlwaysActive {  // after aty = Aᵀ·y_min (CSC order)
   int m;
   double *t_dual, *t_primal;
   double* res;
-  __device__ void operator()(int j, double aty) const {
-    atomic_max_nonneg(max_slot(res, kMaxChkPrimal), bound_violation(x[j], cl[j], cu[j]));
+  struct Acc {
+    double primal = 0.0, dual = 0.0;
+  };
+  __device__ void operator()(int j, double aty, Acc& acc) const {
+    acc.primal = bound_violation(x[j], cl[j], cu[j]);
     const double cj = sense * c[j];
     const double d = cj - aty;
     double viol, contrib;
     multiplier(d, cl[j], cu[j], viol, contrib);
-    atomic_max_nonneg(max_slot(res, kMaxChkDual), viol / c_scale);
+    acc.dual = viol / c_scale;
     t_dual[m + j] = contrib;
     t_primal[j] = cj * x[j];
+  }
+  __device__ void flush(const Acc& a) const {
+    warp_max_atomic(max_slot(res, kMaxChkPrimal), a.primal);
+    warp_max_atomic(max_slot(res, kMaxChkDual), a.dual);
   }
 };
 static __global__ void k_scale_copy(long long n, const double* src, double s, double* dst) {

@@ -57,11 +57,12 @@ class DevBuf {
   }
   ~DevBuf() { release(); }
 
-  // Allocates n elements plus 16 bytes of tail padding (vector loads may read up to one
-  // 16-byte word past the last element; the padding keeps that inside the allocation).
+  // Allocates n elements plus 64 bytes of tail padding: 16-byte-aligned bulk copies of a
+  // range [a, b) are widened to 16-byte boundaries and may read up to 15 bytes past the last
+  // element; the padding keeps that inside the allocation.
   void alloc(std::size_t n) {
     release();
-    const std::size_t bytes = n * sizeof(T) + 16;
+    const std::size_t bytes = n * sizeof(T) + 64;
     void* p = nullptr;
     B200_CHECK(cudaMalloc(&p, bytes));
     p_ = static_cast<T*>(p);
@@ -148,6 +149,26 @@ __device__ __forceinline__ void atomic_max_nonneg(unsigned long long* slot, doub
 }
 __device__ __forceinline__ void atomic_min_pos(unsigned long long* slot, double v) {
   if (v > 0.0) atomicMin(slot, nonneg_key(v));
+}
+
+// Maximum of a non-negative candidate over the whole warp (all 32 lanes must call it), then one
+// atomic per warp: order-independent like atomic_max_nonneg, without the contention of one
+// atomic per element on a single address.
+__device__ __forceinline__ void warp_max_atomic(unsigned long long* slot, double v) {
+  unsigned long long key = (v > 0.0) ? nonneg_key(v) : 0ULL;  // NaN and -0.0 never win
+  for (int off = 16; off > 0; off >>= 1) {
+    const unsigned long long o = __shfl_xor_sync(kFull, key, off);
+    key = o > key ? o : key;
+  }
+  if ((threadIdx.x & 31) == 0 && key != 0ULL) atomicMax(slot, key);
+}
+__device__ __forceinline__ void warp_min_atomic_pos(unsigned long long* slot, double v) {
+  unsigned long long key = (v > 0.0) ? nonneg_key(v) : ~0ULL;
+  for (int off = 16; off > 0; off >>= 1) {
+    const unsigned long long o = __shfl_xor_sync(kFull, key, off);
+    key = o < key ? o : key;
+  }
+  if ((threadIdx.x & 31) == 0 && key != ~0ULL) atomicMin(slot, key);
 }
 
 }  // namespace b200

@@ -264,7 +264,7 @@ void Engine::launch_residual(bool with_restart_terms, const int* skip, SumPlan& 
   B200_LAUNCH_CHECK();
   EpiResY<T> e{v.yb.get(), v.yh.get(), v.y0.get(), v.dy.get(), v.adx.get(), py, cross,
                with_restart_terms ? dyn : nullptr, skip};
-  launch_slab<T>(m, sp_.a_rp.get(), sp_.a_col.get(), sp_.A_val<T>(), v.dx.get(), e, st_);
+  launch_slab_tma<T>(m, sp_.a_rp.get(), sp_.a_col.get(), sp_.A_val<T>(), v.dx.get(), e, st_);
   plan.launch(st_);
   B200_COUNT(2 + plan.kernel_count());
 }
@@ -274,7 +274,7 @@ void Engine::launch_kkt_original() {
   const long long L = static_cast<long long>(m) + n;
   double* K0 = kt_.get();
   EpiKktRows er{{}, yo_.get(), M_.row_lower, M_.row_upper, K0, K0 + L, K0 + 2 * L, res_.get()};
-  launch_slab<double>(m, sp_.a_rp.get(), sp_.a_col.get(), sp_.a_v0.get(), xo_.get(), er, st_);
+  launch_slab_tma<double>(m, sp_.a_rp.get(), sp_.a_col.get(), sp_.a_v0.get(), xo_.get(), er, st_);
   EpiKktCols ec{{}, xo_.get(), M_.c, M_.col_lower, M_.col_upper, static_cast<double>(M_.sense), m,
                 K0 + 3 * L, K0 + L, K0 + 2 * L, res_.get()};
   launch_slab<double>(n, M_.col_start, M_.row_index, M_.value, yo_.get(), ec, st_);
@@ -309,7 +309,7 @@ void Engine::launch_ray(const T* dx, const T* dy, double* r, double* d, int drif
                                               T0 + L, T0 + 2 * L, T0 + 2 * L + n, res_.get(), s_dviol);
   B200_LAUNCH_CHECK();
   EpiRayRows er{{}, r, M_.row_lower, M_.row_upper, T0, T0 + L, res_.get(), s_pviol};
-  launch_slab<double>(m, sp_.a_rp.get(), sp_.a_col.get(), sp_.a_v0.get(), d, er, st_);
+  launch_slab_tma<double>(m, sp_.a_rp.get(), sp_.a_col.get(), sp_.a_v0.get(), d, er, st_);
   SumPlan& p = drift ? plan_ray2_ : plan_ray1_;
   p.launch(st_);
   B200_COUNT(4 + p.kernel_count());
@@ -324,14 +324,17 @@ void Engine::capture_epoch() {
   const StepParams* P = params_.get();
   const int* r0_skip = skip_r0_flag(P);
   cudaGraph_t g;
+  slab_prepare<T, EpiPrimal<T>, B200_STAGE_TMA != 0>();
+  slab_prepare<T, EpiDual<T>, B200_STAGE_TMA != 0>();
+  slab_prepare<T, EpiResY<T>, B200_STAGE_TMA != 0>();
   capturing_ = true;
   capture_count_ = 0;
   B200_CHECK(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
   auto step = [&](int s) {
     EpiPrimal<T> ep{v.x.get(), v.xh.get(), v.xb.get(), v.x0.get(), sp_.c<T>(), sp_.l<T>(), sp_.u<T>(), P, s, 0, 0, 0};
-    launch_slab<T>(n, M_.col_start, sp_.t_ri.get(), sp_.At_val<T>(), v.y.get(), ep, st_);
+    launch_slab_tma<T>(n, M_.col_start, sp_.t_ri.get(), sp_.At_val<T>(), v.y.get(), ep, st_);
     EpiDual<T> ed{v.y.get(), v.yh.get(), v.yb.get(), v.y0.get(), sp_.rl<T>(), sp_.ru<T>(), P, s, 0, 0, 0, 0};
-    launch_slab<T>(m, sp_.a_rp.get(), sp_.a_col.get(), sp_.A_val<T>(), v.xb.get(), ed, st_);
+    launch_slab_tma<T>(m, sp_.a_rp.get(), sp_.a_col.get(), sp_.A_val<T>(), v.xb.get(), ed, st_);
     capture_count_ += 2;
   };
   B200_CHECK(cudaEventRecordWithFlags(ev_[0], st_, cudaEventRecordExternal));
@@ -355,6 +358,10 @@ void Engine::capture_check(int variant) {
   if (g_check_[idx][variant]) return;
   IterVecs<T>& v = vecs<T>();
   cudaGraph_t g;
+  slab_prepare<T, EpiResY<T>, B200_STAGE_TMA != 0>();
+  slab_prepare<double, EpiKktRows, B200_STAGE_TMA != 0>();
+  slab_prepare<double, EpiKktCols, false>();
+  slab_prepare<double, EpiRayRows, B200_STAGE_TMA != 0>();
   capturing_ = true;
   capture_count_ = 0;
   B200_CHECK(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
@@ -533,7 +540,7 @@ void Engine::finish_t(EngineResult& R, Status status, bool use_hat, long long it
   // in-process check (solution_checker.cpp:61-133) on xo and y_min = yo
   double c_scale = std_max(1.0, sp_.c_inf);
   EpiCheckRows cr{{}, yo_.get(), M_.row_lower, M_.row_upper, c_scale, objt_.get() + n, res_.get()};
-  launch_slab<double>(m, sp_.a_rp.get(), sp_.a_col.get(), sp_.a_v0.get(), xo_.get(), cr, st_);
+  launch_slab_tma<double>(m, sp_.a_rp.get(), sp_.a_col.get(), sp_.a_v0.get(), xo_.get(), cr, st_);
   // t_primal lands in objt_[0, n): the objective terms were consumed by plan_obj_ above
   EpiCheckCols cc{{}, xo_.get(), M_.c, M_.col_lower, M_.col_upper, static_cast<double>(M_.sense), c_scale, m,
                   objt_.get() + n, objt_.get(), res_.get()};
@@ -802,8 +809,11 @@ EngineResult run_engine(const DeviceModel& M, const EngineOptions& opt, const De
       if (own) cudaStreamDestroy(s);
     }
   } guard{st, own};
+  const unsigned timeouts = stage_timeouts();
   Engine e(M, opt, st);
-  return e.run(out);
+  EngineResult R = e.run(out);
+  if (stage_timeouts() != timeouts) throw CudaError("a shared-memory staging wait timed out on the device");
+  return R;
 }
 
 EngineResult run_engine_host(const HostModelView& H, const EngineOptions& opt, HostOutputs& out) {

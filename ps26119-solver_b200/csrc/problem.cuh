@@ -26,7 +26,9 @@ static __global__ void k_fill_d(long long n, double* v, double a) {
   B200_FOR(i, n) v[i] = a;
 }
 static __global__ void k_absmax(long long n, const double* v, unsigned long long* key) {
-  B200_FOR(i, n) atomic_max_nonneg(key, fabs(v[i]));
+  double mx = 0.0;
+  B200_FOR(i, n) mx = std_max(mx, fabs(v[i]));
+  warp_max_atomic(key, mx);
 }
 static __global__ void k_prod_terms(int n, const double* a, const double* b, double* t) {
   B200_FOR(i, n) t[i] = a[i] * b[i];
@@ -242,8 +244,8 @@ struct ScaledDevice {
     double theta = 0, theta_old = -1;
     int stagnant = 0;
     for (int k = 0; k < K; ++k) {
-      launch_slab<double>(m, a_rp.get(), a_col.get(), sa.get(), v.get(), EpiStore<double>{{}, t.get()}, st);
-      launch_slab<double>(n, M.col_start, t_ri.get(), sat.get(), t.get(), EpiStore<double>{{}, w.get()}, st);
+      launch_slab_tma<double>(m, a_rp.get(), a_col.get(), sa.get(), v.get(), EpiStore<double>{{}, t.get()}, st);
+      launch_slab_tma<double>(n, M.col_start, t_ri.get(), sat.get(), t.get(), EpiStore<double>{{}, w.get()}, st);
       k_prod_terms<<<grid_for(n), kBlock, 0, st>>>(n, w.get(), v.get(), terms.get());
       B200_LAUNCH_CHECK();
       pal.launch(st);

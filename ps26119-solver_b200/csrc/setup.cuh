@@ -156,14 +156,15 @@ static __global__ void k_sort_long(const int* rp, const int* long_rows, const in
 }
 
 // ------------------------------------------------------------------ scaling kernels
-static __global__ void k_abs_range(long long nnz, const double* v, unsigned long long* amin_key, unsigned long long* amax_key) {
+static __global__ void k_abs_range(long long nnz, const double* v, unsigned long long* amin_key,
+                                   unsigned long long* amax_key) {
+  double lo = INFINITY, hi = 0.0;
   B200_FOR(k, nnz) {
     const double a = fabs(v[k]);
-    if (v[k] != 0.0) {
-      atomicMin(amin_key, nonneg_key(a));
-      atomicMax(amax_key, nonneg_key(a));
-    }
+    if (v[k] != 0.0) lo = std_min(lo, a), hi = std_max(hi, a);
   }
+  warp_min_atomic_pos(amin_key, lo == INFINITY ? 0.0 : lo);
+  warp_max_atomic(amax_key, hi);
 }
 
 __device__ __forceinline__ double clampf_gm(double v) { return std_min(std_max(v, 1e-20), 1e20); }

@@ -13,71 +13,233 @@
 // 4 bytes of row pointer per row and the epilogue's vectors; x gathers hit L2 when x fits.
 #pragma once
 
+#include <algorithm>
 #include <cstddef>
+#include <type_traits>
 
 #include "common.cuh"
 
 namespace b200 {
 
+// Build-time tuning knobs (defaults are the tuned values): CTAs per SM the register budget is
+// sized for, whether the engine's own CSR arrays are staged by TMA bulk copies, and the
+// shared-memory carveout preference (percent, or -1 to leave the driver default).
+#ifndef B200_SLAB_MIN_BLOCKS
+#define B200_SLAB_MIN_BLOCKS 4
+#endif
+#ifndef B200_STAGE_TMA
+#define B200_STAGE_TMA 1
+#endif
+#ifndef B200_SLAB_CARVEOUT
+#define B200_SLAB_CARVEOUT -1
+#endif
+
 constexpr int kSlabRows = 256;
-constexpr int kSlabTile = 2048;
+constexpr int kSlabTile = 2048;  // nonzeros staged per tile
+constexpr int kTilePad = 8;      // room for the 16-byte widening of a bulk copy
 
 template <class T>
 struct SlabSmem {
-  int rp[kSlabRows + 1];
-  int col[kSlabTile];
-  T val[kSlabTile];
+  alignas(16) int col[kSlabTile + kTilePad];
+  alignas(16) T val[kSlabTile + kTilePad];
+  alignas(8) unsigned long long bar;
 };
 
-// Row-sequential fp64 accumulation of `rows` CSR rows; calls epi(row, s) for each row.
-// epi.active() lets graph-replayed launches exit early (device-side flag).
-template <class T, class Epi>
-static __global__ void __launch_bounds__(kSlabRows, 6) k_slab(int rows, const int* __restrict__ rp,
-                                                     const int* __restrict__ col,
-                                                     const T* __restrict__ val,
-                                                     const T* __restrict__ x, Epi epi) {
+// Bulk-copy waits that ran out (a counter the host reads after a solve; never expected to move).
+static __device__ unsigned int g_stage_timeouts;
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+// One TMA bulk copy global -> this CTA's shared memory (no multicast); both addresses and the
+// size are multiples of 16 bytes.
+__device__ __forceinline__ void tma_load_1d(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Waits for phase `parity` of the barrier, at most ~2^22 try_wait rounds.
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
+  for (int it = 0; it < (1 << 22); ++it)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
+// Epilogues may prefetch their operands: `Pre load(int row)` is issued at kernel entry, before
+// the nonzeros are staged, so its latency overlaps the SpMV; `operator()(row, s, pre)` then
+// finishes the update. Epilogues that take maxima expose `Acc` (fields written by the
+// epilogue) and `flush(acc)`, called by every thread after the epilogue so that maxima are
+// combined per warp before one atomic (see warp_max_atomic).
+struct NoPre {};
+struct NoAcc {};
+template <class E>
+__device__ __forceinline__ auto epi_load(const E& e, int i, int) -> decltype(e.load(i)) {
+  return e.load(i);
+}
+template <class E>
+__device__ __forceinline__ NoPre epi_load(const E&, int, long) {
+  return NoPre{};
+}
+template <class E>
+__device__ __forceinline__ auto epi_acc(const E&, int) -> typename E::Acc {
+  return typename E::Acc{};
+}
+template <class E>
+__device__ __forceinline__ NoAcc epi_acc(const E&, long) {
+  return NoAcc{};
+}
+template <class E, class P, class A>
+__device__ __forceinline__ void epi_apply(const E& e, int i, double s, const P& p, A& acc) {
+  if constexpr (!std::is_same<A, NoAcc>::value) e(i, s, acc);
+  else if constexpr (std::is_same<P, NoPre>::value) e(i, s);
+  else e(i, s, p);
+}
+template <class E, class A>
+__device__ __forceinline__ void epi_flush(const E& e, const A& acc) {
+  if constexpr (!std::is_same<A, NoAcc>::value) e.flush(acc);
+}
+
+constexpr int kGatherBatch = 8;  // independent x-gathers issued per round trip
+
+// Row-sequential fp64 accumulation of `rows` CSR rows; calls the epilogue with (row, s).
+// kTma: the tiles of col/val are staged by TMA bulk copies (the arrays must be this library's
+// own allocations, whose 64-byte tail padding covers the 16-byte widening); otherwise by a
+// batched register copy (caller-owned arrays). epi.active() lets graph-replayed launches exit.
+template <class T, class Epi, bool kTma>
+__global__ void __launch_bounds__(kSlabRows, B200_SLAB_MIN_BLOCKS) k_slab(int rows, const int* __restrict__ rp,
+                                                        const int* __restrict__ col,
+                                                        const T* __restrict__ val,
+                                                        const T* __restrict__ x, Epi epi) {
   __shared__ SlabSmem<T> sm;
   if (!epi.active()) return;
   const int r0 = blockIdx.x * kSlabRows;
   const int nr = min(kSlabRows, rows - r0);
-  for (int i = threadIdx.x; i <= nr; i += blockDim.x) sm.rp[i] = rp[r0 + i];
-  __syncthreads();
-  const int k0 = sm.rp[0], k1 = sm.rp[nr];
   const bool mine = threadIdx.x < nr;
-  const int beg = mine ? sm.rp[threadIdx.x] : 0, end = mine ? sm.rp[threadIdx.x + 1] : 0;
+  const int row = r0 + static_cast<int>(threadIdx.x);
+  // independent loads first: the slab's nonzero range, this thread's row bounds, the epilogue
+  const int k0 = __ldg(rp + r0), k1 = __ldg(rp + r0 + nr);
+  const int beg = mine ? __ldg(rp + row) : 0, end = mine ? __ldg(rp + row + 1) : 0;
+  const auto pre = epi_load(epi, mine ? row : r0, 0);
+  auto acc = epi_acc(epi, 0);
+  if constexpr (kTma) {
+    if (threadIdx.x == 0) mbar_init(&sm.bar);
+    __syncthreads();
+  }
+  constexpr int kValAlign = 16 / static_cast<int>(sizeof(T));  // elements per 16 bytes
+  unsigned phase = 0;
   double s = 0.0;
+  bool staged = true;
   for (int t0 = k0; t0 < k1; t0 += kSlabTile) {
     const int t1 = min(t0 + kSlabTile, k1);
+    int c0 = t0, v0 = t0;  // first element held in sm.col / sm.val
     if (t0 != k0) __syncthreads();  // previous tile fully consumed
-    for (int k = t0 + threadIdx.x; k < t1; k += blockDim.x) {
-      sm.col[k - t0] = __ldg(col + k);
-      sm.val[k - t0] = __ldg(val + k);
+    if constexpr (kTma) {
+      c0 = t0 & ~3;
+      v0 = t0 & ~(kValAlign - 1);
+      const int c1 = (t1 + 3) & ~3, v1 = (t1 + kValAlign - 1) & ~(kValAlign - 1);
+      if (threadIdx.x == 0) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        const unsigned cb = static_cast<unsigned>(c1 - c0) * 4u, vb = static_cast<unsigned>(v1 - v0) * sizeof(T);
+        mbar_expect_tx(&sm.bar, cb + vb);
+        tma_load_1d(sm.col, col + c0, cb, &sm.bar);
+        tma_load_1d(sm.val, val + v0, vb, &sm.bar);
+      }
+      const bool ok = mbar_wait_bounded(&sm.bar, phase);
+      phase ^= 1u;
+      if (!__syncthreads_and(ok ? 1 : 0)) {  // never expected: record, drain, give up on the tile
+        if (threadIdx.x == 0) atomicAdd(&g_stage_timeouts, 1u);
+        mbar_wait_bounded(&sm.bar, phase ^ 1u);
+        staged = false;
+        break;
+      }
+    } else {
+      constexpr int kB = 4;
+      for (int base = t0 + static_cast<int>(threadIdx.x); base < t1; base += kB * kSlabRows) {
+        int cc[kB];
+        T vv[kB];
+#pragma unroll
+        for (int q = 0; q < kB; ++q) {
+          const int k = base + q * kSlabRows;
+          if (k < t1) cc[q] = __ldg(col + k), vv[q] = __ldg(val + k);
+        }
+#pragma unroll
+        for (int q = 0; q < kB; ++q) {
+          const int k = base + q * kSlabRows;
+          if (k < t1) sm.col[k - t0] = cc[q], sm.val[k - t0] = vv[q];
+        }
+      }
+      __syncthreads();
     }
-    __syncthreads();
-    const int a = max(beg, t0) - t0, b = min(end, t1) - t0;
-    int k = a;
-    for (; k + 4 <= b; k += 4) {
-      const double p0 = static_cast<double>(sm.val[k]) * static_cast<double>(x[sm.col[k]]);
-      const double p1 = static_cast<double>(sm.val[k + 1]) * static_cast<double>(x[sm.col[k + 1]]);
-      const double p2 = static_cast<double>(sm.val[k + 2]) * static_cast<double>(x[sm.col[k + 2]]);
-      const double p3 = static_cast<double>(sm.val[k + 3]) * static_cast<double>(x[sm.col[k + 3]]);
-      s += p0;
-      s += p1;
-      s += p2;
-      s += p3;
+    const int a = max(beg, t0), b = min(end, t1);
+    for (int k = a; k < b; k += kGatherBatch) {
+      double p[kGatherBatch];
+#pragma unroll
+      for (int q = 0; q < kGatherBatch; ++q)
+        p[q] = (k + q < b) ? static_cast<double>(sm.val[k + q - v0]) * static_cast<double>(x[sm.col[k + q - c0]])
+                           : 0.0;
+#pragma unroll
+      for (int q = 0; q < kGatherBatch; ++q)
+        if (k + q < b) s += p[q];  // in CSR order
     }
-    for (; k < b; ++k) s += static_cast<double>(sm.val[k]) * static_cast<double>(x[sm.col[k]]);
   }
-  if (mine) epi(r0 + threadIdx.x, s);
+  if (!staged) s = __longlong_as_double(0x7ff8000000000000LL);  // NaN: the check reports a numerical error
+  if (mine) epi_apply(epi, row, s, pre, acc);
+  epi_flush(epi, acc);
 }
 
-template <class T, class Epi>
+// Once per instantiation, outside any stream capture: prefer shared memory so that 8 CTAs of
+// 24.6 KB fit on an SM.
+template <class T, class Epi, bool kTma>
+inline void slab_prepare() {
+  static const bool done = [] {
+    if (B200_SLAB_CARVEOUT >= 0)
+      (void)cudaFuncSetAttribute(k_slab<T, Epi, kTma>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 B200_SLAB_CARVEOUT);
+    (void)cudaGetLastError();
+    return true;
+  }();
+  (void)done;
+}
+
+template <class T, class Epi, bool kTma = false>
 inline void launch_slab(int rows, const int* rp, const int* col, const T* val, const T* x, const Epi& epi,
                         cudaStream_t st) {
   if (rows <= 0) return;
+  slab_prepare<T, Epi, kTma>();
   const int grid = (rows + kSlabRows - 1) / kSlabRows;
-  k_slab<T, Epi><<<grid, kSlabRows, 0, st>>>(rows, rp, col, val, x, epi);
+  k_slab<T, Epi, kTma><<<grid, kSlabRows, 0, st>>>(rows, rp, col, val, x, epi);
   B200_LAUNCH_CHECK();
+}
+
+// The TMA-staged form, for CSR arrays allocated by this library (tail-padded DevBufs).
+template <class T, class Epi>
+inline void launch_slab_tma(int rows, const int* rp, const int* col, const T* val, const T* x, const Epi& epi,
+                            cudaStream_t st) {
+  launch_slab<T, Epi, B200_STAGE_TMA != 0>(rows, rp, col, val, x, epi, st);
+}
+
+// Number of bulk-copy waits that ran out since the library was loaded (host side).
+inline unsigned stage_timeouts() {
+  unsigned v = 0;
+  cudaMemcpyFromSymbol(&v, g_stage_timeouts, sizeof v);
+  return v;
 }
 
 // Element-wise form of an epilogue: epi(i, double(v[i])) — the unfused backend ops use the
@@ -133,18 +295,26 @@ struct EpiPrimal {
   const StepParams* P;  // non-null: engine path
   int step;
   double tau, w, rho;   // backend-op path
+  struct Pre {
+    T x, x0, c, l, u;
+  };
   __device__ bool active() const { return P == nullptr || !P->done; }
-  __device__ void operator()(int j, double s) const {
+  __device__ Pre load(int j) const { return Pre{x[j], x0[j], c[j], l[j], u[j]}; }
+  __device__ void operator()(int j, double s) const { (*this)(j, s, load(j)); }
+  __device__ void operator()(int j, double s, const Pre& p) const {
     double tau_d = tau, w_d = w, rho_d = rho;
     if (P) tau_d = P->tau, w_d = halpern_weight(P, step), rho_d = P->rho;
     const T aty = static_cast<T>(s);
     const T t = static_cast<T>(tau_d), tw = static_cast<T>(w_d);
     const T a = static_cast<T>(2 * rho_d), b = static_cast<T>(1 - 2 * rho_d);
-    const T xj = x[j];
-    const T h = ref_clamp<T>(xj - t * (c[j] - aty), l[j], u[j]);
-    xh[j] = h;
+    const T xj = p.x;
+    const T h = ref_clamp<T>(xj - t * (p.c - aty), p.l, p.u);
+    // x̂ is read only by the residual and the check that follow an epoch's first step (when it
+    // starts a Halpern cycle) and its last step; on the other steps it is not stored.
+    const bool store_hat = !P || step == P->K - 1 || P->inner0 + step == 0;
+    if (store_hat) xh[j] = h;
     xb[j] = static_cast<T>(2) * h - xj;
-    x[j] = tw * (a * h + b * xj) + (static_cast<T>(1) - tw) * x0[j];
+    x[j] = tw * (a * h + b * xj) + (static_cast<T>(1) - tw) * p.x0;
   }
 };
 
@@ -159,8 +329,13 @@ struct EpiDual {
   int step;
   double sigma, w, rho;
   int write_yb;  // backend-op path
+  struct Pre {
+    T y, y0, rl, ru;
+  };
   __device__ bool active() const { return P == nullptr || !P->done; }
-  __device__ void operator()(int i, double s) const {
+  __device__ Pre load(int i) const { return Pre{y[i], y0[i], rl[i], ru[i]}; }
+  __device__ void operator()(int i, double s) const { (*this)(i, s, load(i)); }
+  __device__ void operator()(int i, double s, const Pre& p) const {
     double sig_d = sigma, w_d = w, rho_d = rho;
     bool wb = write_yb != 0;
     if (P) {
@@ -170,12 +345,16 @@ struct EpiDual {
     const T ax = static_cast<T>(s);
     const T sg = static_cast<T>(sig_d), tw = static_cast<T>(w_d);
     const T a = static_cast<T>(2 * rho_d), b = static_cast<T>(1 - 2 * rho_d);
-    const T yi = y[i];
+    const T yi = p.y;
     const T v = ax - yi / sg;
-    const T h = yi - sg * ax + sg * ref_clamp<T>(v, rl[i], ru[i]);
-    yh[i] = h;
-    if (wb) yb[i] = static_cast<T>(2) * h - yi;
-    y[i] = tw * (a * h + b * yi) + (static_cast<T>(1) - tw) * y0[i];
+    const T h = yi - sg * ax + sg * ref_clamp<T>(v, p.rl, p.ru);
+    if (wb) {  // ŷ, ȳ are read only after the steps that feed a residual (as x̂ above)
+      yh[i] = h;
+      yb[i] = static_cast<T>(2) * h - yi;
+    } else if (!P) {
+      yh[i] = h;
+    }
+    y[i] = tw * (a * h + b * yi) + (static_cast<T>(1) - tw) * p.y0;
   }
 };
 
