@@ -1,23 +1,29 @@
-"""Benchmark: time to 1e-8 relative KKT of the B200 r²HPDHG engine on the 1M x 1.5M random LP.
+"""Benchmark of the B200 r²HPDHG engine on the 1M x 1.5M random LP (BASELINE config 2 shape).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload random1m|random10k|staircase8760] [--precision fp64|mixed]
+                    [--iterations L | --full]
 
-One STEP is one complete solve to 1e-8 (setup on the device: structure, scaling, ‖Ã‖₂; the
-r²HPDHG iterations; checks; finish) of the seeded synthetic LP. `value` is whole-job throughput
-in solves per second with the model already resident in HBM (ps26119_solve_lp_device), timed
-with CUDA events on the solve's stream, max over ranks. `e2e` is the same metric through the
-reference-facing C API (ps26119_solve_lp_ex, presolve on) from pinned host buffers, with the
-host-to-device copy of the model and the device-to-host copy of x, y, z in the timed region.
+One STEP is one cold solve of the seeded LP on the device: setup (structure, scaling, ‖Ã‖₂),
+L r²HPDHG iterations with their checks every 64 iterations, and the finish (unscaling, KKT,
+z = c − Aᵀy, in-process check). The full solve of this LP to 1e-8 takes 3,724,096 iterations
+(about nine minutes), so the default step caps the iterations at L = 6,400 and the metric is
+r²HPDHG iterations per second, whole job (time to 1e-8 = setup + iterations ÷ this rate).
+`--full` drops the cap: the step is a complete solve to 1e-8 KKT and the metric is solves/s
+(use it with --workload random10k: 249,088 iterations).
 
-With torchrun (N > 1) every rank solves its own replica of the workload: a single LP does not
-shard (no collective on the data path), so the scaling is weak.
+value: model resident in HBM before the timed region (ps26119_solve_lp_device), timed with CUDA
+events on the solve's stream, max over ranks. e2e: the same steps through the reference-facing
+C API (ps26119_solve_lp_ex, presolve and in-process check on) from pinned host buffers, the
+model's host-to-device copy and the x, y, z device-to-host copy inside the timed region.
+
+torchrun (N > 1): every rank solves its own replica (a single LP does not shard; no collective
+on the data path): weak scaling.
 
 --impl reference: the reference's own CPU engine (built from its sources into oracle/_ref) on
-the host cores, all threads, on the same workload. One step is a bounded sample (the setup plus
-a few hundred iterations, iteration-limited); the solve time is the sample's setup plus its
-per-iteration time multiplied by the iteration count the full solve needs (RANDOM1M_ITERATIONS
-below, the GPU engine's count; the engines agree to one check at every size compared).
+the host cores, all threads, through ps26119::solve with presolve (as its C API), on the same LP.
+A step is a bounded sample — setup plus a few hundred iterations — whose per-iteration time is
+applied to the same L iterations as the GPU arm (or the full iteration count with --full).
 """
 from __future__ import annotations
 
@@ -35,17 +41,16 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path[:0] = [os.path.join(ROOT, "ps26119-solver_b200"), os.path.join(ROOT, "oracle")]
 
 WORKLOADS = {
-    "random1m": {"desc": "random equality LP m=1,000,000 n=1,500,000, 6 nnz/row N(0,1), seed 1", "kind": "random",
-                 "m": 1_000_000},
-    "random10k": {"desc": "random equality LP m=10,000 n=15,000, 6 nnz/row N(0,1), seed 1", "kind": "random",
-                  "m": 10_000},
+    "random1m": {"desc": "random equality LP m=1,000,000 n=1,500,000 nnz=6,000,000 (6/row, N(0,1)), seed 1",
+                 "kind": "random", "m": 1_000_000, "full_iterations": 3_724_096},
+    "random10k": {"desc": "random equality LP m=10,000 n=15,000 nnz=60,000 (6/row, N(0,1)), seed 1",
+                  "kind": "random", "m": 10_000, "full_iterations": 249_088},
     "staircase8760": {"desc": "staircase planning LP T=8760 (429,240 x 525,600), seed 1", "kind": "staircase",
-                      "T": 8760},
+                      "T": 8760, "full_iterations": None},
 }
-# Iterations to 1e-8 of the GPU engine (fast mode, fp64) on each workload, used only to
-# extrapolate the reference's bounded CPU sample to a full solve. None = not measured yet
-# (the reference arm then reports per-iteration cost over the sample's own count).
-FULL_ITERATIONS = {"random1m": None, "random10k": 249088, "staircase8760": None}
+# DRAM bytes per iteration (both fused kernels) from the ncu capture summarised in
+# profiles/fused_spmv_random1m.md (fp64); None where not captured.
+NCU_TRAFFIC = {("random1m", "fp64"): None}
 
 
 def make_lp(name):
@@ -55,8 +60,8 @@ def make_lp(name):
 
 
 def bytes_per_iteration(m, n, nnz, s_v, s_w):
-    """Algorithmic bytes of one r²HPDHG iteration: Ã and Ãᵀ streamed once (values + int32
-    column indices), int32 row pointers, and the vectors 9n + 7m in the working precision."""
+    """Algorithmic bytes of one r²HPDHG iteration: Ã and Ãᵀ streamed once (values + int32 column
+    indices), int32 row pointers, and the vectors 9n + 7m in the working precision."""
     return 2 * nnz * (s_v + 4) + 4 * (m + n) + s_w * (9 * n + 7 * m)
 
 
@@ -77,8 +82,8 @@ class ClockSampler:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
                                           "-lms", "200", "-i", self.gpu], stdout=subprocess.PIPE,
                                          stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
         except OSError:
             self.proc = None
         return self
@@ -115,18 +120,18 @@ class ClockSampler:
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def dist_setup(n_gpus):
-    import torch
-    import torch.distributed as dist
+def dist_setup():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if world > 1:
-        if torch.cuda.is_available():
-            torch.cuda.set_device(local)
         import datetime
-        dist.init_process_group("nccl" if torch.cuda.is_available() else "gloo",
-                                timeout=datetime.timedelta(seconds=1800))
+        import torch
+        import torch.distributed as dist
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=900))
     return rank, world, local
 
 
@@ -135,7 +140,8 @@ def max_over_ranks(v, world):
         return v
     import torch
     import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda" if torch.cuda.is_available() else "cpu")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -144,6 +150,13 @@ def barrier(world):
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
+
+
+def metric_name(args):
+    w = args.workload
+    if args.full:
+        return f"time-to-1e-8 KKT on {w} ({args.precision}) as solves/s"
+    return f"r2HPDHG iterations/s on {w} ({args.precision}); time-to-1e-8 = setup + iterations / rate"
 
 
 def run_ours(args, rank, world, local):
@@ -162,13 +175,15 @@ def run_ours(args, rank, world, local):
     y = torch.empty(m, dtype=torch.float64, device=dev)
     z = torch.empty(n, dtype=torch.float64, device=dev)
     stream = torch.cuda.Stream(device=dev)
+    limit = 0 if args.full else args.iterations
     engine = {"presolve": False, "exact": False}
 
     def step():
-        with torch.cuda.stream(stream):
-            r = ps26119.solve_lp_device(m, n, lp.sense, lp.offset, ptrs, precision=args.precision, engine=engine,
-                                        out=(x.data_ptr(), y.data_ptr(), z.data_ptr()), stream=stream.cuda_stream)
-        if r.status != ps26119.OPTIMAL:
+        r = ps26119.solve_lp_device(m, n, lp.sense, lp.offset, ptrs, precision=args.precision,
+                                    iteration_limit=limit, engine=engine,
+                                    out=(x.data_ptr(), y.data_ptr(), z.data_ptr()), stream=stream.cuda_stream)
+        want = ps26119.OPTIMAL if args.full else (ps26119.OPTIMAL, ps26119.ITERATION_LIMIT)
+        if (r.status != want) if args.full else (r.status not in want):
             raise RuntimeError(f"solve ended {r.status_name}: {r.message}")
         return r, ps26119.last_stats()
 
@@ -185,87 +200,100 @@ def run_ours(args, rank, world, local):
             results.append(step())
         ev1.record(stream)
         torch.cuda.synchronize()
+    ms = max_over_ranks(ev0.elapsed_time(ev1), world)
     barrier(world)
-    ms = ev0.elapsed_time(ev1)
-    ms = max_over_ranks(ms, world)
     r, st = results[-1]
-    s_v = 4 if args.precision == "mixed" else 8
-    iters = r.iterations
+    iters_per_step = int(np.mean([rr.iterations for rr, _ in results]))
+    units = args.steps if args.full else args.steps * iters_per_step
+    value = world * units / (ms / 1e3)
+    s_v = s_w = 4 if args.precision == "mixed" else 8
+    bpi = bytes_per_iteration(m, n, nnz, s_v, s_w)
     iter_ms = st["spmv_kernel_ms"] / max(1, st["spmv_kernel_launches"] // 2)
-    bpi = bytes_per_iteration(m, n, nnz, 8, 8) if args.precision == "fp64" else None
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except OSError:
         pass
-    peak = peaks.get("hbm_gbs", 6650.0)
-    achieved = (bpi / (iter_ms * 1e-3) / 1e9) if bpi else None
-    launches = sum(s["kernel_launches"] for _, s in results)
-    # e2e through the C API from pinned host buffers (presolve on, as the reference's C API)
-    e2e = run_e2e(args, lp, world) if not args.no_e2e else None
+    peak = peaks.get("hbm_gbs")
+    peak_src = "measured" if peak else "fallback"
+    peak = peak or 6650.0
+    achieved = bpi / (iter_ms * 1e-3) / 1e9
+    full = WORKLOADS[args.workload]["full_iterations"]
+    rate = value / world
     line = {
-        "metric": f"time-to-1e-8 KKT, {args.workload} ({args.precision}), as solves/s",
-        "value": world * args.steps / (ms / 1e3), "unit": "solves/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
-        "data": "synthetic (seeded generator)",
-        "config": {"workload": WORKLOADS[args.workload]["desc"], "m": m, "n": n, "nnz": nnz,
-                   "tolerance": 1e-8, "precision": args.precision, "entry": "ps26119_solve_lp_device (no presolve)",
-                   "iterations": iters, "parallelism": f"replicas x{world}",
-                   "l2": f"inputs larger than L2: {bpi or 0} algorithmic bytes per iteration"},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": (achieved / peak) if achieved else None, "traffic": None,
-                     "unit_of_work": "one r2HPDHG iteration (the two fused SpMV kernels)",
-                     "iteration_kernel_us": iter_ms * 1e3},
-        "gpu_launches": launches,
+        "metric": metric_name(args), "value": value, "unit": "solves/s" if args.full else "iterations/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "f32+f64", "data": "synthetic (seeded generator)",
+        "config": {"workload": WORKLOADS[args.workload]["desc"], "m": m, "n": n, "nnz": nnz, "tolerance": 1e-8,
+                   "precision": args.precision, "entry": "ps26119_solve_lp_device (engine level, no presolve)",
+                   "iterations_per_step": iters_per_step, "iteration_cap": limit or None,
+                   "iterations_to_1e-8": full, "parallelism": f"replicas x{world}",
+                   "l2": f"inputs larger than L2: {bpi / 1e6:.0f} MB streamed per iteration",
+                   "time_to_1e-8_s": (None if args.full or not full else
+                                      st["setup_seconds"] + full / rate)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": NCU_TRAFFIC.get((args.workload, args.precision)),
+                     "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)",
+                     "unit_of_work": "one r2HPDHG iteration: the two fused SpMV+update kernels",
+                     "algorithmic_bytes": bpi, "kernel_us_per_iteration": iter_ms * 1e3},
+        "gpu_launches": int(sum(s["kernel_launches"] for _, s in results)),
         "clocks": clocks.summary(),
-        "solve": {"objective": r.objective, "primal_residual": r.primal_residual, "dual_residual": r.dual_residual,
-                  "gap": r.gap, "check": r.check, "setup_s": st["setup_seconds"], "loop_s": st["loop_seconds"],
+        "solve": {"status": r.status_name, "iterations": r.iterations, "objective": r.objective,
+                  "primal_residual": r.primal_residual, "dual_residual": r.dual_residual, "gap": r.gap,
+                  "check": r.check, "setup_s": st["setup_seconds"], "loop_s": st["loop_seconds"],
                   "finish_s": st["finish_seconds"], "checks": st["checks"], "restarts": st["restarts"]},
     }
-    if e2e:
-        line["e2e"] = e2e
+    if not args.no_e2e:
+        line["e2e"] = run_e2e(args, lp, world, limit)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = reference_sample(args, lp, iters)
+        line["cpu_baseline"] = reference_sample(args, lp, iters_per_step, full)
     return line
 
 
-def run_e2e(args, lp, world):
+def run_e2e(args, lp, world, limit):
     import torch
     import ps26119
     pin = lambda a, dt: torch.as_tensor(np.ascontiguousarray(a), dtype=dt).pin_memory().numpy()
     c, cl, cu = pin(lp.c, torch.float64), pin(lp.col_lower, torch.float64), pin(lp.col_upper, torch.float64)
     rl, ru = pin(lp.row_lower, torch.float64), pin(lp.row_upper, torch.float64)
     cs, ri, v = pin(lp.col_start, torch.int32), pin(lp.row_index, torch.int32), pin(lp.value, torch.float64)
+    iters = 0
     t0 = time.perf_counter()
-    r = ps26119.solve_lp(c, (cs, ri, v), rl, ru, cl, cu, sense=lp.sense, offset=lp.offset, algorithm="r2hpdhg",
-                         precision=args.precision)
+    for _ in range(args.e2e_steps):
+        r = ps26119.solve_lp(c, (cs, ri, v), rl, ru, cl, cu, sense=lp.sense, offset=lp.offset, algorithm="r2hpdhg",
+                             precision=args.precision, iteration_limit=limit)
+        if r.status not in (ps26119.OPTIMAL, ps26119.ITERATION_LIMIT):
+            raise RuntimeError(f"e2e solve ended {r.status_name}: {r.message}")
+        iters += r.iterations
     sec = max_over_ranks(time.perf_counter() - t0, world)
-    if r.status != ps26119.OPTIMAL:
-        raise RuntimeError(f"e2e solve ended {r.status_name}: {r.message}")
     h2d = lp.nnz * 12 + (lp.num_cols + 1) * 4 + lp.num_cols * 24 + lp.num_rows * 16
     d2h = lp.num_cols * 16 + lp.num_rows * 8
-    return {"value": world / sec, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-            "steps": 1, "entry": "ps26119_solve_lp_ex (presolve on)", "iterations": r.iterations,
-            "check": r.check}
+    units = args.e2e_steps if args.full else iters
+    return {"value": world * units / sec, "unit": "solves/s" if args.full else "iterations/s",
+            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": args.e2e_steps,
+            "entry": "ps26119_solve_lp_ex (presolve + in-process check)", "ms_per_step": sec * 1e3 / args.e2e_steps,
+            "iterations_per_step": iters // max(1, args.e2e_steps), "check": r.check}
 
 
-def reference_sample(args, lp, full_iterations):
-    """The reference CPU engine on this workload: a bounded, iteration-limited sample with all
-    host threads, extrapolated to the full iteration count."""
+def reference_sample(args, lp, iterations, full):
+    """The reference CPU engine on this workload: one bounded, iteration-limited run with all
+    host threads, its per-iteration time applied to the iterations of one GPU step."""
     import reference
-    if not reference.available():
-        return {"value": None, "unit": "solves/s", "cores": os.cpu_count(), "kind": "reference",
-                "sample": "reference library not built"}
     cores = os.cpu_count() or 1
-    limit = args.cpu_sample_iterations
-    s = reference.solve(lp, presolve=False, precision=args.precision, threads=0, iteration_limit=limit)
+    if not reference.available():
+        return {"value": None, "unit": "iterations/s", "cores": cores, "kind": "reference",
+                "sample": "reference library not built"}
+    s = reference.solve(lp, presolve=True, precision=args.precision, threads=0,
+                        iteration_limit=args.cpu_sample_iterations)
     per_iter = (s.seconds - s.setup_seconds) / max(1, s.iterations)
-    total = s.setup_seconds + per_iter * full_iterations
-    return {"value": 1.0 / total, "unit": "solves/s", "cores": cores, "kind": "reference",
-            "sample": f"{s.iterations} iterations + setup ({s.seconds:.1f} s wall), extrapolated to "
-                      f"{full_iterations} iterations; per-iteration {per_iter * 1e3:.2f} ms, setup "
-                      f"{s.setup_seconds:.2f} s"}
+    its = full if args.full else iterations
+    total = s.setup_seconds + per_iter * its
+    return {"value": (1.0 if args.full else its) / total, "unit": "solves/s" if args.full else "iterations/s",
+            "cores": cores, "kind": "reference",
+            "sample": f"reference ps26119::solve (r2hpdhg, presolve, {cores} threads): {s.iterations} iterations "
+                      f"+ setup in {s.seconds:.1f} s ({per_iter * 1e3:.2f} ms/iteration, setup "
+                      f"{s.setup_seconds:.2f} s), applied to {its} iterations"}
 
 
 def run_reference(args, rank, world):
@@ -273,53 +301,52 @@ def run_reference(args, rank, world):
         return None
     import reference
     if not reference.available():
-        return {"impl": "reference", "unavailable": "reference library oracle/_ref not built on this machine"}
+        return {"impl": "reference", "unavailable": "reference library oracle/_ref was not built on this machine"}
     lp = make_lp(args.workload)
-    full = FULL_ITERATIONS.get(args.workload)
+    full = WORKLOADS[args.workload]["full_iterations"]
+    its = full if args.full else args.iterations
     cores = os.cpu_count() or 1
-    limit = args.cpu_sample_iterations
-    times = []
-    sample = None
+    times, sample = [], None
     for i in range(args.warmup + args.steps):
-        s = reference.solve(lp, presolve=True, precision=args.precision, threads=0, iteration_limit=limit)
+        s = reference.solve(lp, presolve=True, precision=args.precision, threads=0,
+                            iteration_limit=args.cpu_sample_iterations)
         per_iter = (s.seconds - s.setup_seconds) / max(1, s.iterations)
-        its = full or s.iterations
-        total = s.setup_seconds + per_iter * its
         if i >= args.warmup:
-            times.append(total)
-        sample = (f"reference ps26119::solve (presolve on, r2hpdhg, {cores} threads): {s.iterations} iterations "
-                  f"+ setup per step, extrapolated to {its} iterations")
+            times.append(s.setup_seconds + per_iter * its)
+        sample = (f"reference ps26119::solve (r2hpdhg, presolve, {cores} threads): {s.iterations} iterations + "
+                  f"setup per step ({per_iter * 1e3:.2f} ms/iteration), applied to {its} iterations")
     sec = float(np.mean(times))
-    value = 1.0 / sec
-    return {"metric": f"time-to-1e-8 KKT, {args.workload} ({args.precision}), as solves/s", "value": value,
-            "unit": "solves/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64" if args.precision == "fp64" else "f32+f64", "data": "synthetic (seeded generator)",
+    value = (1.0 if args.full else its) / sec
+    unit = "solves/s" if args.full else "iterations/s"
+    return {"metric": metric_name(args), "value": value, "unit": unit, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+            "data": "synthetic (seeded generator)",
             "config": {"workload": WORKLOADS[args.workload]["desc"], "m": lp.num_rows, "n": lp.num_cols,
-                       "nnz": lp.nnz, "tolerance": 1e-8, "precision": args.precision},
+                       "nnz": lp.nnz, "tolerance": 1e-8, "precision": args.precision,
+                       "iterations_per_step": its},
             "impl": "reference",
-            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "reference",
-                             "sample": sample},
-            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "cpu_baseline": {"value": value, "unit": unit, "cores": cores, "kind": "reference", "sample": sample},
+            "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="random1m")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--iterations", type=int, default=6400, help="iteration cap of one step")
+    ap.add_argument("--full", action="store_true", help="solve to 1e-8 in every step")
+    ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--cpu-sample-iterations", type=int, default=256)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
-    rank, world, local = dist_setup(args.gpus)
-    if args.impl == "reference":
-        line = run_reference(args, rank, world)
-    else:
-        line = run_ours(args, rank, world, local)
+    rank, world, local = dist_setup()
+    line = run_reference(args, rank, world) if args.impl == "reference" else run_ours(args, rank, world, local)
     if rank == 0 and line is not None:
         print(json.dumps(line))
     if world > 1:
