@@ -48,9 +48,9 @@ WORKLOADS = {
     "staircase8760": {"desc": "staircase planning LP T=8760 (429,240 x 525,600), seed 1", "kind": "staircase",
                       "T": 8760, "full_iterations": None},
 }
-# DRAM bytes per iteration (both fused kernels) from the ncu capture summarised in
-# profiles/fused_spmv_random1m.md (fp64); None where not captured.
-NCU_TRAFFIC = {("random1m", "fp64"): None}
+# DRAM bytes per iteration (both fused kernels: dram__bytes_read.sum + dram__bytes_write.sum of
+# one launch each) from the ncu capture summarised in profiles/fused_spmv_random1m.md.
+NCU_TRAFFIC = {("random1m", "fp64"): 160.1e6 + 126.3e6}
 
 
 def make_lp(name):

@@ -21,7 +21,6 @@
  *   precision policy   src/pdhg/engine.cpp:56-79, 186-192
  *   context / finish   src/pdhg/engine.cpp:195-307
  *   r²HPDHG loop       src/pdhg/r2hpdhg.cpp:11-162
- *   batch              src/pdhg/batch.cpp:129-441
  */
 #ifndef PDHG_ORACLE_H
 #define PDHG_ORACLE_H
