@@ -172,6 +172,12 @@ int solve_host(int num_rows, int num_cols, int sense, double obj_offset, const d
 
 }  // namespace
 
+namespace b200 {
+// Sets the calling thread's last-error text (read through ps26119_backend_last_error); used by
+// entry points defined outside this file.
+void set_backend_error(const std::string& text) { g_backend_error = text; }
+}  // namespace b200
+
 struct ps26119_backend {
   std::unique_ptr<GpuBackend> impl;
 };

@@ -97,7 +97,7 @@ EXPORTS = ["ps26119_version", "ps26119_default_options", "ps26119_solve_lp", "ps
            "ps26119_backend_dual_step", "ps26119_backend_r2h_primal", "ps26119_backend_r2h_dual",
            "ps26119_backend_fused_primal", "ps26119_backend_fused_dual", "ps26119_backend_kkt",
            "ps26119_backend_sync", "ps26119_backend_scaled_get", "ps26119_backend_scaled_structure",
-           "ps26119_backend_scalars", "ps26119_backend_norm2_estimate"]
+           "ps26119_backend_scalars", "ps26119_backend_norm2_estimate", "ps26119_dot_noalloc"]
 
 _lib = None
 
@@ -151,6 +151,8 @@ def load(path: str | None = None):
     L.ps26119_backend_scaled_structure.restype = ctypes.c_longlong
     L.ps26119_backend_scalars.argtypes = [B, _D]
     L.ps26119_backend_norm2_estimate.argtypes = [B, _D]
+    L.ps26119_dot_noalloc.argtypes = [ctypes.c_longlong, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                      ctypes.c_void_p, ctypes.c_void_p]
     if path is None:
         _lib = L
     return L
