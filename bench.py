@@ -1,7 +1,7 @@
 """Benchmark of the B200 r²HPDHG engine on the 1M x 1.5M random LP (BASELINE config 2 shape).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload random1m|random10k|staircase8760] [--precision fp64|mixed]
+                    [--workload random1m|random10k|staircase8760|batch720x64] [--precision fp64|mixed]
                     [--iterations L | --full]
 
 One STEP is one cold solve of the seeded LP on the device: setup (structure, scaling, ‖Ã‖₂),
@@ -47,6 +47,9 @@ WORKLOADS = {
                   "kind": "random", "m": 10_000, "full_iterations": 249_088},
     "staircase8760": {"desc": "staircase planning LP T=8760 (429,240 x 525,600), seed 1", "kind": "staircase",
                       "T": 8760, "full_iterations": None},
+    "batch720x64": {"desc": "64 scenarios (b, c x lognormal(0, 0.1)) of the staircase LP T=720 "
+                            "(35,280 x 43,200, 126,024 nnz), seed 1", "kind": "batch", "T": 720, "K": 64,
+                    "full_iterations": None},
 }
 # DRAM bytes per iteration (both fused kernels: dram__bytes_read.sum + dram__bytes_write.sum of
 # one launch each) from the ncu capture summarised in profiles/fused_spmv_random1m.md.
@@ -57,6 +60,84 @@ def make_lp(name):
     from ps26119 import generators as g
     w = WORKLOADS[name]
     return g.random_lp(w["m"], seed=1) if w["kind"] == "random" else g.staircase_lp(w["T"], seed=1)
+
+
+def make_scenarios(name, lp):
+    from ps26119 import generators as g
+    return g.scenarios(lp, WORKLOADS[name]["K"], sigma=0.1, seed=1)
+
+
+def run_batch(args, rank, world, local):
+    """The shared-matrix batch (ps26119_solve_batch): one step = one batch solve of K scenarios
+    from host arrays (the batch entry point takes host memory, so value and e2e are the same
+    call); unit = scenario-iterations/s (or scenario solves/s with --full)."""
+    import torch
+    import ps26119
+    torch.cuda.set_device(local)
+    lp = make_lp(args.workload)
+    scen = make_scenarios(args.workload, lp)
+    K = len(scen)
+    limit = 0 if args.full else args.iterations
+    A = (lp.col_start, lp.row_index, lp.value)
+
+    def step():
+        res = ps26119.solve_batch(lp.c, A, lp.row_lower, lp.row_upper, lp.col_lower, lp.col_upper, scenarios=scen,
+                                  sense=lp.sense, offset=lp.offset, iteration_limit=limit)
+        bad = [r.status_name for r in res if r.status_name not in ("Optimal", "IterationLimit")]
+        if bad or (args.full and any(r.status_name != "Optimal" for r in res)):
+            raise RuntimeError(f"batch ended {set(r.status_name for r in res)}")
+        return res, ps26119.last_stats()
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier(world)
+    results = []
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            results.append(step())
+        torch.cuda.synchronize()
+        sec = time.perf_counter() - t0
+    sec = max_over_ranks(sec, world)
+    res, st = results[-1]
+    scen_its = sum(r.iterations for r in res)
+    units = K * args.steps if args.full else scen_its * args.steps
+    value = world * units / sec
+    m, n, nnz = lp.num_rows, lp.num_cols, lp.nnz
+    bpi = 2 * nnz * 12 + 4 * (m + n) + K * 8 * (9 * n + 7 * m)  # per lockstep iteration, all K slots
+    unit = "scenario solves/s" if args.full else "scenario-iterations/s"
+    its = max(r.iterations for r in res)
+    line = {
+        "metric": f"batched r2HPDHG on {args.workload} ({unit})", "value": value, "unit": unit, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3 / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
+        "config": {"workload": WORKLOADS[args.workload]["desc"], "m": m, "n": n, "nnz": nnz, "scenarios": K,
+                   "tolerance": 1e-8, "iteration_cap": limit or None, "entry": "ps26119_solve_batch (host arrays)",
+                   "iterations_per_step": its, "parallelism": f"replicas x{world}",
+                   "l2": f"inputs larger than L2: {bpi / 1e6:.0f} MB streamed per lockstep iteration"},
+        "roofline": {"bound": "hbm", "algorithmic_bytes": bpi,
+                     "achieved_whole_step": bpi * its * args.steps / sec / 1e9, "unit": "GB/s",
+                     "note": "iterations x algorithmic bytes / step wall time (setup and checks included)"},
+        "gpu_launches": int(sum(s["kernel_launches"] for _, s in results)),
+        "clocks": clocks.summary(),
+        "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": nnz * 12 + (n + 1) * 4 + K * 8 * (3 * n + 2 * m),
+                "d2h_bytes_per_step": K * 8 * (2 * n + m), "note": "the batch entry point takes host arrays"},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import reference
+        cores = os.cpu_count() or 1
+        if reference.available():
+            t0 = time.perf_counter()
+            w = reference.batch(lp, scen, threads=0, iteration_limit=args.cpu_sample_iterations)
+            rs = time.perf_counter() - t0
+            rits = max(x["iterations"] for x in w)
+            line["cpu_baseline"] = {"value": K * rits / rs, "unit": "scenario-iterations/s", "cores": cores,
+                                    "kind": "reference",
+                                    "sample": f"reference solve_batch ({cores} threads), {rits} lockstep iterations "
+                                              f"of {K} scenarios incl. setup in {rs:.1f} s"}
+    return line
 
 
 def bytes_per_iteration(m, n, nnz, s_v, s_w):
@@ -191,16 +272,17 @@ def run_ours(args, rank, world, local):
         step()
     torch.cuda.synchronize()
     barrier(world)
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
     results = []
     with ClockSampler(local) as clocks:
         torch.cuda.synchronize()
-        ev0.record(stream)
-        for _ in range(args.steps):
+        evs[0].record(stream)
+        for k in range(args.steps):
             results.append(step())
-        ev1.record(stream)
+            evs[k + 1].record(stream)
         torch.cuda.synchronize()
-    ms = max_over_ranks(ev0.elapsed_time(ev1), world)
+    ms = max_over_ranks(evs[0].elapsed_time(evs[-1]), world)
+    step_ms = [evs[k].elapsed_time(evs[k + 1]) for k in range(args.steps)]
     barrier(world)
     r, st = results[-1]
     iters_per_step = int(np.mean([rr.iterations for rr, _ in results]))
@@ -237,6 +319,8 @@ def run_ours(args, rank, world, local):
                      "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)",
                      "unit_of_work": "one r2HPDHG iteration: the two fused SpMV+update kernels",
                      "algorithmic_bytes": bpi, "kernel_us_per_iteration": iter_ms * 1e3},
+        "step_ms": step_ms,
+        "step_engine_ms": [1e3 * rr.seconds for rr, _ in results],
         "gpu_launches": int(sum(s["kernel_launches"] for _, s in results)),
         "clocks": clocks.summary(),
         "solve": {"status": r.status_name, "iterations": r.iterations, "objective": r.objective,
@@ -303,9 +387,33 @@ def run_reference(args, rank, world):
     if not reference.available():
         return {"impl": "reference", "unavailable": "reference library oracle/_ref was not built on this machine"}
     lp = make_lp(args.workload)
+    cores = os.cpu_count() or 1
+    if WORKLOADS[args.workload]["kind"] == "batch":
+        if args.full:
+            return {"impl": "reference", "unavailable": "--full batch: the reference CPU batch to 1e-8 takes hours"}
+        scen = make_scenarios(args.workload, lp)
+        K = len(scen)
+        rates = []
+        for i in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            w = reference.batch(lp, scen, threads=0, iteration_limit=args.cpu_sample_iterations)
+            sec = time.perf_counter() - t0
+            if i >= args.warmup:
+                rates.append(K * max(x["iterations"] for x in w) / sec)
+        value = float(np.mean(rates))
+        unit = "scenario-iterations/s"
+        sample = (f"reference solve_batch ({cores} threads): {args.cpu_sample_iterations} lockstep iterations of "
+                  f"{K} scenarios incl. setup per step")
+        return {"metric": f"batched r2HPDHG on {args.workload} ({unit})", "value": value, "unit": unit,
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": None,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded generator)",
+                "config": {"workload": WORKLOADS[args.workload]["desc"], "scenarios": K, "tolerance": 1e-8},
+                "impl": "reference",
+                "cpu_baseline": {"value": value, "unit": unit, "cores": cores, "kind": "reference", "sample": sample},
+                "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     full = WORKLOADS[args.workload]["full_iterations"]
     its = full if args.full else args.iterations
-    cores = os.cpu_count() or 1
     times, sample = [], None
     for i in range(args.warmup + args.steps):
         s = reference.solve(lp, presolve=True, precision=args.precision, threads=0,
@@ -346,7 +454,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     rank, world, local = dist_setup()
-    line = run_reference(args, rank, world) if args.impl == "reference" else run_ours(args, rank, world, local)
+    if args.impl == "reference":
+        line = run_reference(args, rank, world)
+    elif WORKLOADS[args.workload]["kind"] == "batch":
+        line = run_batch(args, rank, world, local)
+    else:
+        line = run_ours(args, rank, world, local)
     if rank == 0 and line is not None:
         print(json.dumps(line))
     if world > 1:

@@ -162,6 +162,33 @@ typedef struct {
 
 PS26119_API void ps26119_last_stats(ps26119_stats* out);
 
+/* One scenario of a batch: host arrays of the base model's sizes (a pointer carries no length:
+ * each array must hold n or m values); NULL keeps the base's vector (an empty vector in the
+ * reference's ps26119::Scenario, include/ps26119/batch.h:22-28). */
+typedef struct {
+  const double* obj;
+  const double* col_lower;
+  const double* col_upper;
+  const double* row_lower;
+  const double* row_upper;
+} ps26119_scenario;
+
+/* ps26119::solve_batch (reference include/ps26119/batch.h:32-33, src/pdhg/batch.cpp:129-441,
+ * which the reference offers in C++ and through its CLI `batch` command): K LPs that share the
+ * base model's matrix, solved by r²HPDHG in lockstep on the GPU, fp64, no presolve, no
+ * infeasibility detection (as the reference). results[k] receives scenario k's outcome (status,
+ * objective, residuals, iterations, engine "r2hpdhg-batch"); x (K×n), y (K×m), z (K×n),
+ * scenario-major, may be NULL. engine may be NULL; its presolve and warm_primal_weight fields are
+ * ignored. opt->use_gpu is ignored (the batch always runs on the GPU). Returns 0 when the batch
+ * ran (per-scenario status in results), or PS26119_INVALID_ARGUMENT / PS26119_NOT_SOLVED with the
+ * reason in every results[k].message. */
+PS26119_API int ps26119_solve_batch(int num_rows, int num_cols, int sense, double obj_offset, const double* c,
+                                    const double* col_lower, const double* col_upper, const double* row_lower,
+                                    const double* row_upper, const int* col_start, const int* row_index,
+                                    const double* value, int num_scenarios, const ps26119_scenario* scenarios,
+                                    const ps26119_options* opt, const ps26119_engine_options* engine,
+                                    ps26119_result* results, double* x, double* y, double* z);
+
 #ifdef __cplusplus
 }
 #endif

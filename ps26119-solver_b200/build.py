@@ -23,7 +23,7 @@ LIB = os.path.join(LIB_DIR, "libps26119.so")
 CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA, "bin", "nvcc")
 
-CU_SOURCES = ["engine.cu", "backend.cu", "noalloc.cu"]
+CU_SOURCES = ["engine.cu", "backend.cu", "batch.cu", "noalloc.cu"]
 CPP_SOURCES = ["solver.cpp", "c_api.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC", "-Xcompiler",

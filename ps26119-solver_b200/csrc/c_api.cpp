@@ -1,5 +1,6 @@
 // c_api.cpp — the C ABI (include/ps26119.h, include/ps26119_backend.h). Exceptions never
 // cross this boundary (reference src/core/c_api.cpp:1-304 for the five reference symbols).
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -7,6 +8,7 @@
 #include <memory>
 #include <new>
 #include <string>
+#include <vector>
 
 #include <cuda_runtime.h>
 
@@ -471,3 +473,78 @@ int ps26119_backend_scalars(ps26119_backend* b, double* out) { B200_GUARD(b->imp
 int ps26119_backend_norm2_estimate(ps26119_backend* b, double* out) { B200_GUARD(*out = b->impl->norm2_estimate()) }
 
 }  // extern "C"
+
+extern "C" int ps26119_solve_batch(int num_rows, int num_cols, int sense, double obj_offset, const double* c,
+                                   const double* col_lower, const double* col_upper, const double* row_lower,
+                                   const double* row_upper, const int* col_start, const int* row_index,
+                                   const double* value, int num_scenarios, const ps26119_scenario* scenarios,
+                                   const ps26119_options* opt, const ps26119_engine_options* engine,
+                                   ps26119_result* results, double* x, double* y, double* z) {
+  if (num_scenarios < 0 || (num_scenarios > 0 && (!results || !scenarios))) return PS26119_INVALID_ARGUMENT;
+  for (int k = 0; k < num_scenarios; ++k) clear(&results[k]);
+  auto fail = [&](int status, const std::string& why) {
+    for (int k = 0; k < num_scenarios; ++k) {
+      results[k].status = status;
+      set_text(results[k].message, sizeof results[k].message, why);
+    }
+    return status;
+  };
+  if (num_rows < 0 || num_cols < 0) return fail(PS26119_INVALID_ARGUMENT, "negative dimension");
+  if (!col_start) return fail(PS26119_INVALID_ARGUMENT, "col_start is NULL");
+  if (num_cols > 0 && (!c || !col_lower || !col_upper)) return fail(PS26119_INVALID_ARGUMENT, "column data is NULL");
+  if (num_rows > 0 && (!row_lower || !row_upper)) return fail(PS26119_INVALID_ARGUMENT, "row bounds are NULL");
+  const int nnz = col_start[num_cols];
+  if (nnz < 0) return fail(PS26119_INVALID_ARGUMENT, "col_start[n] < 0");
+  if (nnz > 0 && (!row_index || !value)) return fail(PS26119_INVALID_ARGUMENT, "matrix arrays are NULL");
+  try {
+    Model m;
+    m.num_rows = num_rows;
+    m.num_cols = num_cols;
+    m.sense = sense;
+    m.obj_offset = obj_offset;
+    m.obj.assign(c, c + num_cols);
+    m.col_lower.assign(col_lower, col_lower + num_cols);
+    m.col_upper.assign(col_upper, col_upper + num_cols);
+    m.row_lower.assign(row_lower, row_lower + num_rows);
+    m.row_upper.assign(row_upper, row_upper + num_rows);
+    m.col_start.assign(col_start, col_start + num_cols + 1);
+    m.row_index.assign(row_index, row_index + nnz);
+    m.value.assign(value, value + nnz);
+    Options o;
+    if (const char* err = to_options(opt, num_rows, num_cols, o)) return fail(PS26119_INVALID_ARGUMENT, err);
+    if (const char* err = apply_engine_options(engine, o)) return fail(PS26119_INVALID_ARGUMENT, err);
+    std::vector<Scenario> sc(static_cast<std::size_t>(num_scenarios));
+    auto take = [](const double* a, int len) { return a ? std::vector<double>(a, a + len) : std::vector<double>(); };
+    for (int k = 0; k < num_scenarios; ++k) {
+      const ps26119_scenario& s = scenarios[k];
+      sc[k].obj = take(s.obj, num_cols);
+      sc[k].col_lower = take(s.col_lower, num_cols);
+      sc[k].col_upper = take(s.col_upper, num_cols);
+      sc[k].row_lower = take(s.row_lower, num_rows);
+      sc[k].row_upper = take(s.row_upper, num_rows);
+    }
+    const std::vector<Solution> sols = solve_batch(m, sc, o);
+    long long launches = 0;
+    for (int k = 0; k < num_scenarios; ++k) {
+      const Solution& s = sols[k];
+      fill(s, &results[k]);
+      launches = std::max(launches, s.engine_result.kernel_launches);
+      const std::size_t ok = static_cast<std::size_t>(k);
+      if (x && s.x.size() == static_cast<std::size_t>(num_cols))
+        std::copy(s.x.begin(), s.x.end(), x + ok * num_cols);
+      if (y && s.y.size() == static_cast<std::size_t>(num_rows))
+        std::copy(s.y.begin(), s.y.end(), y + ok * num_rows);
+      if (z && s.z.size() == static_cast<std::size_t>(num_cols))
+        std::copy(s.z.begin(), s.z.end(), z + ok * num_cols);
+    }
+    g_stats = ps26119_stats{};
+    g_stats.kernel_launches = launches;
+    g_stats.m = num_rows, g_stats.n = num_cols, g_stats.nnz = nnz;
+    if (num_scenarios > 0) g_stats.setup_seconds = sols[0].setup_seconds;
+    return 0;
+  } catch (const std::bad_alloc&) {
+    return fail(PS26119_NOT_SOLVED, "out of memory");
+  } catch (const std::exception& e) {
+    return fail(PS26119_NUMERICAL_ERROR, e.what());
+  }
+}

@@ -2,6 +2,7 @@
 // dispatcher around the GPU engine. Each function follows the reference function named in
 // its comment (file:line in the reference project); the engine itself runs on the GPU.
 #include "solver.hpp"
+#include "batch.hpp"
 
 #include <algorithm>
 #include <chrono>
@@ -58,11 +59,13 @@ std::string Model::validate() const {  // model.cpp:93-151
   }
   auto check_bounds = [&](const std::vector<double>& lo, const std::vector<double>& up, const char* what) {
     for (std::size_t k = 0; k < lo.size(); ++k) {
+      const bool nan = std::isnan(lo[k]) || std::isnan(up[k]);
+      if (!nan && lo[k] != kInf && up[k] != -kInf) continue;  // the common case builds no message
       std::ostringstream e;
-      if (std::isnan(lo[k]) || std::isnan(up[k])) e << what << " bound " << k << " is NaN";
+      if (nan) e << what << " bound " << k << " is NaN";
       else if (lo[k] == kInf) e << what << " lower bound " << k << " is +inf";
-      else if (up[k] == -kInf) e << what << " upper bound " << k << " is -inf";
-      if (!e.str().empty()) return e.str();
+      else e << what << " upper bound " << k << " is -inf";
+      return e.str();
     }
     return std::string();
   };
@@ -234,24 +237,17 @@ bool within(double v, double lo, double up) {
 PresolveResult presolve(const Model& M) {  // presolve.cpp:22-156 (LP: no integer columns here)
   PresolveResult r;
   const int m = M.num_rows, n = M.num_cols;
-  // row access: CSR of A, columns in increasing order inside each row (la::csr_from_model)
-  std::vector<int> rp(static_cast<std::size_t>(m) + 1, 0), rc(M.nnz());
-  std::vector<double> rv(M.nnz());
-  for (std::size_t k = 0; k < M.nnz(); ++k) ++rp[M.row_index[k] + 1];
-  for (int i = 0; i < m; ++i) rp[i + 1] += rp[i];
-  {
-    std::vector<int> next(rp.begin(), rp.end() - 1);
-    for (int j = 0; j < n; ++j)
-      for (int k = M.col_start[j]; k < M.col_start[j + 1]; ++k) {
-        const int p = next[M.row_index[k]]++;
-        rc[p] = j;
-        rv[p] = M.value[k];
-      }
-  }
+  // A singleton row's one remaining column is recovered as the XOR of the row's live column
+  // indices (kept up to date as columns are removed), and its coefficient by a scan of that
+  // column: the same (j, a) the reference finds by walking the row (presolve.cpp:60-66), with
+  // no row-wise copy of A.
+  std::vector<int> row_xor(static_cast<std::size_t>(m), 0);
+  for (int j = 0; j < n; ++j)
+    for (int k = M.col_start[j]; k < M.col_start[j + 1]; ++k) row_xor[M.row_index[k]] ^= j;
   std::vector<double> rl = M.row_lower, ru = M.row_upper, cl = M.col_lower, cu = M.col_upper;
   std::vector<char> row_alive(m, 1), col_alive(n, 1);
   std::vector<int> row_cnt(m), col_cnt(n);
-  for (int i = 0; i < m; ++i) row_cnt[i] = rp[i + 1] - rp[i];
+  for (int k = 0; k < static_cast<int>(M.nnz()); ++k) ++row_cnt[M.row_index[k]];
   for (int j = 0; j < n; ++j) col_cnt[j] = M.col_start[j + 1] - M.col_start[j];
   r.fixed_value.assign(n, kNaN);
   double offset = M.obj_offset;
@@ -271,11 +267,11 @@ PresolveResult presolve(const Model& M) {  // presolve.cpp:22-156 (LP: no intege
         ++r.removed_rows;
         changed = true;
       } else if (row_cnt[i] == 1) {
-        int j = -1;
+        const int j = row_xor[i];
         double a = 0;
-        for (int p = rp[i]; p < rp[i + 1]; ++p)
-          if (col_alive[rc[p]]) j = rc[p], a = rv[p];
-        if (j < 0 || a == 0.0) continue;
+        for (int p = M.col_start[j]; p < M.col_start[j + 1]; ++p)
+          if (M.row_index[p] == i) a = M.value[p];
+        if (!col_alive[j] || a == 0.0) continue;
         const double lo = a > 0 ? rl[i] / a : ru[i] / a;
         const double hi = a > 0 ? ru[i] / a : rl[i] / a;
         const bool set_lower = lo > cl[j], set_upper = hi < cu[j];
@@ -314,6 +310,7 @@ PresolveResult presolve(const Model& M) {  // presolve.cpp:22-156 (LP: no intege
         if (std::isfinite(rl[i])) rl[i] -= t;
         if (std::isfinite(ru[i])) ru[i] -= t;
         --row_cnt[i];
+        row_xor[i] ^= j;
       }
       offset += M.obj[j] * v;
       r.fixed_value[j] = v;
@@ -336,14 +333,28 @@ PresolveResult presolve(const Model& M) {  // presolve.cpp:22-156 (LP: no intege
   R.obj_offset = offset;
   R.num_rows = static_cast<int>(r.row_map.size());
   R.num_cols = static_cast<int>(r.col_map.size());
+  R.col_start.reserve(r.col_map.size() + 1);
+  R.obj.reserve(r.col_map.size());
+  R.col_lower.reserve(r.col_map.size());
+  R.col_upper.reserve(r.col_map.size());
+  R.row_index.reserve(M.nnz());
+  R.value.reserve(M.nnz());
+  R.row_lower.reserve(r.row_map.size());
+  R.row_upper.reserve(r.row_map.size());
   R.col_start.push_back(0);
   for (int j : r.col_map) {
     R.obj.push_back(M.obj[j]);
     R.col_lower.push_back(cl[j]);
     R.col_upper.push_back(cu[j]);
-    for (int p = M.col_start[j]; p < M.col_start[j + 1]; ++p) {
-      const int i = M.row_index[p];
-      if (new_row[i] >= 0) R.row_index.push_back(new_row[i]), R.value.push_back(M.value[p]);
+    if (r.removed_rows == 0) {  // row numbers unchanged: copy the column as it is
+      R.row_index.insert(R.row_index.end(), M.row_index.begin() + M.col_start[j],
+                         M.row_index.begin() + M.col_start[j + 1]);
+      R.value.insert(R.value.end(), M.value.begin() + M.col_start[j], M.value.begin() + M.col_start[j + 1]);
+    } else {
+      for (int p = M.col_start[j]; p < M.col_start[j + 1]; ++p) {
+        const int i = M.row_index[p];
+        if (new_row[i] >= 0) R.row_index.push_back(new_row[i]), R.value.push_back(M.value[p]);
+      }
     }
     R.col_start.push_back(static_cast<int>(R.value.size()));
   }
@@ -566,23 +577,10 @@ Solution solve_impl(const Model& model, const Options& options) {
     const int m = model.num_rows, n = model.num_cols;
     std::vector<double> ax = std::vector<double>(m, 0.0), aty(n, 0.0), ymin(s.y);
     for (double& v : ymin) v *= model.sense;
-    {  // A·x row-sequential in column order (CSR of A)
-      std::vector<int> rp(static_cast<std::size_t>(m) + 1, 0);
-      for (std::size_t k = 0; k < model.nnz(); ++k) ++rp[model.row_index[k] + 1];
-      for (int i = 0; i < m; ++i) rp[i + 1] += rp[i];
-      std::vector<int> next(rp.begin(), rp.end() - 1), cc(model.nnz());
-      std::vector<double> vv(model.nnz());
-      for (int j = 0; j < n; ++j)
-        for (int k = model.col_start[j]; k < model.col_start[j + 1]; ++k) {
-          const int p = next[model.row_index[k]]++;
-          cc[p] = j, vv[p] = model.value[k];
-        }
-      for (int i = 0; i < m; ++i) {
-        double acc = 0;
-        for (int p = rp[i]; p < rp[i + 1]; ++p) acc += vv[p] * s.x[cc[p]];
-        ax[i] = acc;
-      }
-    }
+    // A·x row-sequential in column order (kkt_general's CSR product): walking the columns in
+    // increasing order and adding into each row adds every row's terms in exactly that order.
+    for (int j = 0; j < n; ++j)
+      for (int k = model.col_start[j]; k < model.col_start[j + 1]; ++k) ax[model.row_index[k]] += model.value[k] * s.x[j];
     for (int j = 0; j < n; ++j) {
       double acc = 0;
       for (int k = model.col_start[j]; k < model.col_start[j + 1]; ++k) acc += model.value[k] * ymin[model.row_index[k]];
@@ -751,6 +749,100 @@ Solution solve(const Model& model, const Options& options) {  // solve.cpp:194-2
     s.message = std::string("internal error: ") + e.what();
     return s;
   }
+}
+
+// ============================================================ batch (batch.cpp:129-441)
+namespace {
+std::string fingerprint_hex(const Model& m) {
+  char buf[17];
+  std::snprintf(buf, sizeof buf, "%016llx", static_cast<unsigned long long>(m.fingerprint()));
+  return buf;
+}
+}  // namespace
+
+std::vector<Solution> solve_batch(const Model& base, const std::vector<Scenario>& scenarios, const Options& options) {
+  const auto t0 = clock_t_::now();
+  const int K = static_cast<int>(scenarios.size());
+  std::vector<Solution> out(K);
+  {  // fingerprints of the scenario models (batch.cpp:113-127): the base with the scenario's vectors
+    Model w = base;
+    for (int k = 0; k < K; ++k) {
+      const Scenario& s = scenarios[k];
+      w.obj = s.obj.empty() ? base.obj : s.obj;
+      w.col_lower = s.col_lower.empty() ? base.col_lower : s.col_lower;
+      w.col_upper = s.col_upper.empty() ? base.col_upper : s.col_upper;
+      w.row_lower = s.row_lower.empty() ? base.row_lower : s.row_lower;
+      w.row_upper = s.row_upper.empty() ? base.row_upper : s.row_upper;
+      out[k].model_fingerprint = fingerprint_hex(w);
+      out[k].engine = "r2hpdhg-batch";
+      out[k].precision = "fp64";
+    }
+  }
+  auto fail_all = [&](const std::string& why) {
+    for (auto& s : out) s.status = Status::NotSolved, s.message = why;
+    return out;
+  };
+  if (K == 0) return out;
+  try {
+    if (auto err = base.validate(); !err.empty()) return fail_all("invalid base model: " + err);
+    const int m = base.num_rows, n = base.num_cols;
+    std::vector<BatchScenarioView> views(K);
+    std::vector<int> slots;
+    for (int k = 0; k < K; ++k) {  // per-scenario validation (batch.cpp:154-181)
+      const Scenario& s = scenarios[k];
+      bool ok = true;
+      auto pick = [&](const std::vector<double>& v, const std::vector<double>& dflt, std::size_t len) {
+        if (v.empty()) return dflt.data();
+        ok = ok && v.size() == len;
+        return v.data();
+      };
+      BatchScenarioView& vw = views[k];
+      vw.c = pick(s.obj, base.obj, n);
+      vw.col_lower = pick(s.col_lower, base.col_lower, n);
+      vw.col_upper = pick(s.col_upper, base.col_upper, n);
+      vw.row_lower = pick(s.row_lower, base.row_lower, m);
+      vw.row_upper = pick(s.row_upper, base.row_upper, m);
+      for (int j = 0; ok && j < n; ++j)
+        ok = std::isfinite(vw.c[j]) && !std::isnan(vw.col_lower[j]) && !std::isnan(vw.col_upper[j]);
+      for (int i = 0; ok && i < m; ++i) ok = !std::isnan(vw.row_lower[i]) && !std::isnan(vw.row_upper[i]);
+      bool crossed = false;
+      for (int j = 0; ok && !crossed && j < n; ++j) crossed = vw.col_lower[j] > vw.col_upper[j];
+      for (int i = 0; ok && !crossed && i < m; ++i) crossed = vw.row_lower[i] > vw.row_upper[i];
+      if (!ok) {
+        out[k].status = Status::NotSolved;
+        out[k].message = "scenario has wrong vector sizes or non-finite data";
+      } else if (crossed) {
+        out[k].status = Status::Infeasible;
+        out[k].message = "bounds cross: scenario has a lower bound above its upper bound";
+      } else {
+        slots.push_back(k);
+      }
+    }
+    if (slots.empty()) return out;
+    require_device();
+    EngineOptions eo = engine_options(options);
+    eo.mixed = false;  // the batch engine is fp64 (batch.cpp:136)
+    std::vector<BatchOutcome> res = run_batch_host(base.view(), views, slots, eo, t0);
+    for (int k : slots) {
+      BatchOutcome& r = res[k];
+      Solution& s = out[k];
+      s.status = r.status;
+      s.message = r.message;
+      s.x = std::move(r.x), s.y = std::move(r.y), s.z = std::move(r.z);
+      s.objective = r.objective, s.dual_objective = r.dual_objective;
+      s.primal_residual = r.primal_residual, s.dual_residual = r.dual_residual, s.gap = r.gap;
+      s.iterations = r.iterations, s.seconds = r.seconds, s.setup_seconds = r.setup_seconds;
+      s.iterations_to_fast = r.iterations_to_fast;
+      s.primal_weight = r.primal_weight;
+      s.engine_result.kernel_launches = r.kernel_launches;
+    }
+  } catch (const std::bad_alloc&) {
+    return fail_all("out of memory");
+  } catch (const std::exception& e) {
+    const std::string what = e.what();
+    return fail_all(what.rfind("no CUDA device", 0) == 0 ? "CUDA backend unavailable: " + what : what);
+  }
+  return out;
 }
 
 }  // namespace b200

@@ -6,6 +6,7 @@
 //   solve()   src/core/solve.cpp:194-609          (presolve wrapper, direct solve, gate)
 //   presolve  src/core/presolve.{h,cpp}            (R1-R4 + primal/dual postsolve)
 //   checker   src/core/solution_checker.{h,cpp}
+//   batch     include/ps26119/batch.h:22-33, src/pdhg/batch.cpp:129-441
 #pragma once
 
 #include <cstdint>
@@ -71,6 +72,8 @@ struct Solution {
   std::string engine = "r2hpdhg-b200", precision = "fp64", message;
   EngineResult engine_result;  // statistics of the last engine run
   double presolve_seconds = 0;
+  std::string model_fingerprint;  // set by solve_batch: the scenario model's (batch.cpp:113-127)
+  long long iterations_to_fast = -1;
 };
 
 // The in-process optimality check (solution_checker.cpp:61-133).
@@ -103,5 +106,14 @@ Solution postsolve(const Model& original, const PresolveResult& r, const Solutio
 
 // The library entry point: never throws (solve.cpp:194-210).
 Solution solve(const Model& model, const Options& options);
+
+// Differences from the base model; an empty vector means "same as the base" (batch.h:22-28).
+struct Scenario {
+  std::vector<double> obj, col_lower, col_upper, row_lower, row_upper;
+};
+// K LPs sharing the base's matrix, solved in lockstep on the GPU (batch.h:32-33): one Solution
+// per scenario, in order. Never throws. Runs on the GPU whatever options.use_gpu says (the
+// reference's batch is CPU-only; this is its replacement).
+std::vector<Solution> solve_batch(const Model& base, const std::vector<Scenario>& scenarios, const Options& options);
 
 }  // namespace b200

@@ -78,6 +78,10 @@ class _Stats(ctypes.Structure):  # ps26119_stats
                 ("spmv_kernel_ms", ctypes.c_double), ("spmv_kernel_launches", ctypes.c_longlong)]
 
 
+class _Scenario(ctypes.Structure):  # ps26119_scenario
+    _fields_ = [("obj", _D), ("col_lower", _D), ("col_upper", _D), ("row_lower", _D), ("row_upper", _D)]
+
+
 class _ScalingOptions(ctypes.Structure):  # ps26119_scaling_options
     _fields_ = [("geometric_mean_iterations", ctypes.c_int), ("geometric_mean_min_log10_range", ctypes.c_double),
                 ("ruiz_iterations", ctypes.c_int), ("pock_chambolle", ctypes.c_int),
@@ -89,7 +93,7 @@ _MODEL = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, _D, _D, _D,
 # Every symbol the C headers declare (include/ps26119.h, include/ps26119_backend.h).
 EXPORTS = ["ps26119_version", "ps26119_default_options", "ps26119_solve_lp", "ps26119_solve_lp_ex",
            "ps26119_solve_mps", "ps26119_default_engine_options", "ps26119_solve_lp_engine",
-           "ps26119_solve_lp_device", "ps26119_last_stats", "ps26119_backend_new", "ps26119_backend_free",
+           "ps26119_solve_lp_device", "ps26119_last_stats", "ps26119_solve_batch", "ps26119_backend_new", "ps26119_backend_free",
            "ps26119_backend_last_error", "ps26119_backend_set_precision", "ps26119_backend_create",
            "ps26119_backend_upload", "ps26119_backend_download", "ps26119_backend_fill", "ps26119_backend_copy",
            "ps26119_backend_axpby", "ps26119_backend_spmv", "ps26119_backend_spmv_t", "ps26119_backend_dot",
@@ -120,6 +124,8 @@ def load(path: str | None = None):
         [ctypes.c_void_p] * 8 + [P(_Options), P(_EngineOptions), P(_Result)] + [ctypes.c_void_p] * 4
     L.ps26119_solve_mps.argtypes = [ctypes.c_char_p, P(_Options), P(_Result), ctypes.c_char_p]
     L.ps26119_last_stats.argtypes = [P(_Stats)]
+    L.ps26119_solve_batch.argtypes = _MODEL + [ctypes.c_int, P(_Scenario), P(_Options), P(_EngineOptions),
+                                               P(_Result), _D, _D, _D]
     B = ctypes.c_void_p
     L.ps26119_backend_new.argtypes = [P(B)] + _MODEL + [P(_ScalingOptions), ctypes.c_int]
     L.ps26119_backend_free.argtypes = [B]
@@ -301,6 +307,53 @@ def solve_lp_device(m, n, sense, offset, ptrs, precision="fp64", tolerance=1e-8,
                                    *[ctypes.c_void_p(p) if p else None for p in out],
                                    ctypes.c_void_p(stream) if stream else None)
     return _result(st, res)
+
+
+def solve_batch(c, A, row_lower, row_upper, col_lower=None, col_upper=None, scenarios=(), sense=1, offset=0.0,
+                tolerance=1e-8, time_limit=3600.0, iteration_limit=0, engine=None, verbosity=0) -> list[Result]:
+    """ps26119::solve_batch on the GPU: the base LP (as :func:`solve_lp`) and a list of scenarios,
+    each a dict with any of obj, col_lower, col_upper, row_lower, row_upper (missing = the
+    base's). Returns one :class:`Result` per scenario (x, y, z set when the scenario has a point)."""
+    c = np.ascontiguousarray(c, dtype=np.float64)
+    n = c.size
+    rl = np.ascontiguousarray(row_lower, dtype=np.float64)
+    ru = np.ascontiguousarray(row_upper, dtype=np.float64)
+    m = rl.size
+    cl = np.zeros(n) if col_lower is None else np.ascontiguousarray(col_lower, dtype=np.float64)
+    cu = np.full(n, np.inf) if col_upper is None else np.ascontiguousarray(col_upper, dtype=np.float64)
+    cs, ri, v = _csc(A, m, n)
+    # A C pointer carries no length: a scenario vector of the wrong size is rejected here, alone,
+    # as the reference's solve_batch rejects it (batch.cpp:154-177); the others still run.
+    sizes = {"obj": n, "col_lower": n, "col_upper": n, "row_lower": m, "row_upper": m}
+    bad = [any(s.get(key) is not None and np.size(s[key]) != ln for key, ln in sizes.items()) for s in scenarios]
+    run = [k for k in range(len(scenarios)) if not bad[k]]
+    K = len(run)
+    keep = []
+    sc = (_Scenario * max(1, K))()
+    for t, k in enumerate(run):
+        for key in sizes:
+            if scenarios[k].get(key) is not None:
+                a = np.ascontiguousarray(scenarios[k][key], dtype=np.float64)
+                keep.append(a)
+                setattr(sc[t], key, _ptr(a))
+    opt = _options("r2hpdhg", "fp64", True, tolerance, time_limit, iteration_limit, verbosity, 1)
+    eo = engine_options(**(engine or {}))
+    res = (_Result * max(1, K))()
+    x, y, z = np.full((K, n), np.nan), np.full((K, m), np.nan), np.full((K, n), np.nan)
+    L = load()
+    L.ps26119_solve_batch(m, n, int(sense), float(offset), _ptr(c), _ptr(cl), _ptr(cu), _ptr(rl), _ptr(ru),
+                          _ptr(cs, ctypes.c_int), _ptr(ri, ctypes.c_int), _ptr(v), K, sc, ctypes.byref(opt),
+                          ctypes.byref(eo), res, _ptr(x), _ptr(y), _ptr(z))
+    out = [None] * len(scenarios)
+    for t, k in enumerate(run):
+        st = res[t].status
+        have = st in (OPTIMAL, ITERATION_LIMIT, TIME_LIMIT)
+        out[k] = _result(st, res[t], x[t] if have else None, y[t] if have else None, z[t] if have else None)
+    for k in range(len(scenarios)):
+        if bad[k]:
+            out[k] = Result(NOT_SOLVED, _STATUS[NOT_SOLVED], np.nan, np.nan, np.nan, np.nan, np.nan, np.nan, 0, 0.0,
+                            "r2hpdhg-batch", "scenario has wrong vector sizes or non-finite data")
+    return out
 
 
 def solve_mps(path, algorithm="auto", precision="fp64", gpu=True, tolerance=1e-8, time_limit=3600.0,
