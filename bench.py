@@ -93,7 +93,7 @@ def run_batch(args, rank, world, local):
     torch.cuda.synchronize()
     barrier(world)
     results = []
-    with ClockSampler(local) as clocks:
+    with clock_sampler(local) as clocks:
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for _ in range(args.steps):
@@ -144,6 +144,68 @@ def bytes_per_iteration(m, n, nnz, s_v, s_w):
     """Algorithmic bytes of one r²HPDHG iteration: Ã and Ãᵀ streamed once (values + int32 column
     indices), int32 row pointers, and the vectors 9n + 7m in the working precision."""
     return 2 * nnz * (s_v + 4) + 4 * (m + n) + s_w * (9 * n + 7 * m)
+
+
+class NvmlClockSampler:
+    """SM clocks and clock-event (throttle) reasons sampled every 200 ms during the timed region,
+    in-process through NVML. Only clocks and reasons are queried: a full nvidia-smi query (power
+    included) every 200 ms was measured to slow the engine's per-check synchronisations."""
+
+    NAMES = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+             ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+             ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+             ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"))
+
+    def __init__(self, gpu_index):
+        import pynvml
+        self.nv = pynvml
+        pynvml.nvmlInit()
+        count = pynvml.nvmlDeviceGetCount()
+        self.h = pynvml.nvmlDeviceGetHandleByIndex(0 if count == 1 else gpu_index)
+        self.samples = []
+        self.stop = threading.Event()
+
+    def _loop(self):
+        nv = self.nv
+        get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            nv.nvmlDeviceGetCurrentClocksThrottleReasons
+        while not self.stop.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+                mx = nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM)
+                self.samples.append((sm, mx, get_reasons(self.h)))
+            except Exception:  # noqa: BLE001 - a failed query is just a missing sample
+                pass
+            self.stop.wait(0.2)
+
+    def __enter__(self):
+        self.thread = threading.Thread(target=self._loop, daemon=True)
+        self.thread.start()
+        return self
+
+    def __exit__(self, *exc):
+        self.stop.set()
+        self.thread.join(timeout=5)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["not sampled"], "samples": 0}
+        reasons = set()
+        for _, _, bits in self.samples:
+            for name, attr in self.NAMES:
+                if bits & getattr(self.nv, attr, 0):
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median([s[0] for s in self.samples])),
+                "sm_max_mhz": float(max(s[1] for s in self.samples)), "reasons": sorted(reasons),
+                "samples": len(self.samples), "source": "nvml"}
+
+
+def clock_sampler(gpu_index):
+    """NVML when it loads, else nvidia-smi."""
+    try:
+        return NvmlClockSampler(gpu_index)
+    except Exception:  # noqa: BLE001 - no NVML: fall back to the nvidia-smi process
+        return ClockSampler(gpu_index)
 
 
 class ClockSampler:
@@ -274,7 +336,7 @@ def run_ours(args, rank, world, local):
     barrier(world)
     evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
     results = []
-    with ClockSampler(local) as clocks:
+    with clock_sampler(local) as clocks:
         torch.cuda.synchronize()
         evs[0].record(stream)
         for k in range(args.steps):

@@ -158,9 +158,34 @@ typedef struct {
   long long m, n, nnz;         /* size of the problem the engine ran on (after presolve) */
   double spmv_kernel_ms;       /* total device time of the fused iteration kernels (CUDA events) */
   long long spmv_kernel_launches;
+  double teardown_seconds;     /* releasing the engine's device state after the loop */
+  double call_seconds;         /* the whole entry-point call, host wall clock */
 } ps26119_stats;
 
 PS26119_API void ps26119_last_stats(ps26119_stats* out);
+
+/* certified_dual_bound (reference src/core/safe_bound.h:37-43, C++ only there): a
+ * rounding-error-proof bound on the model's optimum from ANY row multipliers y (the model's
+ * sense, as ps26119_result's y): at most the optimum for a minimisation, at least for a
+ * maximisation, infinite when a multiplier or reduced cost points at an infinite bound.
+ * use_implied_bounds = 1 lets columns bounded on one side take rigorous implied bounds.
+ * Host computation (no GPU). out[4] = finite (0/1), bound, unbounded row terms, unbounded
+ * column terms. Returns 0, or PS26119_INVALID_ARGUMENT for an invalid model. */
+PS26119_API int ps26119_certified_bound(int num_rows, int num_cols, int sense, double obj_offset, const double* c,
+                                        const double* col_lower, const double* col_upper, const double* row_lower,
+                                        const double* row_upper, const int* col_start, const int* row_index,
+                                        const double* value, const double* y, int use_implied_bounds, double* out);
+
+/* check_infeasibility_certificate / check_unboundedness_certificate (reference
+ * src/core/certificates.h:41-43): kind 0 checks a Farkas vector `ray` (num_rows values; x is
+ * ignored), kind 1 a feasible point x and a recession ray (num_cols values each). Host
+ * computation. out[5] = present, passed, rigorous (Farkas stage 1), measure, violation. Returns 0,
+ * or PS26119_INVALID_ARGUMENT. */
+PS26119_API int ps26119_check_certificate(int kind, int num_rows, int num_cols, int sense, double obj_offset,
+                                          const double* c, const double* col_lower, const double* col_upper,
+                                          const double* row_lower, const double* row_upper, const int* col_start,
+                                          const int* row_index, const double* value, const double* x,
+                                          const double* ray, double* out);
 
 /* One scenario of a batch: host arrays of the base model's sizes (a pointer carries no length:
  * each array must hold n or m values); NULL keeps the base's vector (an empty vector in the

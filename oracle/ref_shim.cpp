@@ -14,6 +14,9 @@
 //                    op-by-op comparison that tests/unit/test_gpu.cpp:33-95 performs.
 //   ref_check        core::check_solution (src/core/solution_checker.cpp:61) and
 //                    certified_dual_bound (src/core/safe_bound.cpp:178).
+//   ref_bound        certified_dual_bound with the implied-bounds switch and its term counts.
+//   ref_certificate  check_infeasibility_certificate / check_unboundedness_certificate
+//                    (src/core/certificates.cpp:14, 88).
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -22,6 +25,7 @@
 #include <string>
 #include <vector>
 
+#include "core/certificates.h"
 #include "core/presolve.h"
 #include "core/safe_bound.h"
 #include "core/solution_checker.h"
@@ -109,7 +113,11 @@ int ref_solve(int m, int n, int sense, double offset, const double* c, const dou
   if (iteration_limit > 0) o.iteration_limit = iteration_limit;
   if (time_limit > 0) o.time_limit = time_limit;
   if (check_every > 0) o.termination_check_every = check_every;
-  for (int k = 0; k < n_params; ++k) o.engine_params.emplace_back(names[k], values[k]);
+  for (int k = 0; k < n_params; ++k) {
+    // "algorithm" is this shim's own switch (2 = PDLP), not an engine parameter
+    if (std::string(names[k]) == "algorithm") o.algorithm = values[k] == 2 ? Algorithm::Pdlp : Algorithm::R2hpdhg;
+    else o.engine_params.emplace_back(names[k], values[k]);
+  }
   if (warm_x) o.warm_x.assign(warm_x, warm_x + n);
   if (warm_y) o.warm_y.assign(warm_y, warm_y + m);
   const Solution s = solve(M, o);
@@ -282,6 +290,30 @@ void ref_check(int m, int n, int sense, double offset, const double* c, const do
   out[4] = r.primal_objective;
   out[5] = r.dual_objective;
   out[6] = certified_dual_bound(M, yv, true).bound;
+}
+
+// out[4] = finite, bound, unbounded_row_terms, unbounded_col_terms
+void ref_bound(int m, int n, int sense, double offset, const double* c, const double* cl, const double* cu,
+               const double* rl, const double* ru, const int* cs, const int* ri, const double* v, const double* y,
+               int use_implied, double* out) {
+  const Model M = make_model(m, n, sense, offset, c, cl, cu, rl, ru, cs, ri, v);
+  const SafeBound b = certified_dual_bound(M, std::vector<double>(y, y + m), use_implied != 0);
+  out[0] = b.finite ? 1.0 : 0.0;
+  out[1] = b.bound;
+  out[2] = b.unbounded_row_terms;
+  out[3] = b.unbounded_col_terms;
+}
+
+// kind 0: infeasibility (ray = m row multipliers); kind 1: unboundedness (x, ray: n each).
+// out[5] = present, passed, rigorous, measure, violation
+void ref_certificate(int kind, int m, int n, int sense, double offset, const double* c, const double* cl,
+                     const double* cu, const double* rl, const double* ru, const int* cs, const int* ri,
+                     const double* v, const double* x, const double* ray, double* out) {
+  const Model M = make_model(m, n, sense, offset, c, cl, cu, rl, ru, cs, ri, v);
+  const CertificateCheck k = kind == 0 ? check_infeasibility_certificate(M, std::vector<double>(ray, ray + m))
+                                       : check_unboundedness_certificate(M, std::vector<double>(x, x + n),
+                                                                         std::vector<double>(ray, ray + n));
+  out[0] = k.present, out[1] = k.passed, out[2] = k.rigorous, out[3] = k.measure, out[4] = k.violation;
 }
 
 }  // extern "C"

@@ -87,6 +87,8 @@ def lib():
         L.ref_backend_r2h_dual.argtypes = L.ref_backend_r2h_primal.argtypes
         L.ref_backend_kkt.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _D]
         L.ref_check.argtypes = model + [_D, _D, _D]
+        L.ref_bound.argtypes = model + [_D, ctypes.c_int, _D]
+        L.ref_certificate.argtypes = [ctypes.c_int] + model + [_D, _D, _D]
         L.ps26119_solve_lp.argtypes = None  # the reference's own C API, used by bench.py
         _lib = L
     return _lib
@@ -134,12 +136,14 @@ class RefSolution:
 
 
 def solve(lp, presolve=False, precision="fp64", threads=1, tol=0.0, iteration_limit=0, time_limit=0.0,
-          check_every=0, params=None, warm_x=None, warm_y=None) -> RefSolution:
-    """ps26119::solve with algorithm r2hpdhg on the CPU (reference src/core/solve.cpp:194)."""
+          check_every=0, params=None, warm_x=None, warm_y=None, algorithm="r2hpdhg") -> RefSolution:
+    """ps26119::solve with algorithm r2hpdhg (or pdlp) on the CPU (reference src/core/solve.cpp:194)."""
     L = lib()
     args, keep = _model_args(lp)
     m, n = lp.num_rows, lp.num_cols
     params = list((params or {}).items())
+    if algorithm == "pdlp":
+        params.append(("algorithm", 2.0))
     names = (ctypes.c_char_p * max(1, len(params)))(*[k.encode() for k, _ in params])
     vals = np.array([v for _, v in params] or [0.0], dtype=np.float64)
     wx = None if warm_x is None else np.ascontiguousarray(warm_x, dtype=np.float64)
@@ -195,6 +199,31 @@ def check(lp, x, y):
     del keep
     return {"passed": bool(out[0]), "primal": out[1], "dual": out[2], "gap": out[3], "primal_objective": out[4],
             "dual_objective": out[5], "certified_bound": out[6]}
+
+
+def bound(lp, y, use_implied=True):
+    """certified_dual_bound (reference src/core/safe_bound.cpp:178)."""
+    L = lib()
+    args, keep = _model_args(lp)
+    out = np.zeros(4)
+    L.ref_bound(*args, _d(np.ascontiguousarray(y, dtype=np.float64)), int(bool(use_implied)), _d(out))
+    del keep
+    return {"finite": bool(out[0]), "bound": out[1], "unbounded_row_terms": int(out[2]),
+            "unbounded_col_terms": int(out[3])}
+
+
+def certificate(lp, ray, x=None):
+    """check_infeasibility_certificate (x None) / check_unboundedness_certificate
+    (reference src/core/certificates.cpp:14, 88)."""
+    L = lib()
+    args, keep = _model_args(lp)
+    r = np.ascontiguousarray(ray, dtype=np.float64)
+    xx = np.zeros(lp.num_cols) if x is None else np.ascontiguousarray(x, dtype=np.float64)
+    out = np.zeros(5)
+    L.ref_certificate(0 if x is None else 1, *args, _d(xx), _d(r), _d(out))
+    del keep
+    return {"present": bool(out[0]), "passed": bool(out[1]), "rigorous": bool(out[2]), "measure": out[3],
+            "violation": out[4]}
 
 
 class Backend:

@@ -1,6 +1,7 @@
 // c_api.cpp — the C ABI (include/ps26119.h, include/ps26119_backend.h). Exceptions never
 // cross this boundary (reference src/core/c_api.cpp:1-304 for the five reference symbols).
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -14,6 +15,7 @@
 
 #include "../../include/ps26119.h"
 #include "../../include/ps26119_backend.h"
+#include "certify.hpp"
 #include "solver.hpp"
 
 using namespace b200;
@@ -91,6 +93,7 @@ void fill_stats(const Solution& s, long long m, long long n, long long nnz) {
   g_stats.m = m, g_stats.n = n, g_stats.nnz = nnz;
   g_stats.spmv_kernel_ms = R.iter_kernel_ms;
   g_stats.spmv_kernel_launches = R.iter_kernel_launches;
+  g_stats.teardown_seconds = R.teardown_seconds;
 }
 
 void fill(const Solution& s, ps26119_result* result) {  // c_api.cpp:58-71
@@ -113,6 +116,7 @@ int solve_host(int num_rows, int num_cols, int sense, double obj_offset, const d
                const int* row_index, const double* value, const ps26119_options* opt,
                const ps26119_engine_options* eo, ps26119_result* result, double* x, double* y, double* z,
                double* dual_ray, double* primal_ray) {
+  const auto call_t0 = std::chrono::steady_clock::now();
   if (!result) return PS26119_INVALID_ARGUMENT;
   clear(result);
   auto invalid = [&](const char* why) {
@@ -148,6 +152,7 @@ int solve_host(int num_rows, int num_cols, int sense, double obj_offset, const d
     const Solution s = solve(m, o);
     fill(s, result);
     fill_stats(s, s.engine_result.iterations > 0 ? num_rows : 0, num_cols, nnz);
+    g_stats.call_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - call_t0).count();
     auto out = [](double* dst, const std::vector<double>& v, int len) {
       if (dst && v.size() == static_cast<std::size_t>(len)) std::memcpy(dst, v.data(), sizeof(double) * len);
     };
@@ -259,6 +264,7 @@ int ps26119_solve_lp_device(int num_rows, int num_cols, int sense, double obj_of
                             const double* d_row_upper, const int* d_col_start, const int* d_row_index,
                             const double* d_value, const ps26119_options* opt, const ps26119_engine_options* eo,
                             ps26119_result* result, double* d_x, double* d_y, double* d_z, void* stream) {
+  const auto call_t0 = std::chrono::steady_clock::now();
   if (!result) return PS26119_INVALID_ARGUMENT;
   clear(result);
   auto invalid = [&](const char* why) {
@@ -320,6 +326,7 @@ int ps26119_solve_lp_device(int num_rows, int num_cols, int sense, double obj_of
     }
     fill(s, result);
     fill_stats(s, num_rows, num_cols, nnz);
+    g_stats.call_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - call_t0).count();
     return result->status;
   } catch (const std::bad_alloc&) {
     result->status = PS26119_NOT_SOLVED;
@@ -546,5 +553,75 @@ extern "C" int ps26119_solve_batch(int num_rows, int num_cols, int sense, double
     return fail(PS26119_NOT_SOLVED, "out of memory");
   } catch (const std::exception& e) {
     return fail(PS26119_NUMERICAL_ERROR, e.what());
+  }
+}
+
+namespace {
+// A validated host Model from the C arrays, or an error text.
+const char* model_from(int m, int n, int sense, double offset, const double* c, const double* cl, const double* cu,
+                       const double* rl, const double* ru, const int* cs, const int* ri, const double* v, Model& M) {
+  if (m < 0 || n < 0) return "negative dimension";
+  if (!cs) return "col_start is NULL";
+  if (n > 0 && (!c || !cl || !cu)) return "column data is NULL";
+  if (m > 0 && (!rl || !ru)) return "row bounds are NULL";
+  const int nnz = cs[n];
+  if (nnz < 0) return "col_start[n] < 0";
+  if (nnz > 0 && (!ri || !v)) return "matrix arrays are NULL";
+  M.num_rows = m, M.num_cols = n, M.sense = sense, M.obj_offset = offset;
+  M.obj.assign(c, c + n), M.col_lower.assign(cl, cl + n), M.col_upper.assign(cu, cu + n);
+  M.row_lower.assign(rl, rl + m), M.row_upper.assign(ru, ru + m);
+  M.col_start.assign(cs, cs + n + 1), M.row_index.assign(ri, ri + nnz), M.value.assign(v, v + nnz);
+  static thread_local std::string err;
+  err = M.validate();
+  return err.empty() ? nullptr : err.c_str();
+}
+}  // namespace
+
+extern "C" int ps26119_certified_bound(int num_rows, int num_cols, int sense, double obj_offset, const double* c,
+                                       const double* col_lower, const double* col_upper, const double* row_lower,
+                                       const double* row_upper, const int* col_start, const int* row_index,
+                                       const double* value, const double* y, int use_implied_bounds, double* out) {
+  if (!out || (num_rows > 0 && !y)) return PS26119_INVALID_ARGUMENT;
+  try {
+    Model M;
+    if (model_from(num_rows, num_cols, sense, obj_offset, c, col_lower, col_upper, row_lower, row_upper, col_start,
+                   row_index, value, M))
+      return PS26119_INVALID_ARGUMENT;
+    const SafeBound b = certified_dual_bound(M, std::vector<double>(y, y + num_rows), use_implied_bounds != 0);
+    out[0] = b.finite ? 1.0 : 0.0;
+    out[1] = b.bound;
+    out[2] = b.unbounded_row_terms;
+    out[3] = b.unbounded_col_terms;
+    return 0;
+  } catch (const std::bad_alloc&) {
+    return PS26119_NOT_SOLVED;
+  } catch (const std::exception&) {
+    return PS26119_NUMERICAL_ERROR;
+  }
+}
+
+extern "C" int ps26119_check_certificate(int kind, int num_rows, int num_cols, int sense, double obj_offset,
+                                         const double* c, const double* col_lower, const double* col_upper,
+                                         const double* row_lower, const double* row_upper, const int* col_start,
+                                         const int* row_index, const double* value, const double* x,
+                                         const double* ray, double* out) {
+  if (!out || (kind != 0 && kind != 1)) return PS26119_INVALID_ARGUMENT;
+  const int len = kind == 0 ? num_rows : num_cols;
+  if (len > 0 && !ray) return PS26119_INVALID_ARGUMENT;
+  if (kind == 1 && num_cols > 0 && !x) return PS26119_INVALID_ARGUMENT;
+  try {
+    Model M;
+    if (model_from(num_rows, num_cols, sense, obj_offset, c, col_lower, col_upper, row_lower, row_upper, col_start,
+                   row_index, value, M))
+      return PS26119_INVALID_ARGUMENT;
+    const std::vector<double> r(ray, ray + len);
+    const CertificateCheck k = kind == 0 ? check_infeasibility_certificate(M, r)
+                                         : check_unboundedness_certificate(M, std::vector<double>(x, x + num_cols), r);
+    out[0] = k.present, out[1] = k.passed, out[2] = k.rigorous, out[3] = k.measure, out[4] = k.violation;
+    return 0;
+  } catch (const std::bad_alloc&) {
+    return PS26119_NOT_SOLVED;
+  } catch (const std::exception&) {
+    return PS26119_NUMERICAL_ERROR;
   }
 }

@@ -9,8 +9,14 @@
 
 #include <cuda_runtime.h>
 
+#include <chrono>
 #include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <mutex>
 #include <new>
+#include <set>
+#include <vector>
 #include <stdexcept>
 #include <string>
 #include <utility>
@@ -37,8 +43,110 @@ struct CudaError : std::runtime_error {
 
 #define B200_LAUNCH_CHECK() B200_CHECK(cudaGetLastError())
 
-// Device allocation owned by the host object. cudaErrorMemoryAllocation becomes
-// std::bad_alloc, reported as NOT_SOLVED "out of memory" (reference cuda_backend.cu:74-80).
+// A process-wide cache of device blocks. Solves allocate the same large buffers again and
+// again; cudaMalloc / cudaFree of gigabytes cost a device-wide synchronisation and, measured on
+// B200, from a few ms up to over a second per solve. Released blocks are kept (per device, by
+// size class: powers of two up to 1 MiB, multiples of 2 MiB above) and handed out again; at
+// most PS26119_DEVICE_CACHE_MB (default 8192) MiB stay cached, the rest is freed. Every
+// release in this library follows a synchronisation of the stream that used the block; as a
+// safety net the first reuse after a release synchronises the device once. On an allocation
+// failure the device's cached blocks are freed and the allocation is retried.
+class DeviceBlockCache {
+ public:
+  static DeviceBlockCache& instance() {
+    static DeviceBlockCache* c = new DeviceBlockCache();  // never destroyed: no CUDA calls at exit
+    return *c;
+  }
+  static std::size_t size_class(std::size_t bytes) {
+    if (bytes <= (1u << 20)) {
+      std::size_t c = 512;
+      while (c < bytes) c <<= 1;
+      return c;
+    }
+    const std::size_t g = 2u << 20;
+    return (bytes + g - 1) / g * g;
+  }
+  void* acquire(std::size_t bytes) {  // bytes: a size class
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) dev = 0;
+    {
+      std::lock_guard<std::mutex> lock(mu_);
+      for (std::size_t k = 0; k < free_.size(); ++k)
+        if (free_[k].device == dev && free_[k].bytes == bytes) {
+          void* p = free_[k].p;
+          free_[k] = free_.back();
+          free_.pop_back();
+          cached_ -= bytes;
+          if (dirty_.count(dev)) {
+            dirty_.erase(dev);
+            (void)cudaDeviceSynchronize();
+          }
+          return p;
+        }
+    }
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e == cudaErrorMemoryAllocation) {
+      (void)cudaGetLastError();
+      trim(dev);
+      e = cudaMalloc(&p, bytes);
+    }
+    if (e == cudaErrorMemoryAllocation) {
+      (void)cudaGetLastError();
+      throw std::bad_alloc();
+    }
+    if (e != cudaSuccess) throw CudaError(std::string("CUDA error: ") + cudaGetErrorString(e) + " in cudaMalloc");
+    return p;
+  }
+  void release(void* p, std::size_t bytes, int dev) {
+    {
+      std::lock_guard<std::mutex> lock(mu_);
+      if (cached_ + bytes <= limit_) {
+        free_.push_back({dev, bytes, p});
+        cached_ += bytes;
+        dirty_.insert(dev);
+        return;
+      }
+    }
+    cudaFree(p);  // never throws from a destructor
+  }
+  void trim(int dev) {  // frees this device's cached blocks
+    std::vector<void*> drop;
+    {
+      std::lock_guard<std::mutex> lock(mu_);
+      for (std::size_t k = 0; k < free_.size();)
+        if (free_[k].device == dev) {
+          drop.push_back(free_[k].p);
+          cached_ -= free_[k].bytes;
+          free_[k] = free_.back();
+          free_.pop_back();
+        } else {
+          ++k;
+        }
+    }
+    if (!drop.empty()) (void)cudaDeviceSynchronize();
+    for (void* p : drop) cudaFree(p);
+  }
+
+ private:
+  DeviceBlockCache() {
+    const char* env = std::getenv("PS26119_DEVICE_CACHE_MB");
+    const long long mb = env ? std::atoll(env) : 8192;
+    limit_ = mb > 0 ? static_cast<std::size_t>(mb) << 20 : 0;
+  }
+  struct Block {
+    int device;
+    std::size_t bytes;
+    void* p;
+  };
+  std::mutex mu_;
+  std::vector<Block> free_;
+  std::set<int> dirty_;
+  std::size_t cached_ = 0, limit_ = 0;
+};
+
+// Device allocation owned by the host object (through DeviceBlockCache). cudaErrorMemoryAllocation
+// becomes std::bad_alloc, reported as NOT_SOLVED "out of memory" (reference cuda_backend.cu:74-80).
 template <class T>
 class DevBuf {
  public:
@@ -46,12 +154,14 @@ class DevBuf {
   explicit DevBuf(std::size_t n) { alloc(n); }
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
-  DevBuf(DevBuf&& o) noexcept : p_(o.p_), n_(o.n_) { o.p_ = nullptr, o.n_ = 0; }
+  DevBuf(DevBuf&& o) noexcept : p_(o.p_), n_(o.n_), bytes_(o.bytes_), dev_(o.dev_) {
+    o.p_ = nullptr, o.n_ = 0, o.bytes_ = 0;
+  }
   DevBuf& operator=(DevBuf&& o) noexcept {
     if (this != &o) {
       release();
-      p_ = o.p_, n_ = o.n_;
-      o.p_ = nullptr, o.n_ = 0;
+      p_ = o.p_, n_ = o.n_, bytes_ = o.bytes_, dev_ = o.dev_;
+      o.p_ = nullptr, o.n_ = 0, o.bytes_ = 0;
     }
     return *this;
   }
@@ -62,11 +172,11 @@ class DevBuf {
   // element; the padding keeps that inside the allocation.
   void alloc(std::size_t n) {
     release();
-    const std::size_t bytes = n * sizeof(T) + 64;
-    void* p = nullptr;
-    B200_CHECK(cudaMalloc(&p, bytes));
-    p_ = static_cast<T*>(p);
+    const std::size_t bytes = DeviceBlockCache::size_class(n * sizeof(T) + 64);
+    if (cudaGetDevice(&dev_) != cudaSuccess) dev_ = 0;
+    p_ = static_cast<T*>(DeviceBlockCache::instance().acquire(bytes));
     n_ = n;
+    bytes_ = bytes;
   }
   void ensure(std::size_t n) {
     if (n_ < n || !p_) alloc(n);
@@ -84,12 +194,14 @@ class DevBuf {
 
  private:
   void release() {
-    if (p_) cudaFree(p_);  // never throws from a destructor
+    if (p_) DeviceBlockCache::instance().release(p_, bytes_, dev_);  // never throws
     p_ = nullptr;
     n_ = 0;
+    bytes_ = 0;
   }
   T* p_ = nullptr;
-  std::size_t n_ = 0;
+  std::size_t n_ = 0, bytes_ = 0;
+  int dev_ = 0;
 };
 
 // Page-locked host memory for the per-check status transfers.
@@ -100,7 +212,14 @@ class PinnedBuf {
   PinnedBuf(const PinnedBuf&) = delete;
   PinnedBuf& operator=(const PinnedBuf&) = delete;
   ~PinnedBuf() {
+#ifdef B200_TEARDOWN_TRACE
+    const auto t0 = std::chrono::steady_clock::now();
+#endif
     if (p_) cudaFreeHost(p_);
+#ifdef B200_TEARDOWN_TRACE
+    std::fprintf(stderr, "teardown: cudaFreeHost %.1f ms\n",
+                 std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
+#endif
   }
   void alloc(std::size_t n) {
     if (p_) cudaFreeHost(p_);

@@ -20,6 +20,7 @@
 #include <cmath>
 #include <cstdio>
 #include <limits>
+#include <memory>
 #include <string>
 
 #include "checks.cuh"
@@ -103,16 +104,31 @@ class Engine {
     for (auto& e : ev_) B200_CHECK(cudaEventCreate(&e));
   }
   ~Engine() {
+#ifdef B200_TEARDOWN_TRACE
+    const auto tt0 = std::chrono::steady_clock::now();
+#endif
     for (auto& g : g_epoch_)
       if (g) cudaGraphExecDestroy(g);
     for (auto& row : g_check_)
       for (auto& g : row)
         if (g) cudaGraphExecDestroy(g);
+    for (auto& row : g_pdlp_)
+      for (auto& g : row)
+        if (g) cudaGraphExecDestroy(g);
+    for (auto& a : g_pdlp_chk_)
+      for (auto& row : a)
+        for (auto& g : row)
+          if (g) cudaGraphExecDestroy(g);
     for (auto& e : ev_)
       if (e) cudaEventDestroy(e);
+#ifdef B200_TEARDOWN_TRACE
+    std::fprintf(stderr, "teardown: graphs+events %.1f ms\n",
+                 std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tt0).count());
+#endif
   }
 
   EngineResult run(const DeviceOutputs& out);
+  EngineResult run_pdlp(const DeviceOutputs& out);
 
  private:
   using clock = std::chrono::steady_clock;
@@ -126,6 +142,7 @@ class Engine {
   void launch_kkt_original();
   template <class T> void launch_ray(const T* dx, const T* dy, double* r, double* d, int drift);
   Kkt read_kkt(const double* h) const;
+  Status ray_verdict(const double* h, int which, const Kkt& k, std::string& why) const;
   void setup();
   void build_plans();
   template <class T> void init_iterates();
@@ -137,6 +154,14 @@ class Engine {
               const DeviceOutputs& out, int ray_test);
   template <class T> void finish_t(EngineResult& R, Status st, bool use_hat, long long it, const std::string& msg,
                                    const DeviceOutputs& out, int ray_test);
+  template <class T> void finish_p(EngineResult& R, Status st, const T* xs, const T* ys, long long it,
+                                   const std::string& msg, const DeviceOutputs& out, int ray_test);
+  // PDLP-style restarted averaged PDHG on the same kernels (pdlp.cpp:9-126)
+  template <class T> void capture_pdlp_epoch(int phase);
+  template <class T> void capture_pdlp_check(int phase, int variant);
+  template <class T> void pdlp_restart(int cur, bool use_avg);
+  template <class T> void pdlp_distances(int cur, bool use_avg, double& dx, double& dy);
+  void promote_pdlp();
   void sync_results() {
     B200_CHECK(cudaMemcpyAsync(hres_.get(), res_.get(), kNumSlots * sizeof(double), cudaMemcpyDeviceToHost, st_));
     B200_CHECK(cudaStreamSynchronize(st_));
@@ -160,6 +185,12 @@ class Engine {
   SumPlan plan_r0_, plan_res_, plan_kkt_, plan_ray1_, plan_ray2_, plan_obj_, plan_chk_;
   cudaGraphExec_t g_epoch_[2] = {nullptr, nullptr};
   cudaGraphExec_t g_check_[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
+  cudaGraphExec_t g_pdlp_[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};         // [precision][phase]
+  cudaGraphExec_t g_pdlp_chk_[2][2][3] = {};                                        // [precision][phase][variant]
+  long long pdlp_kernels_[2][2] = {}, pdlp_chk_kernels_[2][2][3] = {};
+  DevBuf<double> res2_;
+  PinnedBuf<double> hres2_;
+  SumPlan plan_dist_;
   long long epoch_kernels_[2] = {0, 0}, check_kernels_[2][3] = {{0, 0, 0}, {0, 0, 0}};
   cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};
   long long kernels_ = 0;  // counted launches (graph kernel nodes per replay)
@@ -528,11 +559,17 @@ void Engine::finish(EngineResult& R, Status st, bool use_hat, long long it, cons
 template <class T>
 void Engine::finish_t(EngineResult& R, Status status, bool use_hat, long long it, const std::string& msg,
                       const DeviceOutputs& out, int ray_test) {
-  const auto tf = clock::now();
   IterVecs<T>& v = vecs<T>();
+  finish_p<T>(R, status, use_hat ? v.xh.get() : v.x.get(), use_hat ? v.yh.get() : v.y.get(), it, msg, out, ray_test);
+}
+
+template <class T>
+void Engine::finish_p(EngineResult& R, Status status, const T* xs, const T* ys, long long it, const std::string& msg,
+                      const DeviceOutputs& out, int ray_test) {
+  const auto tf = clock::now();
   const int m = M_.m, n = M_.n;
   clear_maxima();
-  launch_kkt_scaled<T>(use_hat ? v.xh.get() : v.x.get(), use_hat ? v.yh.get() : v.y.get());
+  launch_kkt_scaled<T>(xs, ys);
   // objective = offset + Σ c_j x_j (Model::objective_value)
   k_obj_terms<<<grid_for(n), kBlock, 0, st_>>>(n, M_.c, xo_.get(), objt_.get());
   B200_LAUNCH_CHECK();
@@ -598,6 +635,42 @@ void Engine::finish_t(EngineResult& R, Status status, bool use_hat, long long it
   const bool finite_pt = std::isfinite(pobj) && std::isfinite(dobj) && std::isfinite(R.check_primal);
   R.check = finite_pt && R.check_primal <= kVerifyPrimal && R.check_dual <= kVerifyDual && R.check_gap <= kVerifyGap;
   R.finish_seconds = std::chrono::duration<double>(clock::now() - tf).count();
+}
+
+// EngineContext::ray_test on the device sums of one candidate direction (engine.cpp:82-155):
+// which = 1 the last step's Δ, 2 the drift since the restart anchor; k = the current KKT.
+Status Engine::ray_verdict(const double* h, int which, const Kkt& k, std::string& why) const {
+  const int s_rmax = which == 2 ? kMaxRmax2 : kMaxRmax, s_dabs = which == 2 ? kMaxDabs2 : kMaxDabs;
+  const int s_dviol = which == 2 ? kMaxDviol2 : kMaxDviol, s_pviol = which == 2 ? kMaxPviol2 : kMaxPviol;
+  const double obj = h[which == 2 ? kRayObj2 : kRayObj], mag = h[which == 2 ? kRayMag2 : kRayMag];
+  const double cd = h[which == 2 ? kRayCd2 : kRayCd], cmag = h[which == 2 ? kRayCmag2 : kRayCmag];
+  const double rmax = slot_max(h, s_rmax), dmax = slot_max(h, s_dabs);
+  bool pinf = false, dinf = false;
+  double dro = 0, drv = 0, pro = 0, prv = 0;
+  if (rmax > 0) {
+    const double viol = slot_max(h, s_dviol), scale = std_max(rmax, viol);
+    dro = obj / scale, drv = viol / scale;
+    pinf = dro > 0 && obj > kFirstOrderInfeasible * mag && drv <= kFirstOrderInfeasible * dro;
+  }
+  if (dmax > 0) {
+    const double viol = slot_max(h, s_pviol), scale = std_max(dmax, viol);
+    pro = cd / scale, prv = viol / scale;
+    dinf = pro < 0 && -cd > kFirstOrderInfeasible * cmag && prv <= kFirstOrderInfeasible * -pro;
+  }
+  char buf[200];
+  if (pinf) {
+    std::snprintf(buf, sizeof buf, "primal infeasible: dual ray certificate (objective %f, violation %f)", dro, drv);
+    why = buf;
+    return Status::Infeasible;
+  }
+  if (dinf) {
+    const bool feasible = k.rel_primal() <= kVerifyPrimal && k.primal_max_rel <= kVerifyPrimal;
+    std::snprintf(buf, sizeof buf, "unbounded: primal ray certificate (c'd %f, violation %f)%s", pro, prv,
+                  feasible ? " at a primal-feasible iterate" : "; iterate not primal-feasible yet");
+    why = buf;
+    return Status::Unbounded;
+  }
+  return Status::NotSolved;
 }
 
 EngineResult Engine::run(const DeviceOutputs& out) {
@@ -696,39 +769,7 @@ EngineResult Engine::run(const DeviceOutputs& out) {
     if (it >= o_.iteration_limit) return done(Status::IterationLimit, true, it, msg, 0);
     if (elapsed() > o_.time_limit) return done(Status::TimeLimit, true, it, msg, 0);
     if (variant >= 1) {  // EngineContext::check_infeasibility + ray_test (engine.cpp:82-184)
-      auto test = [&](int which, std::string& why) {
-        const int s_rmax = which == 2 ? kMaxRmax2 : kMaxRmax, s_dabs = which == 2 ? kMaxDabs2 : kMaxDabs;
-        const int s_dviol = which == 2 ? kMaxDviol2 : kMaxDviol, s_pviol = which == 2 ? kMaxPviol2 : kMaxPviol;
-        const double obj = h[which == 2 ? kRayObj2 : kRayObj], mag = h[which == 2 ? kRayMag2 : kRayMag];
-        const double cd = h[which == 2 ? kRayCd2 : kRayCd], cmag = h[which == 2 ? kRayCmag2 : kRayCmag];
-        const double rmax = slot_max(h, s_rmax), dmax = slot_max(h, s_dabs);
-        bool pinf = false, dinf = false;
-        double dro = 0, drv = 0, pro = 0, prv = 0;
-        if (rmax > 0) {
-          const double viol = slot_max(h, s_dviol), scale = std_max(rmax, viol);
-          dro = obj / scale, drv = viol / scale;
-          pinf = dro > 0 && obj > kFirstOrderInfeasible * mag && drv <= kFirstOrderInfeasible * dro;
-        }
-        if (dmax > 0) {
-          const double viol = slot_max(h, s_pviol), scale = std_max(dmax, viol);
-          pro = cd / scale, prv = viol / scale;
-          dinf = pro < 0 && -cd > kFirstOrderInfeasible * cmag && prv <= kFirstOrderInfeasible * -pro;
-        }
-        char buf[200];
-        if (pinf) {
-          std::snprintf(buf, sizeof buf, "primal infeasible: dual ray certificate (objective %f, violation %f)", dro, drv);
-          why = buf;
-          return Status::Infeasible;
-        }
-        if (dinf) {
-          const bool feasible = k.rel_primal() <= kVerifyPrimal && k.primal_max_rel <= kVerifyPrimal;
-          std::snprintf(buf, sizeof buf, "unbounded: primal ray certificate (c'd %f, violation %f)%s", pro, prv,
-                        feasible ? " at a primal-feasible iterate" : "; iterate not primal-feasible yet");
-          why = buf;
-          return Status::Unbounded;
-        }
-        return Status::NotSolved;
-      };
+      auto test = [&](int which, std::string& why) { return ray_verdict(h, which, k, why); };
       std::string why;
       int which = 1;
       Status s = test(1, why);
@@ -790,6 +831,305 @@ EngineResult Engine::run(const DeviceOutputs& out) {
   }
 }
 
+
+// ============================================================================ PDLP
+// Restarted averaged PDHG (reference src/pdhg/pdlp.cpp:9-126) on the same fused kernels. The
+// current and next iterates alternate between two buffers (x / x̂ storage, y / ŷ storage): an
+// epoch graph is captured per starting phase. xa / ya (the running averages) live in the Δx / Δy
+// buffers, x̄ in x̄'s. A check evaluates the KKT statistics of the current point and of the
+// average and, after 4K iterations, the ray tests on z_k − z_{k−1} (and the drift z − z0).
+template <class T>
+__global__ void k_dist_terms(long long n, const T* a, const T* b, double* t) {  // (a − b)² in fp64
+  B200_FOR(i, n) {
+    const double d = static_cast<double>(a[i]) - static_cast<double>(b[i]);
+    t[i] = d * d;
+  }
+}
+
+template <class T>
+void Engine::capture_pdlp_epoch(int phase) {
+  const int idx = std::is_same<T, float>::value ? 1 : 0;
+  if (g_pdlp_[idx][phase]) return;
+  IterVecs<T>& v = vecs<T>();
+  const int m = M_.m, n = M_.n, K = o_.check_every;
+  const StepParams* P = params_.get();
+  cudaGraph_t g;
+  slab_prepare<T, EpiPdlpPrimal<T>, B200_STAGE_TMA != 0>();
+  slab_prepare<T, EpiPdlpDual<T>, B200_STAGE_TMA != 0>();
+  capturing_ = true;
+  capture_count_ = 0;
+  B200_CHECK(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
+  B200_CHECK(cudaEventRecordWithFlags(ev_[0], st_, cudaEventRecordExternal));
+  for (int s = 0; s < K; ++s) {
+    const bool odd = ((phase + s) & 1) != 0;
+    T* xc = odd ? v.xh.get() : v.x.get();
+    T* xn = odd ? v.x.get() : v.xh.get();
+    T* yc = odd ? v.yh.get() : v.y.get();
+    T* yn = odd ? v.y.get() : v.yh.get();
+    EpiPdlpPrimal<T> ep{xc, sp_.c<T>(), sp_.l<T>(), sp_.u<T>(), xn, v.xb.get(), v.dx.get(), P, s};
+    launch_slab_tma<T>(n, M_.col_start, sp_.t_ri.get(), sp_.At_val<T>(), yc, ep, st_);
+    EpiPdlpDual<T> ed{yc, sp_.rl<T>(), sp_.ru<T>(), yn, v.dy.get(), P, s};
+    launch_slab_tma<T>(m, sp_.a_rp.get(), sp_.a_col.get(), sp_.A_val<T>(), v.xb.get(), ed, st_);
+    capture_count_ += 2;
+  }
+  B200_CHECK(cudaEventRecordWithFlags(ev_[1], st_, cudaEventRecordExternal));
+  B200_CHECK(cudaEventRecordWithFlags(ev_[2], st_, cudaEventRecordExternal));
+  B200_CHECK(cudaEventRecordWithFlags(ev_[3], st_, cudaEventRecordExternal));
+  const cudaError_t e = cudaStreamEndCapture(st_, &g);
+  capturing_ = false;
+  B200_CHECK(e);
+  B200_CHECK(cudaGraphInstantiate(&g_pdlp_[idx][phase], g, 0));
+  cudaGraphDestroy(g);
+  pdlp_kernels_[idx][phase] = capture_count_;
+}
+
+template <class T>
+void Engine::capture_pdlp_check(int phase, int variant) {
+  const int idx = std::is_same<T, float>::value ? 1 : 0;
+  if (g_pdlp_chk_[idx][phase][variant]) return;
+  IterVecs<T>& v = vecs<T>();
+  const long long m = M_.m, n = M_.n;
+  T* xc = phase ? v.xh.get() : v.x.get();
+  T* xp = phase ? v.x.get() : v.xh.get();  // z_{k−1}, scratch for the ray directions
+  T* yc = phase ? v.yh.get() : v.y.get();
+  T* yp = phase ? v.y.get() : v.yh.get();
+  cudaGraph_t g;
+  slab_prepare<double, EpiKktRows, B200_STAGE_TMA != 0>();
+  slab_prepare<double, EpiKktCols, false>();
+  slab_prepare<double, EpiRayRows, B200_STAGE_TMA != 0>();
+  capturing_ = true;
+  capture_count_ = 0;
+  B200_CHECK(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
+  clear_maxima();
+  launch_kkt_scaled<T>(xc, yc);  // KKT of the current point -> res2_
+  B200_CHECK(cudaMemcpyAsync(res2_.get(), res_.get(), kNumSlots * sizeof(double), cudaMemcpyDeviceToDevice, st_));
+  clear_maxima();
+  launch_kkt_scaled<T>(v.dx.get(), v.dy.get());  // KKT of the average -> res_
+  if (variant >= 1) {  // Δ = z_k − z_{k−1}: axpby(1, x, −1, x_prev) (pdlp.cpp:83-85)
+    k_axpby<T><<<grid_for(n), kBlock, 0, st_>>>(n, static_cast<T>(1.0), xc, static_cast<T>(-1.0), xp);
+    k_axpby<T><<<grid_for(m), kBlock, 0, st_>>>(m, static_cast<T>(1.0), yc, static_cast<T>(-1.0), yp);
+    B200_LAUNCH_CHECK();
+    capture_count_ += 2;
+    launch_ray<T>(xp, yp, r1_.get(), d1_.get(), 0);
+  }
+  if (variant == 2) {  // the drift z − z0: copy + axpby(−1, x0, 1, ·) (pdlp.cpp:89-93)
+    k_diff<T><<<grid_for(n), kBlock, 0, st_>>>(n, xc, v.x0.get(), xp);
+    k_diff<T><<<grid_for(m), kBlock, 0, st_>>>(m, yc, v.y0.get(), yp);
+    B200_LAUNCH_CHECK();
+    capture_count_ += 2;
+    launch_ray<T>(xp, yp, r2_.get(), d2_.get(), 1);
+  }
+  B200_CHECK(cudaMemcpyAsync(hres_.get(), res_.get(), kNumSlots * sizeof(double), cudaMemcpyDeviceToHost, st_));
+  B200_CHECK(cudaMemcpyAsync(hres2_.get(), res2_.get(), kNumSlots * sizeof(double), cudaMemcpyDeviceToHost, st_));
+  const cudaError_t e = cudaStreamEndCapture(st_, &g);
+  capturing_ = false;
+  B200_CHECK(e);
+  B200_CHECK(cudaGraphInstantiate(&g_pdlp_chk_[idx][phase][variant], g, 0));
+  cudaGraphDestroy(g);
+  pdlp_chk_kernels_[idx][phase][variant] = capture_count_;
+}
+
+// ‖c_x − x0‖, ‖c_y − y0‖ (Backend::diff_norm2: la::parallel_sum order) for the chosen point.
+template <class T>
+void Engine::pdlp_distances(int cur, bool use_avg, double& dx, double& dy) {
+  IterVecs<T>& v = vecs<T>();
+  const long long m = M_.m, n = M_.n;
+  const T* cx = use_avg ? v.dx.get() : (cur ? v.xh.get() : v.x.get());
+  const T* cy = use_avg ? v.dy.get() : (cur ? v.yh.get() : v.y.get());
+  k_dist_terms<T><<<grid_for(n), kBlock, 0, st_>>>(n, cx, v.x0.get(), rt_.get());
+  k_dist_terms<T><<<grid_for(m), kBlock, 0, st_>>>(m, cy, v.y0.get(), rt_.get() + 2 * n);
+  B200_LAUNCH_CHECK();
+  plan_dist_.launch(st_);
+  kernels_ += 2 + plan_dist_.kernel_count();
+  sync_results();
+  dx = std::sqrt(hres_[kPx]);
+  dy = std::sqrt(hres_[kPy]);
+}
+
+// Restart from the chosen point: x ← c_x, y ← c_y, then x0 = xa = x, y0 = ya = y (pdlp.cpp:113-120).
+template <class T>
+void Engine::pdlp_restart(int cur, bool use_avg) {
+  IterVecs<T>& v = vecs<T>();
+  const std::size_t nb = static_cast<std::size_t>(M_.n) * sizeof(T), mb = static_cast<std::size_t>(M_.m) * sizeof(T);
+  T* xc = cur ? v.xh.get() : v.x.get();
+  T* yc = cur ? v.yh.get() : v.y.get();
+  if (use_avg) {
+    B200_CHECK(cudaMemcpyAsync(xc, v.dx.get(), nb, cudaMemcpyDeviceToDevice, st_));
+    B200_CHECK(cudaMemcpyAsync(yc, v.dy.get(), mb, cudaMemcpyDeviceToDevice, st_));
+  }
+  B200_CHECK(cudaMemcpyAsync(v.x0.get(), xc, nb, cudaMemcpyDeviceToDevice, st_));
+  B200_CHECK(cudaMemcpyAsync(v.y0.get(), yc, mb, cudaMemcpyDeviceToDevice, st_));
+  B200_CHECK(cudaMemcpyAsync(v.dx.get(), xc, nb, cudaMemcpyDeviceToDevice, st_));
+  B200_CHECK(cudaMemcpyAsync(v.dy.get(), yc, mb, cudaMemcpyDeviceToDevice, st_));
+}
+
+// set_precision(Fp64) for PDLP: every vector that carries state is converted.
+void Engine::promote_pdlp() {
+  const long long m = M_.m, n = M_.n;
+  DevBuf<float>* fs[] = {&vf_.x, &vf_.x0, &vf_.xh, &vf_.xb, &vf_.dx, &vf_.y, &vf_.y0, &vf_.yh, &vf_.yb, &vf_.dy};
+  DevBuf<double>* ds[] = {&vd_.x, &vd_.x0, &vd_.xh, &vd_.xb, &vd_.dx, &vd_.y, &vd_.y0, &vd_.yh, &vd_.yb, &vd_.dy};
+  for (int q = 0; q < 10; ++q) {
+    const long long len = q < 5 ? n : m;
+    k_convert<double, float><<<grid_for(len), kBlock, 0, st_>>>(len, fs[q]->get(), ds[q]->get());
+  }
+  B200_LAUNCH_CHECK();
+  kernels_ += 10;
+  mixed_now_ = false;
+}
+
+EngineResult Engine::run_pdlp(const DeviceOutputs& out) {
+  t0_ = clock::now();
+  EngineResult R;
+  setup();
+  const long long mm = M_.m, nn = M_.n;
+  res2_.alloc(kNumSlots);
+  hres2_.alloc(kNumSlots);
+  plan_dist_.add(rt_.get(), 0, nn, 0.0, SumOrder::kChunk64, res_.get() + kPx);
+  plan_dist_.add(rt_.get() + 2 * nn, 0, mm, 0.0, SumOrder::kChunk64, res_.get() + kPy);
+  plan_dist_.build(o_.exact, nullptr);
+  mixed_now_ = o_.mixed;
+  double omega = initial_primal_weight();
+  if (mixed_now_) init_iterates<float>();
+  else init_iterates<double>();
+  const bool warm = apply_warm_start();
+  primal_weight_ = omega;
+  std::string msg = warm ? "warm start" : "";
+  const int K = o_.check_every;
+  R.setup_seconds = elapsed();
+  int cur = 0;  // 0: the current point is in the x / y buffers, 1: in the x̂ / ŷ buffers
+  auto point = [&](bool avg, auto tag) {
+    using T = decltype(tag);
+    IterVecs<T>& v = vecs<T>();
+    return std::make_pair<const T*, const T*>(avg ? v.dx.get() : (cur ? v.xh.get() : v.x.get()),
+                                             avg ? v.dy.get() : (cur ? v.yh.get() : v.y.get()));
+  };
+  auto done = [&](Status s, bool avg, long long it, const std::string& m, int ray) {
+    R.loop_seconds = elapsed() - R.setup_seconds;
+    if (mixed_now_) {
+      const auto p = point(avg, 0.0f);
+      finish_p<float>(R, s, p.first, p.second, it, m, out, ray);
+    } else {
+      const auto p = point(avg, 0.0);
+      finish_p<double>(R, s, p.first, p.second, it, m, out, ray);
+    }
+    R.kernel_launches = kernels_;
+    R.iter_kernel_ms = iter_ms_;
+    R.iter_kernel_launches = iter_launches_;
+    R.seconds = elapsed();
+    return R;
+  };
+  auto kkt_now = [&](bool avg) {
+    clear_maxima();
+    if (mixed_now_) {
+      const auto p = point(avg, 0.0f);
+      launch_kkt_scaled<float>(p.first, p.second);
+    } else {
+      const auto p = point(avg, 0.0);
+      launch_kkt_scaled<double>(p.first, p.second);
+    }
+    sync_results();
+    return read_kkt(hres_.get());
+  };
+  if (warm) {  // the warm point may already be good enough (pdlp.cpp:37-40)
+    const Kkt kw = kkt_now(false);
+    if (fast_it_ < 0 && kw.rel_kkt() <= kFirstOrderFast) fast_it_ = 0;
+    if (kw.finite() && kw.converged(o_.tolerance)) return done(Status::Optimal, false, 0, "warm start already optimal", 0);
+  }
+  if (mixed_now_) pdlp_restart<float>(cur, false);  // x0 = xa = x, y0 = ya = y
+  else pdlp_restart<double>(cur, false);
+  const Kkt k0 = kkt_now(false);
+  if (fast_it_ < 0 && k0.rel_kkt() <= kFirstOrderFast) fast_it_ = 0;
+  double restart_kkt = k0.rel_kkt(), last_candidate = 1e300;
+  long long it = 0, inner = 0;
+  StepParams& hp = *hparams_.get();
+  for (;;) {
+    hp.tau = eta_ / omega;
+    hp.sigma = eta_ * omega;
+    hp.rho = 1.0;
+    hp.inner0 = inner;
+    hp.K = K;
+    hp.done = 0;
+    hp.skip_r0 = 1;
+    B200_CHECK(cudaMemcpyAsync(params_.get(), &hp, sizeof(StepParams), cudaMemcpyHostToDevice, st_));
+    const int pidx = mixed_now_ ? 1 : 0;
+    if (mixed_now_) capture_pdlp_epoch<float>(cur);
+    else capture_pdlp_epoch<double>(cur);
+    B200_CHECK(cudaGraphLaunch(g_pdlp_[pidx][cur], st_));
+    kernels_ += pdlp_kernels_[pidx][cur];
+    it += K;
+    inner += K;
+    cur = (cur + K) & 1;
+    const int variant = it >= 4LL * K ? (((it / K) % 4 == 0) ? 2 : 1) : 0;
+    if (mixed_now_) capture_pdlp_check<float>(cur, variant);
+    else capture_pdlp_check<double>(cur, variant);
+    B200_CHECK(cudaGraphLaunch(g_pdlp_chk_[pidx][cur][variant], st_));
+    kernels_ += pdlp_chk_kernels_[pidx][cur][variant];
+    B200_CHECK(cudaStreamSynchronize(st_));
+    ++R.checks;
+    {
+      float a = 0;
+      B200_CHECK(cudaEventElapsedTime(&a, ev_[0], ev_[1]));
+      iter_ms_ += a;
+      iter_launches_ += 2LL * K;
+    }
+    const Kkt kc = read_kkt(hres2_.get()), ka = read_kkt(hres_.get());
+    const bool use_avg = ka.finite() && ka.rel_kkt() < kc.rel_kkt();
+    const Kkt& kk = use_avg ? ka : kc;
+    if (o_.verbosity >= 2)
+      std::fprintf(stderr, "pdlp-b200 it %8lld  t %7.2fs  pobj %+.10e  dobj %+.10e  rp %.2e  rd %.2e  gap %.2e  %s%s\n",
+                   it, elapsed(), kk.primal_obj, kk.dual_obj, kk.rel_primal(), kk.rel_dual(), kk.rel_gap(),
+                   mixed_now_ ? "fp32" : "fp64", use_avg ? " avg" : "");
+    if (!kk.finite()) return done(Status::NumericalError, false, it, "non-finite KKT statistics", 0);
+    if (fast_it_ < 0 && kk.rel_kkt() <= kFirstOrderFast) fast_it_ = it;
+    if (kk.converged(o_.tolerance)) return done(Status::Optimal, use_avg, it, msg, 0);
+    if (it >= o_.iteration_limit) return done(Status::IterationLimit, use_avg, it, msg, 0);
+    if (elapsed() > o_.time_limit) return done(Status::TimeLimit, use_avg, it, msg, 0);
+    if (variant >= 1) {  // check_infeasibility on Δ, then the drift (pdlp.cpp:82-98)
+      const double* h = hres_.get();
+      std::string why;
+      int which = 1;
+      Status st = ray_verdict(h, 1, kc, why);
+      if (st == Status::NotSolved && inner >= K && variant == 2) {
+        which = 2;
+        st = ray_verdict(h, 2, kc, why);
+        if (st != Status::NotSolved) why += " (drift since the restart anchor)";
+      }
+      if (st != Status::NotSolved) return done(st, false, it, why, which);
+    }
+    const double e = kk.rel_kkt();
+    bool promoted = false;  // PrecisionPolicy::on_check (engine.cpp:61-79)
+    if (o_.mixed && mixed_now_) {
+      if (e < 0.9 * pol_best_) pol_best_ = e, pol_since_best_ = 0;
+      else ++pol_since_best_;
+      const bool reached = e <= kMixedPrecisionSwitch && o_.tolerance < kMixedPrecisionSwitch;
+      if (reached || pol_since_best_ >= 10) {
+        promote_pdlp();
+        switch_it_ = it;
+        promoted = true;
+        msg += std::string(msg.empty() ? "" : "; ") + "fp32 -> fp64 at iteration " + std::to_string(it);
+      }
+    }
+    const bool restart_now = promoted || e <= 0.2 * restart_kkt ||
+                             (e <= o_.pdlp_restart_necessary * restart_kkt && e > last_candidate) ||
+                             static_cast<double>(inner) >= 0.36 * static_cast<double>(it);
+    last_candidate = e;
+    if (!restart_now) continue;
+    double dx = 0, dy = 0;
+    if (mixed_now_) pdlp_distances<float>(cur, use_avg, dx, dy);
+    else pdlp_distances<double>(cur, use_avg, dx, dy);
+    if (dx > 1e-10 && dy > 1e-10) {
+      const double th = o_.pdlp_primal_weight_smoothing;
+      omega = std::exp(th * std::log(dy / dx) + (1.0 - th) * std::log(omega));
+      primal_weight_ = omega;
+    }
+    if (mixed_now_) pdlp_restart<float>(cur, use_avg);
+    else pdlp_restart<double>(cur, use_avg);
+    ++R.restarts;
+    inner = 0;
+    restart_kkt = e;
+    last_candidate = 1e300;
+  }
+}
 }  // namespace
 
 EngineResult run_engine(const DeviceModel& M, const EngineOptions& opt, const DeviceOutputs& out, void* stream) {
@@ -810,8 +1150,14 @@ EngineResult run_engine(const DeviceModel& M, const EngineOptions& opt, const De
     }
   } guard{st, own};
   const unsigned timeouts = stage_timeouts();
-  Engine e(M, opt, st);
-  EngineResult R = e.run(out);
+  EngineResult R;
+  {
+    auto e = std::make_unique<Engine>(M, opt, st);
+    R = opt.pdlp ? e->run_pdlp(out) : e->run(out);
+    const auto t = std::chrono::steady_clock::now();
+    e.reset();
+    R.teardown_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t).count();
+  }
   if (stage_timeouts() != timeouts) throw CudaError("a shared-memory staging wait timed out on the device");
   return R;
 }

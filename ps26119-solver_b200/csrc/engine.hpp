@@ -39,6 +39,9 @@ struct EngineOptions {
   double restart_sufficient = 0.2, restart_necessary = 0.5, restart_artificial = 0.36;
   double pid_kp = 0.99, pid_ki = 0.01, pid_kd = 0.0, pid_integral_decay = 0.3;
   double pid_max_log_step = 2.302585092994046;
+  // PDLP-style restarted averaged PDHG instead of r²HPDHG (pdlp.cpp; engine.h:44-46 defaults)
+  bool pdlp = false;
+  double pdlp_restart_necessary = 0.8, pdlp_primal_weight_smoothing = 0.5;
   // warm start in the ORIGINAL space (host memory), engine.cpp:237-266
   std::vector<double> warm_x, warm_y;
   double warm_primal_weight = 0.0;
@@ -67,6 +70,7 @@ struct EngineResult {
   double setup_seconds = 0, loop_seconds = 0, finish_seconds = 0, seconds = 0;
   long long kernel_launches = 0;
   double iter_kernel_ms = 0;
+  double teardown_seconds = 0;  // releasing the engine's device state after the loop
   long long iter_kernel_launches = 0;
   bool have_dual_ray = false, have_primal_ray = false;
   // in-process check of the reported point on the engine's model (device-computed)

@@ -3,6 +3,7 @@
 // its comment (file:line in the reference project); the engine itself runs on the GPU.
 #include "solver.hpp"
 #include "batch.hpp"
+#include "certify.hpp"
 
 #include <algorithm>
 #include <chrono>
@@ -398,11 +399,29 @@ Solution postsolve(const Model& M, const PresolveResult& r, const Solution& red)
   return s;
 }
 
+// Maps a Farkas vector of the reduced model to the original rows (presolve.cpp:195-207): kept
+// rows keep their multiplier; a column bound made by a removed singleton row moves onto that
+// row, newest singleton first, when λ_j = −(Aᵀr)_j points at it.
+std::vector<double> postsolve_farkas(const Model& M, const PresolveResult& r, const std::vector<double>& red_ray) {
+  std::vector<double> ray(static_cast<std::size_t>(M.num_rows), 0.0);
+  if (red_ray.size() != r.row_map.size()) return {};
+  for (std::size_t q = 0; q < r.row_map.size(); ++q) ray[r.row_map[q]] = red_ray[q];
+  for (auto it = r.singletons.rbegin(); it != r.singletons.rend(); ++it) {
+    const int j = it->col;
+    double lam = 0.0;
+    for (int p = M.col_start[j]; p < M.col_start[j + 1]; ++p) lam -= M.value[p] * ray[M.row_index[p]];
+    if ((lam > 0 && it->set_lower) || (lam < 0 && it->set_upper)) ray[it->row] = lam / it->a;
+  }
+  return ray;
+}
+
 // ============================================================ dispatcher (solve.cpp)
 namespace {
 
 using clock_t_ = std::chrono::steady_clock;
 double since(clock_t_::time_point t0) { return std::chrono::duration<double>(clock_t_::now() - t0).count(); }
+// The certified bound's implied-bounds refinement runs only within the time budget (solve.cpp:39).
+bool within_bound_budget(double elapsed, double time_limit) { return elapsed < 1.1 * time_limit + 1.0; }
 
 const char* alg_name(Algorithm a) {
   switch (a) {
@@ -433,6 +452,7 @@ EngineOptions engine_options(const Options& o) {  // engine.cpp:168-186
   e.kkt_c_norm = o.kkt_c_norm;
   e.kkt_obj_shift = o.kkt_obj_shift;
   e.verbosity = o.verbosity;
+  e.pdlp = o.algorithm == Algorithm::Pdlp;
   return e;
 }
 
@@ -445,7 +465,7 @@ Solution trivially_infeasible(const Options& options, const std::string& why) {
 }
 
 // The first-order engine on the GPU for one model (solve.cpp:469-609, LP part).
-Solution solve_direct(const Model& model, const Options& options) {
+Solution solve_direct(const Model& model, const Options& options, bool certify = true) {
   const auto t0 = clock_t_::now();
   Solution sol;
   sol.precision = options.precision == Precision::Mixed ? "mixed" : "fp64";
@@ -482,11 +502,41 @@ Solution solve_direct(const Model& model, const Options& options) {
     sol.setup_seconds = R.setup_seconds;
     sol.message = R.message;
     sol.engine_result = R;
+    sol.engine = options.algorithm == Algorithm::Pdlp ? "pdlp-b200" : "r2hpdhg-b200";
     sol.x = std::move(out.x);
     sol.y = std::move(out.y);
     sol.z = std::move(out.z);
     if (R.have_dual_ray) sol.dual_ray = std::move(out.dual_ray);
     if (R.have_primal_ray) sol.primal_ray = std::move(out.primal_ray);
+    if (sol.status == Status::Unbounded && !check_unboundedness_certificate(model, sol.x, sol.primal_ray).passed) {
+      // A ray from an iterate that is not primal-feasible: find a feasible point with the same
+      // engine on the zero-objective model (never unbounded) within what is left of the budget
+      // (solve.cpp:552-581). Feasible → the gate checks point + ray; infeasible → that verdict
+      // with its own certificate; otherwise an honest limit status.
+      Model feas = model;
+      std::fill(feas.obj.begin(), feas.obj.end(), 0.0);
+      Options fo = options;
+      fo.presolve = false;
+      fo.warm_x.clear();
+      fo.warm_y.clear();
+      fo.time_limit = std::max(0.0, options.time_limit - since(t0));
+      fo.iteration_limit = std::max<long long>(0, options.iteration_limit - sol.iterations);
+      Solution f = solve_direct(feas, fo, false);
+      const long long total = sol.iterations + f.iterations;
+      if (f.status == Status::Optimal) {
+        sol.x = f.x;
+        note(sol, "feasible point from a zero-objective solve (" + std::to_string(f.iterations) + " iterations)");
+      } else if (f.status == Status::Infeasible) {
+        f.message = "unbounded direction found, but the model is infeasible: " + f.message;
+        f.primal_ray.clear();
+        sol = f;
+      } else {
+        sol.status = f.status;
+        note(sol, std::string("no feasible point found for the ray (") + status_name(f.status) + ")");
+        sol.primal_ray.clear();
+      }
+      sol.iterations = total;
+    }
   } catch (const std::bad_alloc&) {
     sol = Solution{};
     sol.status = Status::NotSolved;
@@ -496,6 +546,9 @@ Solution solve_direct(const Model& model, const Options& options) {
     sol.status = Status::NumericalError;
     sol.message = e.what();
   }
+  if (certify && static_cast<int>(sol.y.size()) == model.num_rows && model.num_rows + model.num_cols > 0)
+    sol.certified_bound =
+        certified_dual_bound(model, sol.y, within_bound_budget(since(t0), options.time_limit)).bound;
   sol.seconds = since(t0);
   return sol;
 }
@@ -561,7 +614,41 @@ Solution solve_impl(const Model& model, const Options& options) {
     red.status = Status::Optimal;
     red.engine = "presolve";
   } else {
-    red = solve_direct(pr.reduced, budget(inner, 0));
+    red = solve_direct(pr.reduced, budget(inner, 0), /*certify=*/false);
+  }
+  const std::string removed = "presolve removed " + std::to_string(pr.removed_rows) + " rows, " +
+                              std::to_string(pr.removed_cols) + " cols";
+  if (red.status == Status::Infeasible && red.dual_ray.size() == static_cast<std::size_t>(pr.reduced.num_rows)) {
+    // cheaper than a re-solve: the reduced Farkas vector mapped to the original rows and checked
+    // there (solve.cpp:346-364); only if that fails is the original re-solved
+    std::vector<double> r = postsolve_farkas(model, pr, red.dual_ray);
+    if (!r.empty() && check_infeasibility_certificate(model, r).passed) {
+      Solution s = red;
+      s.x.clear(), s.y.clear(), s.z.clear();
+      s.dual_ray = std::move(r);
+      note(s, removed + "; reduced-model Farkas certificate postsolved to the original rows");
+      s.presolve_seconds = presolve_s;
+      s.seconds = since(t0);
+      return s;
+    }
+  }
+  if (red.status == Status::Unbounded && red.primal_ray.size() == static_cast<std::size_t>(pr.reduced.num_cols) &&
+      red.x.size() == static_cast<std::size_t>(pr.reduced.num_cols)) {
+    // the same for a primal ray: fixed columns get d = 0, kept columns keep d_j; the point is the
+    // ordinary primal postsolve (solve.cpp:365-391)
+    std::vector<double> d(static_cast<std::size_t>(model.num_cols), 0.0);
+    for (int j = 0; j < pr.reduced.num_cols; ++j) d[pr.col_map[j]] = red.primal_ray[j];
+    Solution s = postsolve(model, pr, red);
+    if (check_unboundedness_certificate(model, s.x, d).passed) {
+      s.status = Status::Unbounded;
+      s.primal_ray = std::move(d);
+      s.dual_ray.clear(), s.y.clear(), s.z.clear();
+      s.objective = s.dual_objective = kNaN;
+      note(s, removed + "; reduced-model ray and point postsolved to the original model");
+      s.presolve_seconds = presolve_s;
+      s.seconds = since(t0);
+      return s;
+    }
   }
   if (red.status == Status::Infeasible || red.status == Status::Unbounded)
     return on_original(red, std::string("reduced model ") + status_name(red.status));
@@ -637,7 +724,7 @@ Solution solve_impl(const Model& model, const Options& options) {
     tight.tolerance = std::max(options.tolerance * 1e-2, 1e-13);
     tight.warm_x = red.x;
     tight.warm_y = red.y;
-    const Solution red2 = solve_direct(pr.reduced, budget(tight, red.iterations));
+    const Solution red2 = solve_direct(pr.reduced, budget(tight, red.iterations), /*certify=*/false);
     Solution post2 = postsolve(model, pr, red2);
     post2.iterations += red.iterations;
     if (post2.status == Status::Optimal && passes(post2)) {
@@ -654,6 +741,9 @@ Solution solve_impl(const Model& model, const Options& options) {
   } else if (post.status == Status::Optimal && static_cast<int>(post.x.size()) != model.num_cols) {
     post.status = Status::NumericalError;
   }
+  if (static_cast<int>(post.y.size()) == model.num_rows && model.num_rows + model.num_cols > 0)
+    post.certified_bound =
+        certified_dual_bound(model, post.y, within_bound_budget(since(t0), options.time_limit)).bound;
   post.presolve_seconds = presolve_s;
   post.seconds = since(t0);
   return post;
@@ -667,8 +757,20 @@ void gate(const Model& model, const Options& options, Solution& s) {
       s.check = "PASS";
       return;
     }
-    s.check.clear();
-    note(s, "not certified (certificate verification is not part of this library)");
+    // claims other than Optimal are verified too (certificates.cpp)
+    const CertificateCheck c = s.status == Status::Infeasible ? check_infeasibility_certificate(model, s.dual_ray)
+                                                              : check_unboundedness_certificate(model, s.x, s.primal_ray);
+    if (!c.present) {
+      s.check.clear();
+      note(s, "not certified (the engine returned no certificate)");
+    } else if (c.passed) {
+      s.check = "PASS";
+      note(s, c.detail);
+    } else {
+      s.check = "FAIL";
+      note(s, std::string(status_name(s.status)) + " withdrawn, " + c.detail);
+      s.status = Status::NumericalError;
+    }
     return;
   }
   if (s.status != Status::Optimal) return;
@@ -707,14 +809,14 @@ Solution solve_unguarded(const Model& model, const Options& options) {  // solve
     prefix = buf;
   }
   Solution s;
-  if (resolved.algorithm != Algorithm::R2hpdhg) {
+  if (resolved.algorithm != Algorithm::R2hpdhg && resolved.algorithm != Algorithm::Pdlp) {
     s.status = Status::NotSolved;
     s.engine = alg_name(resolved.algorithm);
     s.message = std::string("algorithm '") + alg_name(resolved.algorithm) +
-                "' is not provided by this library: it runs r2hpdhg on the GPU (use_gpu = 1)";
+                "' is not provided by this library: it runs r2hpdhg and pdlp on the GPU (use_gpu = 1)";
   } else if (!options.use_gpu) {
     s.status = Status::NotSolved;
-    s.message = "this library runs r2hpdhg on the GPU only: set use_gpu = 1 (there is no CPU fallback)";
+    s.message = "this library runs r2hpdhg and pdlp on the GPU only: set use_gpu = 1 (there is no CPU fallback)";
   } else {
     bool device = true;
     try {

@@ -33,6 +33,11 @@ namespace b200 {
 #ifndef B200_SLAB_CARVEOUT
 #define B200_SLAB_CARVEOUT -1
 #endif
+// 1: the staged CSR tiles (read once per iteration) are loaded with an L2 evict-first policy, so
+// they do not push the gathered vector out of L2.
+#ifndef B200_TMA_EVICT_FIRST
+#define B200_TMA_EVICT_FIRST 1
+#endif
 
 constexpr int kSlabRows = 256;
 constexpr int kSlabTile = 2048;  // nonzeros staged per tile
@@ -61,10 +66,20 @@ __device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned
 // One TMA bulk copy global -> this CTA's shared memory (no multicast); both addresses and the
 // size are multiples of 16 bytes.
 __device__ __forceinline__ void tma_load_1d(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+#if B200_TMA_EVICT_FIRST
+  unsigned long long policy;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(policy));
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(policy)
+      : "memory");
+#else
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
                    smem_u32(dst)),
                "l"(src), "r"(bytes), "r"(smem_u32(bar))
                : "memory");
+#endif
 }
 __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
   unsigned ok;
@@ -355,6 +370,57 @@ struct EpiDual {
       yh[i] = h;
     }
     y[i] = tw * (a * h + b * yi) + (static_cast<T>(1) - tw) * p.y0;
+  }
+};
+
+// PDLP steps (pdlp.cpp:54-67), in the backend ops' arithmetic, fused after the SpMVs. The running
+// averages use w_a = 1/inner with inner = inner0 + step + 1 (the iterate count since the last
+// restart, after this step):
+//   primal, after aty = Ãᵀy:  x⁺ = clamp(x − τ(c − aty), l, u);  x̄ = −1·x + 2·x⁺ (copy + axpby);
+//                             xa ← w_a·x⁺ + (1 − w_a)·xa
+//   dual, after ax = Ãx̄:     y⁺ = y − σ·ax + σ·clamp(ax − y/σ, rl, ru);  ya ← w_a·y⁺ + (1 − w_a)·ya
+template <class T>
+struct EpiPdlpPrimal {
+  const T *x, *c, *l, *u;
+  T *xn, *xb, *xa;
+  const StepParams* P;
+  int step;
+  struct Pre {
+    T x, c, l, u, xa;
+  };
+  __device__ bool active() const { return !P->done; }
+  __device__ Pre load(int j) const { return Pre{x[j], c[j], l[j], u[j], xa[j]}; }
+  __device__ void operator()(int j, double s) const { (*this)(j, s, load(j)); }
+  __device__ void operator()(int j, double s, const Pre& p) const {
+    const T t = static_cast<T>(P->tau);
+    const T aty = static_cast<T>(s);
+    const T h = ref_clamp<T>(p.x - t * (p.c - aty), p.l, p.u);
+    xn[j] = h;
+    xb[j] = static_cast<T>(-1.0) * p.x + static_cast<T>(2.0) * h;
+    const double wa = 1.0 / static_cast<double>(P->inner0 + step + 1);
+    xa[j] = static_cast<T>(wa) * h + static_cast<T>(1.0 - wa) * p.xa;
+  }
+};
+template <class T>
+struct EpiPdlpDual {
+  const T *y, *rl, *ru;
+  T *yn, *ya;
+  const StepParams* P;
+  int step;
+  struct Pre {
+    T y, rl, ru, ya;
+  };
+  __device__ bool active() const { return !P->done; }
+  __device__ Pre load(int i) const { return Pre{y[i], rl[i], ru[i], ya[i]}; }
+  __device__ void operator()(int i, double s) const { (*this)(i, s, load(i)); }
+  __device__ void operator()(int i, double s, const Pre& p) const {
+    const T sg = static_cast<T>(P->sigma);
+    const T ax = static_cast<T>(s);
+    const T v = ax - p.y / sg;
+    const T h = p.y - sg * ax + sg * ref_clamp<T>(v, p.rl, p.ru);
+    yn[i] = h;
+    const double wa = 1.0 / static_cast<double>(P->inner0 + step + 1);
+    ya[i] = static_cast<T>(wa) * h + static_cast<T>(1.0 - wa) * p.ya;
   }
 };
 

@@ -75,7 +75,8 @@ class _Stats(ctypes.Structure):  # ps26119_stats
                 ("restarts", ctypes.c_longlong), ("iterations_to_fast", ctypes.c_longlong),
                 ("switch_iteration", ctypes.c_longlong), ("kernel_launches", ctypes.c_longlong),
                 ("m", ctypes.c_longlong), ("n", ctypes.c_longlong), ("nnz", ctypes.c_longlong),
-                ("spmv_kernel_ms", ctypes.c_double), ("spmv_kernel_launches", ctypes.c_longlong)]
+                ("spmv_kernel_ms", ctypes.c_double), ("spmv_kernel_launches", ctypes.c_longlong),
+                ("teardown_seconds", ctypes.c_double), ("call_seconds", ctypes.c_double)]
 
 
 class _Scenario(ctypes.Structure):  # ps26119_scenario
@@ -93,7 +94,8 @@ _MODEL = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, _D, _D, _D,
 # Every symbol the C headers declare (include/ps26119.h, include/ps26119_backend.h).
 EXPORTS = ["ps26119_version", "ps26119_default_options", "ps26119_solve_lp", "ps26119_solve_lp_ex",
            "ps26119_solve_mps", "ps26119_default_engine_options", "ps26119_solve_lp_engine",
-           "ps26119_solve_lp_device", "ps26119_last_stats", "ps26119_solve_batch", "ps26119_backend_new", "ps26119_backend_free",
+           "ps26119_solve_lp_device", "ps26119_last_stats", "ps26119_solve_batch",
+           "ps26119_certified_bound", "ps26119_check_certificate", "ps26119_backend_new", "ps26119_backend_free",
            "ps26119_backend_last_error", "ps26119_backend_set_precision", "ps26119_backend_create",
            "ps26119_backend_upload", "ps26119_backend_download", "ps26119_backend_fill", "ps26119_backend_copy",
            "ps26119_backend_axpby", "ps26119_backend_spmv", "ps26119_backend_spmv_t", "ps26119_backend_dot",
@@ -126,6 +128,8 @@ def load(path: str | None = None):
     L.ps26119_last_stats.argtypes = [P(_Stats)]
     L.ps26119_solve_batch.argtypes = _MODEL + [ctypes.c_int, P(_Scenario), P(_Options), P(_EngineOptions),
                                                P(_Result), _D, _D, _D]
+    L.ps26119_certified_bound.argtypes = _MODEL + [_D, ctypes.c_int, _D]
+    L.ps26119_check_certificate.argtypes = [ctypes.c_int] + _MODEL + [_D, _D, _D]
     B = ctypes.c_void_p
     L.ps26119_backend_new.argtypes = [P(B)] + _MODEL + [P(_ScalingOptions), ctypes.c_int]
     L.ps26119_backend_free.argtypes = [B]
@@ -354,6 +358,42 @@ def solve_batch(c, A, row_lower, row_upper, col_lower=None, col_upper=None, scen
             out[k] = Result(NOT_SOLVED, _STATUS[NOT_SOLVED], np.nan, np.nan, np.nan, np.nan, np.nan, np.nan, 0, 0.0,
                             "r2hpdhg-batch", "scenario has wrong vector sizes or non-finite data")
     return out
+
+
+def _model_args(lp):
+    f = lambda a: np.ascontiguousarray(a, dtype=np.float64)
+    g = lambda a: np.ascontiguousarray(a, dtype=np.int32)
+    arrs = [f(lp.c), f(lp.col_lower), f(lp.col_upper), f(lp.row_lower), f(lp.row_upper), g(lp.col_start),
+            g(lp.row_index), f(lp.value)]
+    args = [lp.num_rows, lp.num_cols, int(lp.sense), float(lp.offset)] + \
+        [_ptr(a) for a in arrs[:5]] + [_ptr(arrs[5], ctypes.c_int), _ptr(arrs[6], ctypes.c_int), _ptr(arrs[7])]
+    return args, arrs
+
+
+def certified_bound(lp, y, use_implied_bounds=True) -> dict:
+    """Rounding-error-proof bound on the optimum of ``lp`` (an object with the generators.Lp
+    fields) from row multipliers ``y`` (host computation)."""
+    args, keep = _model_args(lp)
+    yy = np.ascontiguousarray(y, dtype=np.float64)
+    out = np.zeros(4)
+    rc = load().ps26119_certified_bound(*args, _ptr(yy), int(bool(use_implied_bounds)), _ptr(out))
+    if rc != 0:
+        raise ValueError(f"ps26119_certified_bound failed ({rc})")
+    return {"finite": bool(out[0]), "bound": out[1], "unbounded_row_terms": int(out[2]),
+            "unbounded_col_terms": int(out[3])}
+
+
+def check_certificate(lp, ray, x=None) -> dict:
+    """Farkas (x None: ray has num_rows values) or unboundedness (x and ray: num_cols values) check."""
+    args, keep = _model_args(lp)
+    r = np.ascontiguousarray(ray, dtype=np.float64)
+    xx = None if x is None else np.ascontiguousarray(x, dtype=np.float64)
+    out = np.zeros(5)
+    rc = load().ps26119_check_certificate(0 if x is None else 1, *args, _ptr(xx), _ptr(r), _ptr(out))
+    if rc != 0:
+        raise ValueError(f"ps26119_check_certificate failed ({rc})")
+    return {"present": bool(out[0]), "passed": bool(out[1]), "rigorous": bool(out[2]), "measure": out[3],
+            "violation": out[4]}
 
 
 def solve_mps(path, algorithm="auto", precision="fp64", gpu=True, tolerance=1e-8, time_limit=3600.0,

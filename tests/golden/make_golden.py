@@ -6,7 +6,8 @@ loadable, and the CPU tests pin the C oracle to them.
     python tests/golden/make_golden.py [--with-c1]
 
 Each record: case, precision, presolve, status, iterations, objective / dual objective /
-primal weight (exact, as float.hex), sha256 of x, y, z, and for small models x and y.
+primal weight / certified bound (exact, as float.hex), the in-process check, sha256 of x, y, z,
+and for small models x and y.
 """
 import argparse
 import hashlib
@@ -60,7 +61,7 @@ def main():
                 rec = {"case": name, "precision": precision, "presolve": presolve, "status": s.status,
                        "iterations": s.iterations, "objective": hexf(s.objective),
                        "dual_objective": hexf(s.dual_objective), "primal_weight": hexf(s.primal_weight),
-                       "check": s.check, "message": s.message, "m": lp.num_rows, "n": lp.num_cols,
+                       "check": s.check, "certified_bound": hexf(s.certified_bound), "message": s.message, "m": lp.num_rows, "n": lp.num_cols,
                        "nnz": lp.nnz, "x_sha256": digest(s.x), "y_sha256": digest(s.y), "z_sha256": digest(s.z),
                        "seconds": round(time.time() - t, 3)}
                 if lp.num_rows + lp.num_cols <= 800:

@@ -66,6 +66,9 @@ def test_exact_mode_trajectory_is_bit_identical(name, precision):
     assert s.iterations == r.iterations
     assert np.array_equal(s.x, r.x) and np.array_equal(s.y, r.y) and np.array_equal(s.z, r.z)
     assert s.objective == r.objective
+    if hasattr(r, "certified_bound"):  # the reference's rounding-proof bound from the same y
+        assert s.certified_bound == r.certified_bound or (np.isnan(s.certified_bound) and np.isnan(r.certified_bound))
+        assert (s.check == "PASS") == (r.check == 1)
 
 
 def fast_mode_bar(name, s, r):
@@ -105,6 +108,7 @@ def test_c_api_exact_mode_with_presolve_is_bit_identical(name):
     assert s.objective == float.fromhex(rec["objective"])
     assert hashlib.sha256(s.x.tobytes()).hexdigest() == rec["x_sha256"]
     assert hashlib.sha256(s.y.tobytes()).hexdigest() == rec["y_sha256"]
+    assert s.certified_bound == float.fromhex(rec["certified_bound"])
 
 
 @pytest.mark.parametrize("name", ["wyndor", "mixed_rows", "random_m300_s1", "staircase_T4_s1", "staircase_T8_s1"])
@@ -142,9 +146,16 @@ def test_infeasible_and_unbounded_verdicts(precision):
     s = gpu_solve(lps.infeasible(), precision, exact=False)
     assert s.status == ps26119.INFEASIBLE, s.message
     assert s.dual_ray is not None
+    assert s.check == "PASS" and "Farkas certificate" in s.message  # checked on the original model
     s = gpu_solve(lps.unbounded(), precision, exact=False)
     assert s.status == ps26119.UNBOUNDED, s.message
     assert s.primal_ray is not None
+    assert s.check == "PASS"  # point and ray checked on the original model
+    # through the C API with presolve, as the reference's C API answers (golden records: check 1)
+    for lp, name in ((lps.infeasible(), "infeasible"), (lps.unbounded(), "unbounded")):
+        rec = golden(name, precision, True)
+        s = gpu_solve(lp, precision, exact=False, presolve=True)
+        assert s.status_name == rec["status"] and (s.check == "PASS") == (rec["check"] == 1), s.message
 
 
 def test_repeated_solves_are_bit_identical():
