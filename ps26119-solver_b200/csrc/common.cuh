@@ -204,7 +204,51 @@ class DevBuf {
   int dev_ = 0;
 };
 
-// Page-locked host memory for the per-check status transfers.
+// Page-locked host blocks, cached like the device blocks: cudaFreeHost synchronises the device
+// and was measured to take from under a millisecond to over ten per call. At most 256 MiB stay
+// cached; blocks are reused by exact size class.
+class PinnedBlockCache {
+ public:
+  static PinnedBlockCache& instance() {
+    static PinnedBlockCache* c = new PinnedBlockCache();  // never destroyed: no CUDA calls at exit
+    return *c;
+  }
+  void* acquire(std::size_t bytes) {
+    {
+      std::lock_guard<std::mutex> lock(mu_);
+      for (std::size_t k = 0; k < free_.size(); ++k)
+        if (free_[k].first == bytes) {
+          void* p = free_[k].second;
+          free_[k] = free_.back();
+          free_.pop_back();
+          cached_ -= bytes;
+          return p;
+        }
+    }
+    void* p = nullptr;
+    B200_CHECK(cudaMallocHost(&p, bytes));
+    return p;
+  }
+  void release(void* p, std::size_t bytes) {
+    {
+      std::lock_guard<std::mutex> lock(mu_);
+      if (cached_ + bytes <= (256u << 20)) {
+        free_.push_back({bytes, p});
+        cached_ += bytes;
+        return;
+      }
+    }
+    cudaFreeHost(p);
+  }
+
+ private:
+  std::mutex mu_;
+  std::vector<std::pair<std::size_t, void*>> free_;
+  std::size_t cached_ = 0;
+};
+
+// Page-locked host memory for the per-check status transfers. The host code syncs the stream
+// that used a block before the block goes back to the cache.
 template <class T>
 class PinnedBuf {
  public:
@@ -212,19 +256,13 @@ class PinnedBuf {
   PinnedBuf(const PinnedBuf&) = delete;
   PinnedBuf& operator=(const PinnedBuf&) = delete;
   ~PinnedBuf() {
-#ifdef B200_TEARDOWN_TRACE
-    const auto t0 = std::chrono::steady_clock::now();
-#endif
-    if (p_) cudaFreeHost(p_);
-#ifdef B200_TEARDOWN_TRACE
-    std::fprintf(stderr, "teardown: cudaFreeHost %.1f ms\n",
-                 std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
-#endif
+    if (p_) PinnedBlockCache::instance().release(p_, bytes_);
   }
   void alloc(std::size_t n) {
-    if (p_) cudaFreeHost(p_);
+    if (p_) PinnedBlockCache::instance().release(p_, bytes_);
     p_ = nullptr;
-    B200_CHECK(cudaMallocHost(reinterpret_cast<void**>(&p_), (n ? n : 1) * sizeof(T)));
+    bytes_ = DeviceBlockCache::size_class((n ? n : 1) * sizeof(T));
+    p_ = static_cast<T*>(PinnedBlockCache::instance().acquire(bytes_));
     n_ = n;
   }
   T* get() { return p_; }
@@ -233,7 +271,7 @@ class PinnedBuf {
 
  private:
   T* p_ = nullptr;
-  std::size_t n_ = 0;
+  std::size_t n_ = 0, bytes_ = 0;
 };
 
 constexpr int kBlock = 256;
