@@ -99,7 +99,11 @@ PS26119_API int ps26119_solve_lp_ex(int num_rows, int num_cols, int sense, doubl
                         const double* value, const ps26119_options* opt, ps26119_result* result,
                         double* x, double* y, double* z, double* dual_ray, double* primal_ray);
 
-/* Replaces reference ps26119_solve_mps (ps26119.h:93-94; c_api.cpp:261-302). */
+/* Replaces reference ps26119_solve_mps (ps26119.h:90-94; c_api.cpp:161-202): reads an MPS file
+ * (free or fixed format), solves it, and writes the solution file (the reference's .sol format)
+ * when solution_path is non-NULL. Read errors return PS26119_INVALID_ARGUMENT with the reason and
+ * line in result->message. Integer markers are read but the LP relaxation is solved (this library
+ * has no MILP engine); the message then starts with "LP relaxation (integrality ignored)". */
 PS26119_API int ps26119_solve_mps(const char* path, const ps26119_options* opt, ps26119_result* result,
                       const char* solution_path);
 

@@ -26,6 +26,8 @@
 #include <vector>
 
 #include "core/certificates.h"
+#include "io/lpm_reader.h"
+#include "io/mps_reader.h"
 #include "core/presolve.h"
 #include "core/safe_bound.h"
 #include "core/solution_checker.h"
@@ -290,6 +292,25 @@ void ref_check(int m, int n, int sense, double offset, const double* c, const do
   out[4] = r.primal_objective;
   out[5] = r.dual_objective;
   out[6] = certified_dual_bound(M, yv, true).bound;
+}
+
+// The reference's readers: fingerprint of the model read from `path` (.lpm or .mps), dims[3] =
+// rows, cols, nnz. Returns 1 on success, 0 on a read error (message in fp).
+int ref_read_fingerprint(const char* path, char* fp, int cap, long long* dims) {
+  Model m;
+  const std::string p(path);
+  bool ok = false;
+  std::string err;
+  if (p.size() > 4 && p.compare(p.size() - 4, 4, ".lpm") == 0) {
+    const auto r = io::read_lpm(p, m);
+    ok = r.ok;
+    err = r.error;
+  } else {
+    ok = io::read_mps(p, m, err);
+  }
+  std::snprintf(fp, static_cast<std::size_t>(cap), "%s", ok ? m.fingerprint_hex().c_str() : err.c_str());
+  if (ok) dims[0] = m.num_rows, dims[1] = m.num_cols, dims[2] = static_cast<long long>(m.nnz());
+  return ok ? 1 : 0;
 }
 
 // out[4] = finite, bound, unbounded_row_terms, unbounded_col_terms

@@ -88,6 +88,8 @@ def lib():
         L.ref_backend_kkt.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _D]
         L.ref_check.argtypes = model + [_D, _D, _D]
         L.ref_bound.argtypes = model + [_D, ctypes.c_int, _D]
+        L.ref_read_fingerprint.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int,
+                                           ctypes.POINTER(ctypes.c_longlong)]
         L.ref_certificate.argtypes = [ctypes.c_int] + model + [_D, _D, _D]
         L.ps26119_solve_lp.argtypes = None  # the reference's own C API, used by bench.py
         _lib = L
@@ -199,6 +201,16 @@ def check(lp, x, y):
     del keep
     return {"passed": bool(out[0]), "primal": out[1], "dual": out[2], "gap": out[3], "primal_objective": out[4],
             "dual_objective": out[5], "certified_bound": out[6]}
+
+
+def read_fingerprint(path):
+    """The reference reader's view of a model file: (fingerprint hex, (rows, cols, nnz)) or
+    (None, error text)."""
+    L = lib()
+    buf = ctypes.create_string_buffer(512)
+    dims = (ctypes.c_longlong * 3)()
+    ok = L.ref_read_fingerprint(os.fsencode(path), buf, 512, dims)
+    return (buf.value.decode(), tuple(dims)) if ok else (None, buf.value.decode())
 
 
 def bound(lp, y, use_implied=True):

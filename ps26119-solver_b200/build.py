@@ -20,11 +20,12 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB_DIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIB_DIR, "libps26119.so")
+CLI = os.path.join(LIB_DIR, "ps26119")  # the command-line tool
 CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA, "bin", "nvcc")
 
 CU_SOURCES = ["engine.cu", "backend.cu", "batch.cu", "noalloc.cu"]
-CPP_SOURCES = ["solver.cpp", "certify.cpp", "c_api.cpp"]
+CPP_SOURCES = ["solver.cpp", "certify.cpp", "io.cpp", "c_api.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC", "-Xcompiler",
               "-ffp-contract=off", "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr"] + ARCH
@@ -76,6 +77,12 @@ def build(force: bool = False, jobs: int = 4, verbose: bool = False) -> str:
         list(ex.map(_compile, cmds))
     if cmds or not os.path.exists(LIB) or any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs):
         _compile([NVCC, "-shared"] + ARCH + ["-o", LIB] + objs + ["-lpthread"])
+    # the command-line tool, linked from the same objects
+    cli_src, cli_obj = os.path.join(CSRC, "cli.cpp"), os.path.join(BUILD, "cli.cpp.o")
+    if force or _stale(cli_obj, cli_src, headers):
+        _compile(["g++"] + CXX_FLAGS + ["-c", cli_src, "-o", cli_obj])
+    if not os.path.exists(CLI) or any(os.path.getmtime(o) > os.path.getmtime(CLI) for o in objs + [cli_obj]):
+        _compile([NVCC] + ARCH + ["-o", CLI, cli_obj] + objs + ["-lpthread"])
     return LIB
 
 

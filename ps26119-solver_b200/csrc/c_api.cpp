@@ -16,6 +16,7 @@
 #include "../../include/ps26119.h"
 #include "../../include/ps26119_backend.h"
 #include "certify.hpp"
+#include "io.hpp"
 #include "solver.hpp"
 
 using namespace b200;
@@ -247,16 +248,49 @@ int ps26119_solve_lp_engine(int num_rows, int num_cols, int sense, double obj_of
 }
 
 int ps26119_solve_mps(const char* path, const ps26119_options* opt, ps26119_result* result,
-                      const char* solution_path) {
-  (void)opt;
-  (void)solution_path;
+                      const char* solution_path) {  // c_api.cpp:161-202
   if (!result) return PS26119_INVALID_ARGUMENT;
   clear(result);
-  result->status = PS26119_INVALID_ARGUMENT;
-  set_text(result->message, sizeof result->message,
-           path ? "read error: MPS input is not supported by this library yet (pass the model in CSC form)"
-                : "path is NULL");
-  return result->status;
+  auto invalid = [&](const std::string& why) {
+    result->status = PS26119_INVALID_ARGUMENT;
+    set_text(result->message, sizeof result->message, why);
+    return result->status;
+  };
+  if (!path) return invalid("path is NULL");
+  if (solution_path) {  // fail before solving: the solution file must be writable
+    std::FILE* probe = std::fopen(solution_path, "r");
+    const bool existed = probe != nullptr;
+    if (probe) std::fclose(probe);
+    std::FILE* f = std::fopen(solution_path, "a");
+    if (!f) return invalid(std::string("cannot write the solution file '") + solution_path + "'");
+    std::fclose(f);
+    if (!existed) std::remove(solution_path);
+  }
+  try {
+    Model m;
+    ModelInfo info;
+    std::string err;
+    if (!read_mps(path, m, info, err)) return invalid("read error: " + err);
+    if (opt && (opt->warm_x || opt->warm_y)) return invalid("warm start is not supported by ps26119_solve_mps");
+    Options o;
+    if (const char* bad = to_options(opt, m.num_rows, m.num_cols, o)) return invalid(bad);
+    Solution s = solve(m, o);
+    if (info.has_integers())
+      s.message = std::string("LP relaxation (integrality ignored)") + (s.message.empty() ? "" : "; ") + s.message;
+    s.model_fingerprint = fingerprint_hex(m);
+    fill(s, result);
+    if (solution_path && !write_solution(solution_path, m, info, s, err))
+      set_text(result->message, sizeof result->message, "solved, but " + err);
+    return result->status;
+  } catch (const std::bad_alloc&) {
+    result->status = PS26119_NOT_SOLVED;
+    set_text(result->message, sizeof result->message, "out of memory");
+    return result->status;
+  } catch (const std::exception& e) {
+    result->status = PS26119_NUMERICAL_ERROR;
+    set_text(result->message, sizeof result->message, e.what());
+    return result->status;
+  }
 }
 
 int ps26119_solve_lp_device(int num_rows, int num_cols, int sense, double obj_offset, const double* d_c,

@@ -131,7 +131,7 @@ std::uint64_t Model::fingerprint() const {  // model.cpp:20-85: FNV-1a over the 
     i64(static_cast<std::int64_t>(col.size()));
     for (const auto& [i, v] : col) i64(i), f64(v);
   }
-  for (int j = 0; j < num_cols; ++j) i64(0);
+  for (int j = 0; j < num_cols; ++j) i64(j < static_cast<int>(is_integer.size()) && is_integer[j] ? 1 : 0);
   return h;
 }
 

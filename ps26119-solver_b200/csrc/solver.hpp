@@ -27,6 +27,8 @@ struct Model {
   std::vector<double> obj, col_lower, col_upper, row_lower, row_upper;
   std::vector<int> col_start, row_index;
   std::vector<double> value;
+  std::vector<char> is_integer;  // from a file with integer markers; empty = all continuous (the
+                                 // solve is the LP relaxation; only the fingerprint uses it)
 
   std::size_t nnz() const { return value.size(); }
   std::string validate() const;        // model.cpp:93-160
