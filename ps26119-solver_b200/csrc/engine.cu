@@ -189,6 +189,7 @@ class Engine {
   cudaGraphExec_t g_pdlp_chk_[2][2][3] = {};                                        // [precision][phase][variant]
   long long pdlp_kernels_[2][2] = {}, pdlp_chk_kernels_[2][2][3] = {};
   DevBuf<double> res2_;
+  DevBuf<int2> slab_a_, slab_t_;
   PinnedBuf<double> hres2_;
   SumPlan plan_dist_;
   long long epoch_kernels_[2] = {0, 0}, check_kernels_[2][3] = {{0, 0, 0}, {0, 0, 0}};
@@ -217,6 +218,13 @@ void Engine::setup() {
   eta_ = norm > 0 ? 0.998 / norm : 1.0;  // engine.cpp:203-204
   kernels_ += sp_.kernels;
   const int m = M_.m, n = M_.n;
+  // each slab's nonzero range for the iteration kernels (Ã rows; Ãᵀ rows = the columns)
+  slab_a_.alloc(static_cast<std::size_t>(std::max(1, slab_count(m))));
+  slab_t_.alloc(static_cast<std::size_t>(std::max(1, slab_count(n))));
+  if (m > 0) k_slab_table<<<grid_for(slab_count(m)), kBlock, 0, st_>>>(m, sp_.a_rp.get(), slab_a_.get());
+  if (n > 0) k_slab_table<<<grid_for(slab_count(n)), kBlock, 0, st_>>>(n, M_.col_start, slab_t_.get());
+  B200_LAUNCH_CHECK();
+  kernels_ += 2;
   vd_.alloc(n, m);
   if (o_.mixed) vf_.alloc(n, m);
   params_.alloc(1);
@@ -363,9 +371,9 @@ void Engine::capture_epoch() {
   B200_CHECK(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
   auto step = [&](int s) {
     EpiPrimal<T> ep{v.x.get(), v.xh.get(), v.xb.get(), v.x0.get(), sp_.c<T>(), sp_.l<T>(), sp_.u<T>(), P, s, 0, 0, 0};
-    launch_slab_tma<T>(n, M_.col_start, sp_.t_ri.get(), sp_.At_val<T>(), v.y.get(), ep, st_);
+    launch_slab_tma<T>(n, M_.col_start, sp_.t_ri.get(), sp_.At_val<T>(), v.y.get(), ep, st_, slab_t_.get());
     EpiDual<T> ed{v.y.get(), v.yh.get(), v.yb.get(), v.y0.get(), sp_.rl<T>(), sp_.ru<T>(), P, s, 0, 0, 0, 0};
-    launch_slab_tma<T>(m, sp_.a_rp.get(), sp_.a_col.get(), sp_.A_val<T>(), v.xb.get(), ed, st_);
+    launch_slab_tma<T>(m, sp_.a_rp.get(), sp_.a_col.get(), sp_.A_val<T>(), v.xb.get(), ed, st_, slab_a_.get());
     capture_count_ += 2;
   };
   B200_CHECK(cudaEventRecordWithFlags(ev_[0], st_, cudaEventRecordExternal));
@@ -867,9 +875,9 @@ void Engine::capture_pdlp_epoch(int phase) {
     T* yc = odd ? v.yh.get() : v.y.get();
     T* yn = odd ? v.y.get() : v.yh.get();
     EpiPdlpPrimal<T> ep{xc, sp_.c<T>(), sp_.l<T>(), sp_.u<T>(), xn, v.xb.get(), v.dx.get(), P, s};
-    launch_slab_tma<T>(n, M_.col_start, sp_.t_ri.get(), sp_.At_val<T>(), yc, ep, st_);
+    launch_slab_tma<T>(n, M_.col_start, sp_.t_ri.get(), sp_.At_val<T>(), yc, ep, st_, slab_t_.get());
     EpiPdlpDual<T> ed{yc, sp_.rl<T>(), sp_.ru<T>(), yn, v.dy.get(), P, s};
-    launch_slab_tma<T>(m, sp_.a_rp.get(), sp_.a_col.get(), sp_.A_val<T>(), v.xb.get(), ed, st_);
+    launch_slab_tma<T>(m, sp_.a_rp.get(), sp_.a_col.get(), sp_.A_val<T>(), v.xb.get(), ed, st_, slab_a_.get());
     capture_count_ += 2;
   }
   B200_CHECK(cudaEventRecordWithFlags(ev_[1], st_, cudaEventRecordExternal));

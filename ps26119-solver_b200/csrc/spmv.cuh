@@ -38,6 +38,17 @@ namespace b200 {
 #ifndef B200_TMA_EVICT_FIRST
 #define B200_TMA_EVICT_FIRST 1
 #endif
+// 1: the iteration kernels read each slab's nonzero range [k0, k1) from a small precomputed
+// table kept in L2 (evict-last), instead of from the row pointers: the first load of a block
+// is then an L2 hit, not a DRAM round trip, and the tile copy starts sooner.
+#ifndef B200_SLAB_TABLE
+#define B200_SLAB_TABLE 0
+#endif
+// 1: the iteration epilogues load their streamed operands evict-first and store the vector the
+// next kernel gathers (x̄, y) evict-last, so that it is still in L2 when the gathers come.
+#ifndef B200_EPI_HINTS
+#define B200_EPI_HINTS 1
+#endif
 
 constexpr int kSlabRows = 256;
 constexpr int kSlabTile = 2048;  // nonzeros staged per tile
@@ -97,6 +108,52 @@ __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsig
   return false;
 }
 
+// L2-policy loads and stores (createpolicy + .L2::cache_hint).
+__device__ __forceinline__ unsigned long long l2_policy_last() {
+  unsigned long long p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ unsigned long long l2_policy_first() {
+  unsigned long long p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ int2 ld_keep(const int2* p) {
+  int2 v;
+  asm volatile("ld.global.L2::cache_hint.v2.s32 {%0, %1}, [%2], %3;" : "=r"(v.x), "=r"(v.y) : "l"(p), "l"(l2_policy_last()));
+  return v;
+}
+template <class T>
+__device__ __forceinline__ T ld_stream(const T* p) {
+#if B200_EPI_HINTS
+  if constexpr (sizeof(T) == 8) {
+    double v;
+    asm volatile("ld.global.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(l2_policy_first()));
+    return static_cast<T>(v);
+  } else {
+    float v;
+    asm volatile("ld.global.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(l2_policy_first()));
+    return static_cast<T>(v);
+  }
+#else
+  return *p;
+#endif
+}
+template <class T>
+__device__ __forceinline__ void st_keep(T* p, T v) {
+#if B200_EPI_HINTS
+  if constexpr (sizeof(T) == 8)
+    asm volatile("st.global.L2::cache_hint.f64 [%0], %1, %2;" ::"l"(p), "d"(static_cast<double>(v)), "l"(l2_policy_last())
+                 : "memory");
+  else
+    asm volatile("st.global.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(p), "f"(static_cast<float>(v)), "l"(l2_policy_last())
+                 : "memory");
+#else
+  *p = v;
+#endif
+}
+
 // Epilogues may prefetch their operands: `Pre load(int row)` is issued at kernel entry, before
 // the nonzeros are staged, so its latency overlaps the SpMV; `operator()(row, s, pre)` then
 // finishes the update. Epilogues that take maxima expose `Acc` (fields written by the
@@ -141,7 +198,8 @@ template <class T, class Epi, bool kTma>
 __global__ void __launch_bounds__(kSlabRows, B200_SLAB_MIN_BLOCKS) k_slab(int rows, const int* __restrict__ rp,
                                                         const int* __restrict__ col,
                                                         const T* __restrict__ val,
-                                                        const T* __restrict__ x, Epi epi) {
+                                                        const T* __restrict__ x, Epi epi,
+                                                        const int2* __restrict__ slab) {
   __shared__ SlabSmem<T> sm;
   if (!epi.active()) return;
   const int r0 = blockIdx.x * kSlabRows;
@@ -149,7 +207,13 @@ __global__ void __launch_bounds__(kSlabRows, B200_SLAB_MIN_BLOCKS) k_slab(int ro
   const bool mine = threadIdx.x < nr;
   const int row = r0 + static_cast<int>(threadIdx.x);
   // independent loads first: the slab's nonzero range, this thread's row bounds, the epilogue
-  const int k0 = __ldg(rp + r0), k1 = __ldg(rp + r0 + nr);
+  int k0, k1;
+  if (slab) {
+    const int2 kr = ld_keep(slab + blockIdx.x);
+    k0 = kr.x, k1 = kr.y;
+  } else {
+    k0 = __ldg(rp + r0), k1 = __ldg(rp + r0 + nr);
+  }
   const int beg = mine ? __ldg(rp + row) : 0, end = mine ? __ldg(rp + row + 1) : 0;
   const auto pre = epi_load(epi, mine ? row : r0, 0);
   auto acc = epi_acc(epi, 0);
@@ -235,20 +299,31 @@ inline void slab_prepare() {
 
 template <class T, class Epi, bool kTma = false>
 inline void launch_slab(int rows, const int* rp, const int* col, const T* val, const T* x, const Epi& epi,
-                        cudaStream_t st) {
+                        cudaStream_t st, const int2* slab = nullptr) {
   if (rows <= 0) return;
   slab_prepare<T, Epi, kTma>();
   const int grid = (rows + kSlabRows - 1) / kSlabRows;
-  k_slab<T, Epi, kTma><<<grid, kSlabRows, 0, st>>>(rows, rp, col, val, x, epi);
+  k_slab<T, Epi, kTma><<<grid, kSlabRows, 0, st>>>(rows, rp, col, val, x, epi, slab);
   B200_LAUNCH_CHECK();
 }
 
-// The TMA-staged form, for CSR arrays allocated by this library (tail-padded DevBufs).
+// The TMA-staged form, for CSR arrays allocated by this library (tail-padded DevBufs). `slab`:
+// an optional table of each slab's nonzero range (see slab_table).
 template <class T, class Epi>
 inline void launch_slab_tma(int rows, const int* rp, const int* col, const T* val, const T* x, const Epi& epi,
-                            cudaStream_t st) {
-  launch_slab<T, Epi, B200_STAGE_TMA != 0>(rows, rp, col, val, x, epi, st);
+                            cudaStream_t st, const int2* slab = nullptr) {
+  launch_slab<T, Epi, B200_STAGE_TMA != 0>(rows, rp, col, val, x, epi, st, B200_SLAB_TABLE ? slab : nullptr);
 }
+
+// The nonzero range [rp[b·kSlabRows], rp[min((b+1)·kSlabRows, rows)]) of every slab b.
+static __global__ void k_slab_table(int rows, const int* rp, int2* out) {
+  const int nb = (rows + kSlabRows - 1) / kSlabRows;
+  B200_FOR(b, nb) {
+    const int r0 = static_cast<int>(b) * kSlabRows, r1 = min(r0 + kSlabRows, rows);
+    out[b] = make_int2(rp[r0], rp[r1]);
+  }
+}
+inline int slab_count(int rows) { return rows <= 0 ? 0 : (rows + kSlabRows - 1) / kSlabRows; }
 
 // Number of bulk-copy waits that ran out since the library was loaded (host side).
 inline unsigned stage_timeouts() {
@@ -314,7 +389,9 @@ struct EpiPrimal {
     T x, x0, c, l, u;
   };
   __device__ bool active() const { return P == nullptr || !P->done; }
-  __device__ Pre load(int j) const { return Pre{x[j], x0[j], c[j], l[j], u[j]}; }
+  __device__ Pre load(int j) const {
+    return Pre{ld_stream(x + j), ld_stream(x0 + j), ld_stream(c + j), ld_stream(l + j), ld_stream(u + j)};
+  }
   __device__ void operator()(int j, double s) const { (*this)(j, s, load(j)); }
   __device__ void operator()(int j, double s, const Pre& p) const {
     double tau_d = tau, w_d = w, rho_d = rho;
@@ -328,7 +405,7 @@ struct EpiPrimal {
     // starts a Halpern cycle) and its last step; on the other steps it is not stored.
     const bool store_hat = !P || step == P->K - 1 || P->inner0 + step == 0;
     if (store_hat) xh[j] = h;
-    xb[j] = static_cast<T>(2) * h - xj;
+    st_keep(xb + j, static_cast<T>(static_cast<T>(2) * h - xj));  // gathered by the dual kernel next
     x[j] = tw * (a * h + b * xj) + (static_cast<T>(1) - tw) * p.x0;
   }
 };
@@ -348,7 +425,7 @@ struct EpiDual {
     T y, y0, rl, ru;
   };
   __device__ bool active() const { return P == nullptr || !P->done; }
-  __device__ Pre load(int i) const { return Pre{y[i], y0[i], rl[i], ru[i]}; }
+  __device__ Pre load(int i) const { return Pre{ld_stream(y + i), ld_stream(y0 + i), ld_stream(rl + i), ld_stream(ru + i)}; }
   __device__ void operator()(int i, double s) const { (*this)(i, s, load(i)); }
   __device__ void operator()(int i, double s, const Pre& p) const {
     double sig_d = sigma, w_d = w, rho_d = rho;
@@ -369,7 +446,7 @@ struct EpiDual {
     } else if (!P) {
       yh[i] = h;
     }
-    y[i] = tw * (a * h + b * yi) + (static_cast<T>(1) - tw) * p.y0;
+    st_keep(y + i, static_cast<T>(tw * (a * h + b * yi) + (static_cast<T>(1) - tw) * p.y0));  // gathered next
   }
 };
 

@@ -58,7 +58,7 @@ def write_mps(lp, path, fixed=False, extras=None, name="GEN"):
     lines.append("COLUMNS")
     lines += extras.get("COLUMNS_PRE", [])
     for j in range(lp.num_cols):
-        if lp.c[j] != 0:
+        if lp.c[j] != 0 or lp.col_start[j] == lp.col_start[j + 1]:  # every column appears once at least
             lines.append(f("", f"X{j}", "COST", num(lp.c[j])))
         for p in range(lp.col_start[j], lp.col_start[j + 1]):
             lines.append(f("", f"X{j}", f"R{lp.row_index[p]}", num(lp.value[p])))
