@@ -52,8 +52,8 @@ WORKLOADS = {
                     "full_iterations": None},
 }
 # DRAM bytes per iteration (both fused kernels: dram__bytes_read.sum + dram__bytes_write.sum of
-# one launch each) from the ncu capture summarised in profiles/fused_spmv_random1m.md.
-NCU_TRAFFIC = {("random1m", "fp64"): 160.1e6 + 126.3e6}
+# one launch each) from the ncu capture summarised in profiles/k_slab_fed_random1m.md.
+NCU_TRAFFIC = {("random1m", "fp64"): 151.6e6 + 123.3e6}
 
 
 def make_lp(name):
@@ -405,6 +405,9 @@ def run_e2e(args, lp, world, limit):
     rl, ru = pin(lp.row_lower, torch.float64), pin(lp.row_upper, torch.float64)
     cs, ri, v = pin(lp.col_start, torch.int32), pin(lp.row_index, torch.int32), pin(lp.value, torch.float64)
     iters = 0
+    if args.warmup > 0:  # one untimed call: first-call costs (host allocations, caches) stay out
+        ps26119.solve_lp(c, (cs, ri, v), rl, ru, cl, cu, sense=lp.sense, offset=lp.offset, algorithm="r2hpdhg",
+                         precision=args.precision, iteration_limit=limit)
     t0 = time.perf_counter()
     for _ in range(args.e2e_steps):
         r = ps26119.solve_lp(c, (cs, ri, v), rl, ru, cl, cu, sense=lp.sense, offset=lp.offset, algorithm="r2hpdhg",
@@ -510,7 +513,7 @@ def main():
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--iterations", type=int, default=6400, help="iteration cap of one step")
     ap.add_argument("--full", action="store_true", help="solve to 1e-8 in every step")
-    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-sample-iterations", type=int, default=256)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -133,6 +133,8 @@ int solve_host(int num_rows, int num_cols, int sense, double obj_offset, const d
   if (nnz < 0) return invalid("col_start[n] < 0");
   if (nnz > 0 && (!row_index || !value)) return invalid("matrix arrays are NULL");
   try {
+    phase_log_begin(opt && opt->verbosity >= 1);
+    auto t_model = std::chrono::steady_clock::now();
     Model m;
     m.num_rows = num_rows;
     m.num_cols = num_cols;
@@ -146,10 +148,14 @@ int solve_host(int num_rows, int num_cols, int sense, double obj_offset, const d
     m.col_start.assign(col_start, col_start + num_cols + 1);
     m.row_index.assign(row_index, row_index + nnz);
     m.value.assign(value, value + nnz);
-    if (auto err = m.validate(); !err.empty()) return invalid(("invalid model: " + err).c_str());
+    if (auto err = m.validate(); !err.empty()) {
+      phase_log_begin(false);
+      return invalid(("invalid model: " + err).c_str());
+    }
+    phase_note("model", std::chrono::duration<double>(std::chrono::steady_clock::now() - t_model).count());
     Options o;
-    if (const char* bad = to_options(opt, num_rows, num_cols, o)) return invalid(bad);
-    if (const char* bad = apply_engine_options(eo, o)) return invalid(bad);
+    if (const char* bad = to_options(opt, num_rows, num_cols, o)) return phase_log_begin(false), invalid(bad);
+    if (const char* bad = apply_engine_options(eo, o)) return phase_log_begin(false), invalid(bad);
     const Solution s = solve(m, o);
     fill(s, result);
     fill_stats(s, s.engine_result.iterations > 0 ? num_rows : 0, num_cols, nnz);
@@ -162,16 +168,21 @@ int solve_host(int num_rows, int num_cols, int sense, double obj_offset, const d
     out(z, s.z, num_cols);
     out(dual_ray, s.dual_ray, num_rows);
     out(primal_ray, s.primal_ray, num_cols);
+    phase_note("call", std::chrono::duration<double>(std::chrono::steady_clock::now() - call_t0).count());
+    phase_log_end("solve_lp");
     return result->status;
   } catch (const std::bad_alloc&) {
+    phase_log_begin(false);
     result->status = PS26119_NOT_SOLVED;
     set_text(result->message, sizeof result->message, "out of memory");
     return result->status;
   } catch (const std::exception& e) {
+    phase_log_begin(false);
     result->status = PS26119_NUMERICAL_ERROR;
     set_text(result->message, sizeof result->message, e.what());
     return result->status;
   } catch (...) {
+    phase_log_begin(false);
     result->status = PS26119_NUMERICAL_ERROR;
     set_text(result->message, sizeof result->message, "unknown error");
     return result->status;

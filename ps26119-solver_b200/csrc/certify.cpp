@@ -12,6 +12,7 @@
 //   expansions     Shewchuk, "Adaptive precision floating-point arithmetic" (1997), GROW-EXPANSION
 //                  with zero elimination
 #include "certify.hpp"
+#include "parallel.hpp"
 
 #include <algorithm>
 #include <cmath>
@@ -149,21 +150,6 @@ struct SafeSum {
   }
   double error() const { return static_cast<double>(count + 2) * (kRel * abs_sum * 1.0000001 + kAbs); }
 };
-
-// Runs f(begin, end) over [0, n) on the host's threads (contiguous ranges; small n inline).
-template <class F>
-void parallel_ranges(long long n, F&& f) {
-  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-  const long long T = n < 65536 ? 1 : std::min<long long>(hw, 32);
-  if (T <= 1) {
-    f(0LL, n);
-    return;
-  }
-  std::vector<std::thread> th;
-  for (long long t = 1; t < T; ++t) th.emplace_back([&, t] { f(n * t / T, n * (t + 1) / T); });
-  f(0LL, n / T);
-  for (auto& x : th) x.join();
-}
 
 // The bound for multipliers y (already cleared where they point at an infinite row bound) and
 // column bounds [col_lo, col_up] (safe_bound.cpp:92-173).

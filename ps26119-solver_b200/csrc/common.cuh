@@ -282,6 +282,19 @@ inline int grid_for(std::int64_t n, int block = kBlock) {
   return static_cast<int>(g < 1 ? 1 : (g > (1LL << 30) ? (1LL << 30) : g));
 }
 
+// Streaming multiprocessors of the current device (cached per device).
+inline int sm_count() {
+  static int cached[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+  if (cached[dev] == 0) {
+    int n = 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+    cached[dev] = n;
+  }
+  return cached[dev];
+}
+
 // Grid-stride helper over [0, n).
 #define B200_FOR(i, n) \
   for (std::int64_t i = blockIdx.x * static_cast<std::int64_t>(blockDim.x) + threadIdx.x; i < (n); \

@@ -190,6 +190,7 @@ class Engine {
   long long pdlp_kernels_[2][2] = {}, pdlp_chk_kernels_[2][2][3] = {};
   DevBuf<double> res2_;
   DevBuf<int2> slab_a_, slab_t_;
+  int cap_a_ = kSlabTile, cap_t_ = kSlabTile;  // k_slab_fed tile capacities (largest slab, rounded up)
   PinnedBuf<double> hres2_;
   SumPlan plan_dist_;
   long long epoch_kernels_[2] = {0, 0}, check_kernels_[2][3] = {{0, 0, 0}, {0, 0, 0}};
@@ -225,6 +226,8 @@ void Engine::setup() {
   if (n > 0) k_slab_table<<<grid_for(slab_count(n)), kBlock, 0, st_>>>(n, M_.col_start, slab_t_.get());
   B200_LAUNCH_CHECK();
   kernels_ += 2;
+  cap_a_ = fed_tile_capacity(slab_max_nnz(slab_a_.get(), slab_count(m), st_));
+  cap_t_ = fed_tile_capacity(slab_max_nnz(slab_t_.get(), slab_count(n), st_));
   vd_.alloc(n, m);
   if (o_.mixed) vf_.alloc(n, m);
   params_.alloc(1);
@@ -371,9 +374,9 @@ void Engine::capture_epoch() {
   B200_CHECK(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
   auto step = [&](int s) {
     EpiPrimal<T> ep{v.x.get(), v.xh.get(), v.xb.get(), v.x0.get(), sp_.c<T>(), sp_.l<T>(), sp_.u<T>(), P, s, 0, 0, 0};
-    launch_slab_tma<T>(n, M_.col_start, sp_.t_ri.get(), sp_.At_val<T>(), v.y.get(), ep, st_, slab_t_.get());
+    launch_slab_fed<T>(n, sp_.t_rp.get(), sp_.t_ri.get(), sp_.At_val<T>(), v.y.get(), ep, st_, slab_t_.get(), cap_t_);
     EpiDual<T> ed{v.y.get(), v.yh.get(), v.yb.get(), v.y0.get(), sp_.rl<T>(), sp_.ru<T>(), P, s, 0, 0, 0, 0};
-    launch_slab_tma<T>(m, sp_.a_rp.get(), sp_.a_col.get(), sp_.A_val<T>(), v.xb.get(), ed, st_, slab_a_.get());
+    launch_slab_fed<T>(m, sp_.a_rp.get(), sp_.a_col.get(), sp_.A_val<T>(), v.xb.get(), ed, st_, slab_a_.get(), cap_a_);
     capture_count_ += 2;
   };
   B200_CHECK(cudaEventRecordWithFlags(ev_[0], st_, cudaEventRecordExternal));
@@ -875,9 +878,9 @@ void Engine::capture_pdlp_epoch(int phase) {
     T* yc = odd ? v.yh.get() : v.y.get();
     T* yn = odd ? v.y.get() : v.yh.get();
     EpiPdlpPrimal<T> ep{xc, sp_.c<T>(), sp_.l<T>(), sp_.u<T>(), xn, v.xb.get(), v.dx.get(), P, s};
-    launch_slab_tma<T>(n, M_.col_start, sp_.t_ri.get(), sp_.At_val<T>(), yc, ep, st_, slab_t_.get());
+    launch_slab_fed<T>(n, sp_.t_rp.get(), sp_.t_ri.get(), sp_.At_val<T>(), yc, ep, st_, slab_t_.get(), cap_t_);
     EpiPdlpDual<T> ed{yc, sp_.rl<T>(), sp_.ru<T>(), yn, v.dy.get(), P, s};
-    launch_slab_tma<T>(m, sp_.a_rp.get(), sp_.a_col.get(), sp_.A_val<T>(), v.xb.get(), ed, st_, slab_a_.get());
+    launch_slab_fed<T>(m, sp_.a_rp.get(), sp_.a_col.get(), sp_.A_val<T>(), v.xb.get(), ed, st_, slab_a_.get(), cap_a_);
     capture_count_ += 2;
   }
   B200_CHECK(cudaEventRecordWithFlags(ev_[1], st_, cudaEventRecordExternal));

@@ -54,6 +54,7 @@ struct ScaledDevice {
   long long nnz = 0;
   DeviceModel M;
   DevBuf<int> a_rp, a_col, t_ri;
+  DevBuf<int> t_rp;  // this library's copy of the caller's col_start (Ãᵀ row pointers, TMA-staged)
   DevBuf<double> a_v0, t_v0, sa, sat;
   DevBuf<float> saf, satf;
   DevBuf<double> row_scale, col_scale;
@@ -76,6 +77,8 @@ struct ScaledDevice {
     const std::size_t mm = static_cast<std::size_t>(m), nn = static_cast<std::size_t>(n);
     const std::size_t nz = static_cast<std::size_t>(nnz);
     a_rp.alloc(mm + 1);
+    t_rp.alloc(nn + 1);
+    B200_CHECK(cudaMemcpyAsync(t_rp.get(), dm.col_start, (nn + 1) * sizeof(int), cudaMemcpyDeviceToDevice, st));
     a_col.alloc(nz);
     a_v0.alloc(nz);
     t_ri.alloc(nz);

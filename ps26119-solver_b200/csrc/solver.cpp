@@ -4,15 +4,18 @@
 #include "solver.hpp"
 #include "batch.hpp"
 #include "certify.hpp"
+#include "parallel.hpp"
 
 #include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <sstream>
 #include <stdexcept>
+#include <thread>
 
 namespace b200 {
 
@@ -31,32 +34,62 @@ std::string Model::validate() const {  // model.cpp:93-151
   if (col_start[0] != 0) return "col_start[0] must be 0";
   if (row_index.size() != value.size()) return "row_index and value differ in size";
   if (static_cast<std::size_t>(col_start[n]) != value.size()) return "col_start[n] != nnz";
-  std::vector<int> seen(m, -1);
-  for (std::size_t j = 0; j < n; ++j) {
-    if (col_start[j + 1] < col_start[j]) {
-      err << "col_start not monotone at column " << j;
-      return err.str();
+  // Columns are checked in parallel ranges; each range reports its first failing column and the
+  // smallest such column's message is returned, the same message a sequential scan gives. The
+  // column pointers are scanned first: the parallel pass covers only the columns before the first
+  // one whose pointers decrease or pass nnz, so no range reads outside the entry arrays.
+  const std::size_t nnz = value.size();
+  std::size_t lim = n;
+  for (std::size_t j = 0; j < n; ++j)
+    if (col_start[j + 1] < col_start[j] || static_cast<std::size_t>(col_start[j + 1]) > nnz) {
+      lim = j;
+      break;
     }
-    if (!std::isfinite(obj[j])) {
-      err << "objective coefficient of column " << j << " is not finite";
-      return err.str();
+  // A column whose row indices are in range, strictly increasing and whose values are finite has
+  // no error: that is checked with sequential reads only. Any other column is examined by the
+  // entry-by-entry rules (first error in entry order), with a row-stamp array for duplicates.
+  auto column_error = [&](std::size_t j, std::vector<int>& seen) -> std::string {
+    if (!std::isfinite(obj[j])) return "objective coefficient of column " + std::to_string(j) + " is not finite";
+    bool clean = true;
+    int prev = -1;
+    for (int k = col_start[j]; k < col_start[j + 1] && clean; ++k) {
+      const int i = row_index[k];
+      clean = i > prev && static_cast<std::size_t>(i) < m && std::isfinite(value[k]);
+      prev = i;
     }
+    if (clean) return std::string();
+    if (seen.empty()) seen.assign(m, -1);
     for (int k = col_start[j]; k < col_start[j + 1]; ++k) {
       const int i = row_index[k];
-      if (i < 0 || static_cast<std::size_t>(i) >= m) {
-        err << "row index out of range in column " << j;
-        return err.str();
-      }
-      if (seen[i] == static_cast<int>(j)) {
-        err << "duplicate entry (" << i << "," << j << ")";
-        return err.str();
-      }
+      if (i < 0 || static_cast<std::size_t>(i) >= m) return "row index out of range in column " + std::to_string(j);
+      if (seen[i] == static_cast<int>(j))
+        return "duplicate entry (" + std::to_string(i) + "," + std::to_string(j) + ")";
       seen[i] = static_cast<int>(j);
-      if (!std::isfinite(value[k])) {
-        err << "matrix entry (" << i << "," << j << ") is not finite";
-        return err.str();
+      if (!std::isfinite(value[k]))
+        return "matrix entry (" + std::to_string(i) + "," + std::to_string(j) + ") is not finite";
+    }
+    return std::string();
+  };
+  std::vector<std::pair<std::size_t, std::string>> first;  // (column, message), one per failing range
+  std::mutex mu;
+  parallel_ranges(static_cast<long long>(lim), [&](long long jb, long long je) {
+    std::vector<int> seen;
+    for (long long j = jb; j < je; ++j) {
+      std::string e = column_error(static_cast<std::size_t>(j), seen);
+      if (!e.empty()) {
+        std::lock_guard<std::mutex> lock(mu);
+        first.emplace_back(static_cast<std::size_t>(j), std::move(e));
+        return;
       }
     }
+  });
+  if (!first.empty()) return std::min_element(first.begin(), first.end())->second;
+  if (lim < n) {  // the first column whose pointers decrease (one exists after a pointer past nnz)
+    for (std::size_t j = lim; j < n; ++j)
+      if (col_start[j + 1] < col_start[j]) {
+        err << "col_start not monotone at column " << j;
+        return err.str();
+      }
   }
   auto check_bounds = [&](const std::vector<double>& lo, const std::vector<double>& up, const char* what) {
     for (std::size_t k = 0; k < lo.size(); ++k) {
@@ -242,13 +275,22 @@ PresolveResult presolve(const Model& M) {  // presolve.cpp:22-156 (LP: no intege
   // indices (kept up to date as columns are removed), and its coefficient by a scan of that
   // column: the same (j, a) the reference finds by walking the row (presolve.cpp:60-66), with
   // no row-wise copy of A.
-  std::vector<int> row_xor(static_cast<std::size_t>(m), 0);
-  for (int j = 0; j < n; ++j)
-    for (int k = M.col_start[j]; k < M.col_start[j + 1]; ++k) row_xor[M.row_index[k]] ^= j;
+  // One pass over the entries, threads over column ranges: XOR and count are commutative, so
+  // relaxed integer atomics give the arrays of a sequential pass.
+  std::vector<int> row_xor(static_cast<std::size_t>(m), 0), row_cnt(static_cast<std::size_t>(m), 0);
+  parallel_ranges(n, [&](long long jb, long long je) {
+    for (long long jj = jb; jj < je; ++jj) {
+      const int j = static_cast<int>(jj);
+      for (int k = M.col_start[j]; k < M.col_start[j + 1]; ++k) {
+        const int i = M.row_index[k];
+        __atomic_fetch_xor(&row_xor[i], j, __ATOMIC_RELAXED);
+        __atomic_fetch_add(&row_cnt[i], 1, __ATOMIC_RELAXED);
+      }
+    }
+  });
   std::vector<double> rl = M.row_lower, ru = M.row_upper, cl = M.col_lower, cu = M.col_upper;
   std::vector<char> row_alive(m, 1), col_alive(n, 1);
-  std::vector<int> row_cnt(m), col_cnt(n);
-  for (int k = 0; k < static_cast<int>(M.nnz()); ++k) ++row_cnt[M.row_index[k]];
+  std::vector<int> col_cnt(n);
   for (int j = 0; j < n; ++j) col_cnt[j] = M.col_start[j + 1] - M.col_start[j];
   r.fixed_value.assign(n, kNaN);
   double offset = M.obj_offset;
@@ -343,21 +385,37 @@ PresolveResult presolve(const Model& M) {  // presolve.cpp:22-156 (LP: no intege
   R.row_lower.reserve(r.row_map.size());
   R.row_upper.reserve(r.row_map.size());
   R.col_start.push_back(0);
-  for (int j : r.col_map) {
-    R.obj.push_back(M.obj[j]);
-    R.col_lower.push_back(cl[j]);
-    R.col_upper.push_back(cu[j]);
-    if (r.removed_rows == 0) {  // row numbers unchanged: copy the column as it is
-      R.row_index.insert(R.row_index.end(), M.row_index.begin() + M.col_start[j],
-                         M.row_index.begin() + M.col_start[j + 1]);
-      R.value.insert(R.value.end(), M.value.begin() + M.col_start[j], M.value.begin() + M.col_start[j + 1]);
-    } else {
+  if (r.removed_rows == 0) {
+    // row numbers unchanged: the kept columns are copied as they are, one block per run of kept
+    // columns whose entries are contiguous (removed columns without entries do not break a run)
+    const int nk = static_cast<int>(r.col_map.size());
+    for (int q = 0; q < nk;) {
+      int e = q + 1;
+      while (e < nk && M.col_start[r.col_map[e]] == M.col_start[r.col_map[e - 1] + 1]) ++e;
+      const int k0 = M.col_start[r.col_map[q]], k1 = M.col_start[r.col_map[e - 1] + 1];
+      const int base = static_cast<int>(R.value.size()) - k0;
+      R.row_index.insert(R.row_index.end(), M.row_index.begin() + k0, M.row_index.begin() + k1);
+      R.value.insert(R.value.end(), M.value.begin() + k0, M.value.begin() + k1);
+      for (int c = q; c < e; ++c) {
+        const int j = r.col_map[c];
+        R.obj.push_back(M.obj[j]);
+        R.col_lower.push_back(cl[j]);
+        R.col_upper.push_back(cu[j]);
+        R.col_start.push_back(M.col_start[j + 1] + base);
+      }
+      q = e;
+    }
+  } else {
+    for (int j : r.col_map) {
+      R.obj.push_back(M.obj[j]);
+      R.col_lower.push_back(cl[j]);
+      R.col_upper.push_back(cu[j]);
       for (int p = M.col_start[j]; p < M.col_start[j + 1]; ++p) {
         const int i = M.row_index[p];
         if (new_row[i] >= 0) R.row_index.push_back(new_row[i]), R.value.push_back(M.value[p]);
       }
+      R.col_start.push_back(static_cast<int>(R.value.size()));
     }
-    R.col_start.push_back(static_cast<int>(R.value.size()));
   }
   for (int i : r.row_map) {
     R.row_lower.push_back(rl[i]);
@@ -388,8 +446,10 @@ Solution postsolve(const Model& M, const PresolveResult& r, const Solution& red)
     if ((zm > 0 && it->set_lower) || (zm < 0 && it->set_upper)) s.y[it->row] = z / it->a;
   }
   s.z = M.obj;
-  for (int j = 0; j < n; ++j)
-    for (int p = M.col_start[j]; p < M.col_start[j + 1]; ++p) s.z[j] -= M.value[p] * s.y[M.row_index[p]];
+  parallel_ranges(n, [&](long long jb, long long je) {  // each z_j in its own column order
+    for (long long j = jb; j < je; ++j)
+      for (int p = M.col_start[j]; p < M.col_start[j + 1]; ++p) s.z[j] -= M.value[p] * s.y[M.row_index[p]];
+  });
   s.objective = M.objective_value(s.x);
   if (!have_x) {
     s.x.clear();
@@ -434,6 +494,16 @@ const char* alg_name(Algorithm a) {
 }
 
 void note(Solution& s, const std::string& t) { s.message += std::string(s.message.empty() ? "" : "; ") + t; }
+
+thread_local std::vector<std::pair<const char*, double>>* g_phases = nullptr;
+
+// Times a scope as one phase of the current phase log.
+struct PhaseTimer {
+  const char* name;
+  clock_t_::time_point t0 = clock_t_::now();
+  explicit PhaseTimer(const char* n) : name(n) {}
+  ~PhaseTimer() { phase_note(name, since(t0)); }
+};
 
 EngineOptions engine_options(const Options& o) {  // engine.cpp:168-186
   EngineOptions e;
@@ -490,7 +560,16 @@ Solution solve_direct(const Model& model, const Options& options, bool certify =
   if (auto why = model.crossed_bounds(); !why.empty()) return trivially_infeasible(options, why);
   try {
     HostOutputs out;
+    const auto te = clock_t_::now();
     const EngineResult R = run_engine_host(model.view(), engine_options(options), out);
+    if (g_phases) {
+      const double total = since(te);
+      phase_note("engine.setup", R.setup_seconds);
+      phase_note("engine.loop", R.loop_seconds);
+      phase_note("engine.finish", R.finish_seconds);
+      phase_note("engine.teardown", R.teardown_seconds);
+      phase_note("engine.copies", total - R.setup_seconds - R.loop_seconds - R.finish_seconds - R.teardown_seconds);
+    }
     sol.status = R.status;
     sol.iterations = R.iterations;
     sol.objective = R.objective;
@@ -546,9 +625,11 @@ Solution solve_direct(const Model& model, const Options& options, bool certify =
     sol.status = Status::NumericalError;
     sol.message = e.what();
   }
-  if (certify && static_cast<int>(sol.y.size()) == model.num_rows && model.num_rows + model.num_cols > 0)
+  if (certify && static_cast<int>(sol.y.size()) == model.num_rows && model.num_rows + model.num_cols > 0) {
+    PhaseTimer pt("certified_bound");
     sol.certified_bound =
         certified_dual_bound(model, sol.y, within_bound_budget(since(t0), options.time_limit)).bound;
+  }
   sol.seconds = since(t0);
   return sol;
 }
@@ -564,6 +645,7 @@ Solution solve_impl(const Model& model, const Options& options) {
   const auto t0 = clock_t_::now();
   PresolveResult pr = presolve(model);
   const double presolve_s = since(t0);
+  phase_note("presolve", presolve_s);
   if (pr.outcome == PresolveResult::Outcome::Unchanged) {
     Solution s = solve_direct(model, options);
     s.presolve_seconds = presolve_s;
@@ -652,7 +734,11 @@ Solution solve_impl(const Model& model, const Options& options) {
   }
   if (red.status == Status::Infeasible || red.status == Status::Unbounded)
     return on_original(red, std::string("reduced model ") + status_name(red.status));
-  Solution post = postsolve(model, pr, red);
+  Solution post;
+  {
+    PhaseTimer pt("postsolve");
+    post = postsolve(model, pr, red);
+  }
   const std::string pnote = "presolve removed " + std::to_string(pr.removed_rows) + " rows, " +
                             std::to_string(pr.removed_cols) + " cols";
   post.message = post.message.empty() ? pnote : post.message + "; " + pnote;
@@ -719,7 +805,12 @@ Solution solve_impl(const Model& model, const Options& options) {
     if (options.tolerance >= 1e-6) return true;
     return pmax <= 1e-6 && dmax / (1.0 + cinf) <= 1e-6 && gap <= 1e-6;
   };
-  if (post.status == Status::Optimal && !passes(post)) {  // solve.cpp:414-450
+  bool passed = true;
+  if (post.status == Status::Optimal) {
+    PhaseTimer pt("original_kkt");
+    passed = passes(post);
+  }
+  if (post.status == Status::Optimal && !passed) {  // solve.cpp:414-450
     Options tight = inner;
     tight.tolerance = std::max(options.tolerance * 1e-2, 1e-13);
     tight.warm_x = red.x;
@@ -741,9 +832,11 @@ Solution solve_impl(const Model& model, const Options& options) {
   } else if (post.status == Status::Optimal && static_cast<int>(post.x.size()) != model.num_cols) {
     post.status = Status::NumericalError;
   }
-  if (static_cast<int>(post.y.size()) == model.num_rows && model.num_rows + model.num_cols > 0)
+  if (static_cast<int>(post.y.size()) == model.num_rows && model.num_rows + model.num_cols > 0) {
+    PhaseTimer pt("certified_bound");
     post.certified_bound =
         certified_dual_bound(model, post.y, within_bound_budget(since(t0), options.time_limit)).bound;
+  }
   post.presolve_seconds = presolve_s;
   post.seconds = since(t0);
   return post;
@@ -828,6 +921,7 @@ Solution solve_unguarded(const Model& model, const Options& options) {  // solve
     }
     if (device) {
       s = solve_impl(model, resolved);
+      PhaseTimer pt("gate");
       gate(model, resolved, s);
     }
   }
@@ -836,6 +930,26 @@ Solution solve_unguarded(const Model& model, const Options& options) {  // solve
 }
 
 }  // namespace
+
+void phase_log_begin(bool on) {
+  delete g_phases;
+  g_phases = on ? new std::vector<std::pair<const char*, double>>() : nullptr;
+}
+void phase_note(const char* name, double seconds) {
+  if (g_phases) g_phases->emplace_back(name, seconds);
+}
+void phase_log_end(const char* what) {
+  if (!g_phases) return;
+  std::string line = std::string("ps26119-b200 ") + what + " phases:";
+  char buf[96];
+  for (const auto& [name, sec] : *g_phases) {
+    std::snprintf(buf, sizeof buf, " %s %.1f ms", name, 1e3 * sec);
+    line += buf;
+  }
+  std::fprintf(stderr, "%s\n", line.c_str());
+  delete g_phases;
+  g_phases = nullptr;
+}
 
 Solution solve(const Model& model, const Options& options) {  // solve.cpp:194-210
   try {

@@ -109,6 +109,13 @@ Solution postsolve(const Model& original, const PresolveResult& r, const Solutio
 // The library entry point: never throws (solve.cpp:194-210).
 Solution solve(const Model& model, const Options& options);
 
+// Host phase timings of one entry-point call: phase_log_begin(on) starts a log on this thread
+// (nothing is recorded when `on` is false), phase_note adds one phase, phase_log_end prints the
+// phases to stderr on one line and closes the log.
+void phase_log_begin(bool on);
+void phase_note(const char* name, double seconds);
+void phase_log_end(const char* what);
+
 // Differences from the base model; an empty vector means "same as the base" (batch.h:22-28).
 struct Scenario {
   std::vector<double> obj, col_lower, col_upper, row_lower, row_upper;

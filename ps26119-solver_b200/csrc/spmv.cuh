@@ -15,7 +15,9 @@
 
 #include <algorithm>
 #include <cstddef>
+#include <cstdint>
 #include <type_traits>
+#include <vector>
 
 #include "common.cuh"
 
@@ -50,7 +52,20 @@ namespace b200 {
 #define B200_EPI_HINTS 1
 #endif
 
-constexpr int kSlabRows = 256;
+// 1: the iteration kernels stage their epilogue operands and row pointers by TMA as well
+// (k_slab_fed); 0: they use k_slab.
+#ifndef B200_SLAB_FED
+#define B200_SLAB_FED 1
+#endif
+
+#ifndef B200_SLAB_ROWS
+#define B200_SLAB_ROWS 256
+#endif
+#ifndef B200_GATHER_BATCH
+#define B200_GATHER_BATCH 4
+#endif
+
+constexpr int kSlabRows = B200_SLAB_ROWS;  // rows per slab = threads per block
 constexpr int kSlabTile = 2048;  // nonzeros staged per tile
 constexpr int kTilePad = 8;      // room for the 16-byte widening of a bulk copy
 
@@ -154,6 +169,28 @@ __device__ __forceinline__ void st_keep(T* p, T v) {
 #endif
 }
 
+// The gathered operand x[col] of the row products. B200_GATHER_NA=1 loads it with
+// L1::no_allocate (the gathers have almost no L1 reuse).
+#ifndef B200_GATHER_NA
+#define B200_GATHER_NA 1
+#endif
+template <class T>
+__device__ __forceinline__ double gather(const T* __restrict__ x, int i) {
+#if B200_GATHER_NA
+  if constexpr (sizeof(T) == 8) {
+    double v;
+    asm volatile("ld.global.nc.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(x + i));
+    return v;
+  } else {
+    float v;
+    asm volatile("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(x + i));
+    return static_cast<double>(v);
+  }
+#else
+  return static_cast<double>(x[i]);
+#endif
+}
+
 // Epilogues may prefetch their operands: `Pre load(int row)` is issued at kernel entry, before
 // the nonzeros are staged, so its latency overlaps the SpMV; `operator()(row, s, pre)` then
 // finishes the update. Epilogues that take maxima expose `Acc` (fields written by the
@@ -188,7 +225,7 @@ __device__ __forceinline__ void epi_flush(const E& e, const A& acc) {
   if constexpr (!std::is_same<A, NoAcc>::value) e.flush(acc);
 }
 
-constexpr int kGatherBatch = 8;  // independent x-gathers issued per round trip
+constexpr int kGatherBatch = B200_GATHER_BATCH;  // independent x-gathers issued per round trip
 
 // Row-sequential fp64 accumulation of `rows` CSR rows; calls the epilogue with (row, s).
 // kTma: the tiles of col/val are staged by TMA bulk copies (the arrays must be this library's
@@ -240,11 +277,14 @@ __global__ void __launch_bounds__(kSlabRows, B200_SLAB_MIN_BLOCKS) k_slab(int ro
         tma_load_1d(sm.col, col + c0, cb, &sm.bar);
         tma_load_1d(sm.val, val + v0, vb, &sm.bar);
       }
-      const bool ok = mbar_wait_bounded(&sm.bar, phase);
+      // thread 0 waits; the others sleep in the barrier instead of spinning on the barrier word
+      const int ok = threadIdx.x == 0 ? (mbar_wait_bounded(&sm.bar, phase) ? 1 : 0) : 1;
       phase ^= 1u;
-      if (!__syncthreads_and(ok ? 1 : 0)) {  // never expected: record, drain, give up on the tile
-        if (threadIdx.x == 0) atomicAdd(&g_stage_timeouts, 1u);
-        mbar_wait_bounded(&sm.bar, phase ^ 1u);
+      if (!__syncthreads_and(ok)) {  // never expected: record, drain, give up on the tile
+        if (threadIdx.x == 0) {
+          atomicAdd(&g_stage_timeouts, 1u);
+          mbar_wait_bounded(&sm.bar, phase ^ 1u);
+        }
         staged = false;
         break;
       }
@@ -283,6 +323,145 @@ __global__ void __launch_bounds__(kSlabRows, B200_SLAB_MIN_BLOCKS) k_slab(int ro
   epi_flush(epi, acc);
 }
 
+// ---------------------------------------------------------------------- fully staged form
+// k_slab_fed: the row products and epilogue of k_slab, with every streamed operand of the slab
+// brought in by TMA bulk copies issued at block entry: the slab's row pointers and the
+// epilogue's per-row operand vectors (Epi::vec(k), rows r0 … r0+nr) on one barrier, the col/val
+// tile on another. Threads hold no operand registers while the gathers are in flight (lower
+// register use), and the start of a slab waits on one DRAM round trip (the copies, all issued
+// together) instead of a chain of them. The slab's nonzero range comes from the L2-resident slab
+// table. Sums are k_slab's sequential CSR-order sums.
+//
+// The tile capacity `cap` is chosen per matrix (the largest slab, rounded up; see
+// fed_tile_capacity) and the shared memory is sized to it: the gathers' outstanding L1 misses
+// need L1 capacity, which shared memory takes away. A slab with more than `cap` nonzeros is
+// summed in several tiles. Only thread 0 waits on the barriers; the other threads sleep in
+// __syncthreads instead of spinning on the shared-memory barrier word.
+// Requirements (checked on the host): rp, col, val and every Epi::vec(k) are this library's
+// 16-byte-aligned, tail-padded allocations.
+struct FedLayout {
+  unsigned rp, vec, col, val, bytes;  // byte offsets into the dynamic shared memory, and its size
+};
+// bar[2] (16 bytes) and the slab's nonzero range (8 bytes) come first.
+__host__ __device__ constexpr FedLayout fed_layout(int vecs, int elem, int cap) {
+  const unsigned rp = 32u;
+  const unsigned vec = rp + static_cast<unsigned>(kSlabRows + kTilePad) * 4u;
+  const unsigned col = vec + static_cast<unsigned>(vecs * kSlabRows * elem);
+  const unsigned val = col + static_cast<unsigned>(cap + kTilePad) * 4u;
+  const unsigned bytes = val + static_cast<unsigned>((cap + kTilePad) * elem);
+  return FedLayout{rp, vec, col, val, bytes};
+}
+// Tile capacity for a matrix whose largest slab has `max_slab_nnz` nonzeros: a multiple of 16,
+// at least 16, at most kSlabTile.
+inline int fed_tile_capacity(long long max_slab_nnz) {
+  const long long c = (std::max(16LL, max_slab_nnz) + 15) / 16 * 16;
+  return static_cast<int>(std::min<long long>(c, kSlabTile));
+}
+
+#ifndef B200_FED_MIN_BLOCKS
+#define B200_FED_MIN_BLOCKS 5
+#endif
+
+template <class T, class Epi>
+__global__ void __launch_bounds__(kSlabRows, B200_FED_MIN_BLOCKS) k_slab_fed(int rows, const int* __restrict__ rp,
+                                                           const int* __restrict__ col,
+                                                           const T* __restrict__ val,
+                                                           const T* __restrict__ x, Epi epi,
+                                                           const int2* __restrict__ slab, int cap) {
+  constexpr int V = Epi::kVecs;
+  constexpr int kValAlign = 16 / static_cast<int>(sizeof(T));
+  extern __shared__ __align__(16) unsigned char fed_smem[];
+  if (!epi.active()) return;
+  const FedLayout L = fed_layout(V, static_cast<int>(sizeof(T)), cap);
+  unsigned long long* bar = reinterpret_cast<unsigned long long*>(fed_smem);  // [0] rp + vectors, [1] tile
+  int2* krange = reinterpret_cast<int2*>(fed_smem + 16);
+  int* s_rp = reinterpret_cast<int*>(fed_smem + L.rp);
+  T* s_vec = reinterpret_cast<T*>(fed_smem + L.vec);
+  int* s_col = reinterpret_cast<int*>(fed_smem + L.col);
+  T* s_val = reinterpret_cast<T*>(fed_smem + L.val);
+  const int tid = static_cast<int>(threadIdx.x);
+  const int r0 = blockIdx.x * kSlabRows;
+  const int nr = min(kSlabRows, rows - r0);
+  auto issue_tile = [&](int t0, int t1) {  // thread 0
+    const int c0 = t0 & ~3, v0 = t0 & ~(kValAlign - 1);
+    const int c1 = (t1 + 3) & ~3, v1 = (t1 + kValAlign - 1) & ~(kValAlign - 1);
+    const unsigned cb = static_cast<unsigned>(c1 - c0) * 4u, vb = static_cast<unsigned>(v1 - v0) * sizeof(T);
+    mbar_expect_tx(&bar[1], cb + vb);
+    tma_load_1d(s_col, col + c0, cb, &bar[1]);
+    tma_load_1d(s_val, val + v0, vb, &bar[1]);
+  };
+  bool tile_pending = false;  // thread 0: a tile copy not yet waited for
+  if (tid == 0) {
+    mbar_init(&bar[0]);
+    mbar_init(&bar[1]);
+    const unsigned rb = (static_cast<unsigned>(nr + 1) * 4u + 15u) & ~15u;
+    const unsigned vb = (static_cast<unsigned>(nr) * sizeof(T) + 15u) & ~15u;
+    mbar_expect_tx(&bar[0], rb + V * vb);
+    tma_load_1d(s_rp, rp + r0, rb, &bar[0]);
+#pragma unroll
+    for (int k = 0; k < V; ++k) tma_load_1d(s_vec + k * kSlabRows, epi.vec(k) + r0, vb, &bar[0]);
+    const int2 kr = slab ? ld_keep(slab + blockIdx.x) : make_int2(__ldg(rp + r0), __ldg(rp + r0 + nr));
+    *krange = kr;
+    if (kr.x < kr.y) {
+      issue_tile(kr.x, min(kr.x + cap, kr.y));
+      tile_pending = true;
+    }
+  }
+  int ok = 1;
+  if (tid == 0) ok = mbar_wait_bounded(&bar[0], 0) ? 1 : 0;
+  bool staged = __syncthreads_and(ok) != 0;
+  const int2 kr = *krange;
+  const bool mine = tid < nr;
+  int beg = 0, end = 0;
+  if (staged && mine) beg = s_rp[tid], end = s_rp[tid + 1];
+  auto acc = epi_acc(epi, 0);
+  unsigned phase = 0;
+  double s = 0.0;
+  for (int t0 = kr.x; staged && t0 < kr.y; t0 += cap) {
+    const int t1 = min(t0 + cap, kr.y);
+    if (t0 != kr.x) {  // later tiles of a long slab: reuse the buffer once the previous tile is summed
+      __syncthreads();
+      if (tid == 0) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        issue_tile(t0, t1);
+        tile_pending = true;
+      }
+    }
+    if (tid == 0) {
+      ok = mbar_wait_bounded(&bar[1], phase) ? 1 : 0;
+      if (ok) phase ^= 1u, tile_pending = false;
+    }
+    if (!__syncthreads_and(ok)) {
+      staged = false;
+      break;
+    }
+    const int c0 = t0 & ~3, v0 = t0 & ~(kValAlign - 1);
+    const int a = max(beg, t0), b = min(end, t1);
+    for (int k = a; k < b; k += kGatherBatch) {
+      double p[kGatherBatch];
+#pragma unroll
+      for (int q = 0; q < kGatherBatch; ++q)
+        p[q] = (k + q < b) ? static_cast<double>(s_val[k + q - v0]) * gather(x, s_col[k + q - c0]) : 0.0;
+#pragma unroll
+      for (int q = 0; q < kGatherBatch; ++q)
+        if (k + q < b) s += p[q];  // in CSR order
+    }
+  }
+  if (!staged) {  // never expected: record, wait (bounded) for copies still in flight, report NaN
+    if (tid == 0) {
+      atomicAdd(&g_stage_timeouts, 1u);
+      mbar_wait_bounded(&bar[0], 0);
+      if (tile_pending) mbar_wait_bounded(&bar[1], phase);
+    }
+    s = __longlong_as_double(0x7ff8000000000000LL);
+  }
+  if (mine) {
+    const auto pre = staged ? epi.pre_at(s_vec, tid) : epi.load(r0 + tid);
+    epi_apply(epi, r0 + tid, s, pre, acc);
+  }
+  epi_flush(epi, acc);
+}
+
 // Once per instantiation, outside any stream capture: prefer shared memory so that 8 CTAs of
 // 24.6 KB fit on an SM.
 template <class T, class Epi, bool kTma>
@@ -315,6 +494,24 @@ inline void launch_slab_tma(int rows, const int* rp, const int* col, const T* va
   launch_slab<T, Epi, B200_STAGE_TMA != 0>(rows, rp, col, val, x, epi, st, B200_SLAB_TABLE ? slab : nullptr);
 }
 
+// The fully staged form (k_slab_fed) for the iteration epilogues, whose operand vectors are
+// library allocations; `rp` must be one too, `slab` the slab table of rp and `cap` the tile
+// capacity from fed_tile_capacity. Falls back to launch_slab_tma when an operand is not 16-byte
+// aligned or the shared memory would exceed the 48 KB that needs no opt-in.
+template <class T, class Epi>
+inline void launch_slab_fed(int rows, const int* rp, const int* col, const T* val, const T* x, const Epi& epi,
+                            cudaStream_t st, const int2* slab, int cap) {
+  if (rows <= 0) return;
+  const FedLayout L = fed_layout(Epi::kVecs, static_cast<int>(sizeof(T)), cap);
+  bool ok = B200_SLAB_FED && B200_STAGE_TMA && cap >= 16 && cap % 16 == 0 && L.bytes <= 48u * 1024u &&
+            (reinterpret_cast<std::uintptr_t>(rp) & 15u) == 0;
+  for (int k = 0; k < Epi::kVecs; ++k) ok = ok && (reinterpret_cast<std::uintptr_t>(epi.vec(k)) & 15u) == 0;
+  if (!ok) return launch_slab_tma<T>(rows, rp, col, val, x, epi, st, slab);
+  const int grid = (rows + kSlabRows - 1) / kSlabRows;
+  k_slab_fed<T, Epi><<<grid, kSlabRows, L.bytes, st>>>(rows, rp, col, val, x, epi, slab, cap);
+  B200_LAUNCH_CHECK();
+}
+
 // The nonzero range [rp[b·kSlabRows], rp[min((b+1)·kSlabRows, rows)]) of every slab b.
 static __global__ void k_slab_table(int rows, const int* rp, int2* out) {
   const int nb = (rows + kSlabRows - 1) / kSlabRows;
@@ -324,6 +521,17 @@ static __global__ void k_slab_table(int rows, const int* rp, int2* out) {
   }
 }
 inline int slab_count(int rows) { return rows <= 0 ? 0 : (rows + kSlabRows - 1) / kSlabRows; }
+
+// The largest slab's nonzero count, from a slab table (synchronises `st`; setup only).
+inline long long slab_max_nnz(const int2* table, int nb, cudaStream_t st) {
+  if (nb <= 0) return 0;
+  std::vector<int2> h(static_cast<std::size_t>(nb));
+  B200_CHECK(cudaMemcpyAsync(h.data(), table, h.size() * sizeof(int2), cudaMemcpyDeviceToHost, st));
+  B200_CHECK(cudaStreamSynchronize(st));
+  long long mx = 0;
+  for (const int2& r : h) mx = std::max<long long>(mx, static_cast<long long>(r.y) - r.x);
+  return mx;
+}
 
 // Number of bulk-copy waits that ran out since the library was loaded (host side).
 inline unsigned stage_timeouts() {
@@ -392,6 +600,12 @@ struct EpiPrimal {
   __device__ Pre load(int j) const {
     return Pre{ld_stream(x + j), ld_stream(x0 + j), ld_stream(c + j), ld_stream(l + j), ld_stream(u + j)};
   }
+  // The streamed operands as arrays (k_slab_fed stages their slab ranges in shared memory).
+  static constexpr int kVecs = 5;
+  __host__ __device__ const T* vec(int k) const { return k == 0 ? x : k == 1 ? x0 : k == 2 ? c : k == 3 ? l : u; }
+  __device__ Pre pre_at(const T* sv, int t) const {
+    return Pre{sv[t], sv[kSlabRows + t], sv[2 * kSlabRows + t], sv[3 * kSlabRows + t], sv[4 * kSlabRows + t]};
+  }
   __device__ void operator()(int j, double s) const { (*this)(j, s, load(j)); }
   __device__ void operator()(int j, double s, const Pre& p) const {
     double tau_d = tau, w_d = w, rho_d = rho;
@@ -426,6 +640,11 @@ struct EpiDual {
   };
   __device__ bool active() const { return P == nullptr || !P->done; }
   __device__ Pre load(int i) const { return Pre{ld_stream(y + i), ld_stream(y0 + i), ld_stream(rl + i), ld_stream(ru + i)}; }
+  static constexpr int kVecs = 4;
+  __host__ __device__ const T* vec(int k) const { return k == 0 ? y : k == 1 ? y0 : k == 2 ? rl : ru; }
+  __device__ Pre pre_at(const T* sv, int t) const {
+    return Pre{sv[t], sv[kSlabRows + t], sv[2 * kSlabRows + t], sv[3 * kSlabRows + t]};
+  }
   __device__ void operator()(int i, double s) const { (*this)(i, s, load(i)); }
   __device__ void operator()(int i, double s, const Pre& p) const {
     double sig_d = sigma, w_d = w, rho_d = rho;
@@ -467,6 +686,11 @@ struct EpiPdlpPrimal {
   };
   __device__ bool active() const { return !P->done; }
   __device__ Pre load(int j) const { return Pre{x[j], c[j], l[j], u[j], xa[j]}; }
+  static constexpr int kVecs = 5;
+  __host__ __device__ const T* vec(int k) const { return k == 0 ? x : k == 1 ? c : k == 2 ? l : k == 3 ? u : xa; }
+  __device__ Pre pre_at(const T* sv, int t) const {
+    return Pre{sv[t], sv[kSlabRows + t], sv[2 * kSlabRows + t], sv[3 * kSlabRows + t], sv[4 * kSlabRows + t]};
+  }
   __device__ void operator()(int j, double s) const { (*this)(j, s, load(j)); }
   __device__ void operator()(int j, double s, const Pre& p) const {
     const T t = static_cast<T>(P->tau);
@@ -489,6 +713,11 @@ struct EpiPdlpDual {
   };
   __device__ bool active() const { return !P->done; }
   __device__ Pre load(int i) const { return Pre{y[i], rl[i], ru[i], ya[i]}; }
+  static constexpr int kVecs = 4;
+  __host__ __device__ const T* vec(int k) const { return k == 0 ? y : k == 1 ? rl : k == 2 ? ru : ya; }
+  __device__ Pre pre_at(const T* sv, int t) const {
+    return Pre{sv[t], sv[kSlabRows + t], sv[2 * kSlabRows + t], sv[3 * kSlabRows + t]};
+  }
   __device__ void operator()(int i, double s) const { (*this)(i, s, load(i)); }
   __device__ void operator()(int i, double s, const Pre& p) const {
     const T sg = static_cast<T>(P->sigma);
