@@ -53,7 +53,7 @@ WORKLOADS = {
 }
 # DRAM bytes per iteration (both fused kernels: dram__bytes_read.sum + dram__bytes_write.sum of
 # one launch each) from the ncu capture summarised in profiles/k_slab_fed_random1m.md.
-NCU_TRAFFIC = {("random1m", "fp64"): 151.6e6 + 123.3e6}
+NCU_TRAFFIC = {("random1m", "fp64"): 152.4e6 + 123.5e6}
 
 
 def make_lp(name):
@@ -390,11 +390,31 @@ def run_ours(args, rank, world, local):
                   "check": r.check, "setup_s": st["setup_seconds"], "loop_s": st["loop_seconds"],
                   "finish_s": st["finish_seconds"], "checks": st["checks"], "restarts": st["restarts"]},
     }
+    g = gather_ceiling(lp.num_rows if args.workload.startswith("random") else None, lp)
+    if g:  # the second ceiling: 2·nnz random gathers of x̄ / y per iteration
+        achieved_g = 2 * lp.nnz / (iter_ms * 1e-3)
+        line["roofline"]["gather"] = {"achieved_gathers_per_s": achieved_g, "peak_gathers_per_s": g["gathers_per_s"],
+                                      "frac": achieved_g / g["gathers_per_s"],
+                                      "peak_source": "measured live by lib/gather_rate (random 8-byte gathers "
+                                                     f"of a {lp.num_cols:,}-element vector resident in L2)"}
     if not args.no_e2e:
         line["e2e"] = run_e2e(args, lp, world, limit)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = reference_sample(args, lp, iters_per_step, full)
     return line
+
+
+def gather_ceiling(m, lp):
+    """Runs lib/gather_rate (built with the library) for this matrix's shape: random gathers from
+    an n-element vector, nnz of them. None when the program is absent or fails."""
+    exe = os.path.join(ROOT, "ps26119-solver_b200", "lib", "gather_rate")
+    if m is None or not os.path.exists(exe):
+        return None
+    try:
+        r = subprocess.run([exe, str(lp.num_cols), str(lp.nnz)], capture_output=True, text=True, timeout=120)
+        return json.loads(r.stdout.strip().splitlines()[-1]) if r.returncode == 0 else None
+    except (subprocess.SubprocessError, ValueError, IndexError):
+        return None
 
 
 def run_e2e(args, lp, world, limit):
