@@ -1,7 +1,8 @@
-"""Benchmark of the B200 r²HPDHG engine on the 1M x 1.5M random LP (BASELINE config 2 shape).
+"""Benchmark of the B200 r²HPDHG engine on the 1M x 1.5M random LP and the other workloads below.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload random1m|random10k|staircase8760|batch720x64] [--precision fp64|mixed]
+                    [--workload random1m|random10k|staircase8760|batch720x64|serve48]
+                    [--precision fp64|mixed]
                     [--iterations L | --full]
 
 One STEP is one cold solve of the seeded LP on the device: setup (structure, scaling, ‖Ã‖₂),
@@ -50,6 +51,10 @@ WORKLOADS = {
     "batch720x64": {"desc": "64 scenarios (b, c x lognormal(0, 0.1)) of the staircase LP T=720 "
                             "(35,280 x 43,200, 126,024 nnz), seed 1", "kind": "batch", "T": 720, "K": 64,
                     "full_iterations": None},
+    "serve48": {"desc": "48 LP requests from the random-LP generator, m log-uniform in [1e3, 2e4] (n = 1.5m, "
+                        "6 nnz/row), Poisson arrivals, each solved to 1e-8 (a bounded sample of the "
+                        "2,000-request stream with m up to 2e5), seed 1", "kind": "serve", "N": 48,
+                "m_lo": 1_000, "m_hi": 20_000, "slots": 16, "full_iterations": None},
 }
 # DRAM bytes per iteration (both fused kernels: dram__bytes_read.sum + dram__bytes_write.sum of
 # one launch each) from the ncu capture summarised in profiles/k_slab_fed_random1m.md.
@@ -65,6 +70,91 @@ def make_lp(name):
 def make_scenarios(name, lp):
     from ps26119 import generators as g
     return g.scenarios(lp, WORKLOADS[name]["K"], sigma=0.1, seed=1)
+
+
+def make_requests(name):
+    from ps26119 import generators as g
+    w = WORKLOADS[name]
+    rng = np.random.default_rng(1)
+    ms = np.exp(rng.uniform(np.log(w["m_lo"]), np.log(w["m_hi"]), w["N"])).astype(int)
+    return [g.random_lp(int(m), seed=1000 + k) for k, m in enumerate(ms)]
+
+
+def run_serve(args, rank, world, local):
+    """The request loop (ps26119_server_*): one step = one stream of N requests arriving as a
+    Poisson process, admitted by slots and HBM budget, each solved to 1e-8 (mixed precision with
+    its fp64 polish, or fp64). value = served solves/s over the stream (first submission to last
+    completion); latency = completion − submission. The sequential baseline is a sample of the
+    same requests solved one at a time in plain fp64 through ps26119_solve_lp_ex; the arrival
+    rate is slots × that sequential rate, so the device stays saturated."""
+    import torch
+    import ps26119
+    torch.cuda.set_device(local)
+    w = WORKLOADS[args.workload]
+    reqs = make_requests(args.workload)
+    N, slots = len(reqs), w["slots"]
+
+    def alone(lp, precision="fp64"):
+        return ps26119.solve_lp(lp.c, (lp.col_start, lp.row_index, lp.value), lp.row_lower, lp.row_upper,
+                                lp.col_lower, lp.col_upper, sense=lp.sense, offset=lp.offset, algorithm="r2hpdhg",
+                                precision=precision)
+
+    alone(min(reqs, key=lambda lp: lp.num_rows))  # warm-up: first-call costs stay out
+    S = min(N, args.serve_sample)
+    seq = []
+    for lp in reqs[:S]:
+        t0 = time.perf_counter()
+        r = alone(lp)
+        seq.append(time.perf_counter() - t0)
+        if r.status != ps26119.OPTIMAL:
+            raise RuntimeError(f"sequential solve ended {r.status_name}")
+    t_seq = float(np.mean(seq))
+    rate = slots / t_seq
+    gaps = np.random.default_rng(2).exponential(1.0 / rate, N)
+    steps = []
+    with clock_sampler(local) as clocks:
+        for _ in range(args.steps):
+            with ps26119.Server(slots=slots) as srv:
+                t0 = time.perf_counter()
+                ids, due = [], 0.0
+                for lp, gap in zip(reqs, gaps):
+                    due += gap
+                    pause = due - (time.perf_counter() - t0)
+                    if pause > 0:
+                        time.sleep(pause)
+                    ids.append(srv.submit(lp, precision=args.precision))
+                out = [srv.result(i) for i in ids]
+            bad = [r.status_name for r, _ in out if r.status != ps26119.OPTIMAL or r.check != "PASS"]
+            if bad:
+                raise RuntimeError(f"served solves ended {sorted(set(bad))}")
+            sub = np.array([t[0] for _, t in out])
+            fin = np.array([t[2] for _, t in out])
+            steps.append((fin.max() - sub.min(), fin - sub, [r.iterations for r, _ in out]))
+    sec = max_over_ranks(float(np.mean([s[0] for s in steps])), world)
+    lat = np.concatenate([s[1] for s in steps])
+    value = world * N / sec
+    h2d = sum(lp.nnz * 12 + (lp.num_cols + 1) * 4 + lp.num_cols * 24 + lp.num_rows * 16 for lp in reqs)
+    d2h = sum(lp.num_cols * 16 + lp.num_rows * 8 for lp in reqs)
+    unit = "solves/s"
+    return {
+        "metric": f"served LP solves/s on {args.workload} ({args.precision}, p50/p99 latency)", "value": value,
+        "unit": unit, "n_gpus": world, "steps": args.steps, "warmup": 1, "ms_per_step": sec * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "f32+f64", "data": "synthetic (seeded generator)",
+        "config": {"workload": w["desc"], "requests": N, "slots": slots, "precision": args.precision,
+                   "tolerance": 1e-8, "arrival_rate_per_s": rate, "rows": [int(lp.num_rows) for lp in reqs],
+                   "entry": "ps26119_server_submit / ps26119_server_poll (host arrays)",
+                   "parallelism": f"replicas x{world}", "l2": "many small LPs: L2-resident, latency-bound"},
+        "latency_ms": {"p50": float(np.percentile(lat, 50) * 1e3), "p99": float(np.percentile(lat, 99) * 1e3),
+                       "mean": float(lat.mean() * 1e3)},
+        "sequential_fp64": {"solves_per_s": 1.0 / t_seq, "speedup": value * t_seq / world,
+                            "sample": f"{S} of the requests solved one at a time, plain fp64, ps26119_solve_lp_ex"},
+        "iterations": steps[-1][2],
+        "gpu_launches": None,
+        "clocks": clocks.summary(),
+        "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "note": "the server takes host arrays: every request's copies are inside the stream's time"},
+    }
 
 
 def run_batch(args, rank, world, local):
@@ -471,6 +561,9 @@ def run_reference(args, rank, world):
     import reference
     if not reference.available():
         return {"impl": "reference", "unavailable": "reference library oracle/_ref was not built on this machine"}
+    if WORKLOADS[args.workload]["kind"] == "serve":
+        return {"impl": "reference", "unavailable": "the reference solves the 48 requests to 1e-8 one at a time on "
+                "the CPU (about a minute per request); no bounded sample of a latency stream is meaningful"}
     lp = make_lp(args.workload)
     cores = os.cpu_count() or 1
     if WORKLOADS[args.workload]["kind"] == "batch":
@@ -537,12 +630,15 @@ def main():
     ap.add_argument("--cpu-sample-iterations", type=int, default=256)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve-sample", type=int, default=8, help="requests solved sequentially for the baseline")
     args = ap.parse_args()
     rank, world, local = dist_setup()
     if args.impl == "reference":
         line = run_reference(args, rank, world)
     elif WORKLOADS[args.workload]["kind"] == "batch":
         line = run_batch(args, rank, world, local)
+    elif WORKLOADS[args.workload]["kind"] == "serve":
+        line = run_serve(args, rank, world, local)
     else:
         line = run_ours(args, rank, world, local)
     if rank == 0 and line is not None:

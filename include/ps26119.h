@@ -218,6 +218,48 @@ PS26119_API int ps26119_solve_batch(int num_rows, int num_cols, int sense, doubl
                                     const ps26119_options* opt, const ps26119_engine_options* engine,
                                     ps26119_result* results, double* x, double* y, double* z);
 
+/* ---- Serving: a request loop for independent LPs on one GPU (continuous batching).
+ * No reference counterpart: the reference solves one LP per call. Requests are admitted in
+ * arrival order when one of `slots` is free and the device memory the request needs fits in the
+ * HBM budget left by the requests running (the first request in flight is always admitted). Each
+ * slot runs the same solve as ps26119_solve_lp_ex (presolve, the GPU engine on the slot's own
+ * stream, the gate), so a request's result equals that call's result; requests that arrive while
+ * others run start as slots and memory free up, and their work overlaps on the device. */
+typedef struct ps26119_server ps26119_server;
+
+typedef struct {
+  int slots;               /* requests solved at the same time (0 = 8) */
+  double hbm_budget_bytes; /* device memory for the running requests (0 = 80% of free memory) */
+  double dry_run_seconds;  /* > 0: requests are admitted and timed but not solved (each holds its
+                              slot and memory this long); status NOT_SOLVED, engine "dry-run" */
+} ps26119_server_options;
+
+typedef struct {
+  double submitted, started, finished; /* seconds on the server's steady clock */
+} ps26119_request_times;
+
+/* A server on the current device; NULL if opt has a negative field (opt NULL = defaults). */
+PS26119_API ps26119_server* ps26119_server_create(const ps26119_server_options* opt);
+
+/* Queues one LP (the arguments of ps26119_solve_lp_ex; the library copies them). Returns the
+ * request id (>= 0), or -PS26119_INVALID_ARGUMENT with the reason in error->message (error may
+ * be NULL) when the model or the options are invalid. */
+PS26119_API long long ps26119_server_submit(ps26119_server* server, int num_rows, int num_cols, int sense,
+                                            double obj_offset, const double* c, const double* col_lower,
+                                            const double* col_upper, const double* row_lower,
+                                            const double* row_upper, const int* col_start,
+                                            const int* row_index, const double* value,
+                                            const ps26119_options* opt, ps26119_result* error);
+
+/* Request `id`: 1 when it has finished (waiting for it if wait != 0) — result, x, y, z (each
+ * may be NULL) and times are written and the request is forgotten; 0 while it is pending; -1
+ * for an unknown id. */
+PS26119_API int ps26119_server_poll(ps26119_server* server, long long id, int wait, ps26119_result* result,
+                                    double* x, double* y, double* z, ps26119_request_times* times);
+
+/* Finishes every request already submitted, then releases the server. */
+PS26119_API void ps26119_server_destroy(ps26119_server* server);
+
 #ifdef __cplusplus
 }
 #endif

@@ -26,7 +26,7 @@ CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA, "bin", "nvcc")
 
 CU_SOURCES = ["engine.cu", "backend.cu", "batch.cu", "noalloc.cu"]
-CPP_SOURCES = ["solver.cpp", "certify.cpp", "io.cpp", "c_api.cpp"]
+CPP_SOURCES = ["solver.cpp", "certify.cpp", "io.cpp", "serve.cpp", "c_api.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC", "-Xcompiler",
               "-ffp-contract=off", "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr"] + ARCH

@@ -18,6 +18,7 @@
 #include "certify.hpp"
 #include "io.hpp"
 #include "solver.hpp"
+#include "serve.hpp"
 
 using namespace b200;
 
@@ -670,3 +671,76 @@ extern "C" int ps26119_check_certificate(int kind, int num_rows, int num_cols, i
     return PS26119_NUMERICAL_ERROR;
   }
 }
+
+// ============================================================ serving (serve.hpp)
+struct ps26119_server {
+  b200::Server server;
+  explicit ps26119_server(const b200::ServerOptions& o) : server(o) {}
+};
+
+extern "C" ps26119_server* ps26119_server_create(const ps26119_server_options* opt) {
+  b200::ServerOptions o;
+  if (opt) {
+    if (opt->slots < 0 || !(opt->hbm_budget_bytes >= 0) || !(opt->dry_run_seconds >= 0)) return nullptr;
+    o.slots = opt->slots;
+    o.hbm_budget_bytes = opt->hbm_budget_bytes;
+    o.dry_run_seconds = opt->dry_run_seconds;
+  }
+  try {
+    return new ps26119_server(o);
+  } catch (...) {
+    return nullptr;
+  }
+}
+
+extern "C" long long ps26119_server_submit(ps26119_server* server, int num_rows, int num_cols, int sense,
+                                           double obj_offset, const double* c, const double* col_lower,
+                                           const double* col_upper, const double* row_lower, const double* row_upper,
+                                           const int* col_start, const int* row_index, const double* value,
+                                           const ps26119_options* opt, ps26119_result* error) {
+  if (error) clear(error);
+  auto invalid = [&](const std::string& why) {
+    if (error) {
+      error->status = PS26119_INVALID_ARGUMENT;
+      set_text(error->message, sizeof error->message, why);
+    }
+    return -static_cast<long long>(PS26119_INVALID_ARGUMENT);
+  };
+  if (!server) return invalid("server is NULL");
+  try {
+    Model m;
+    if (const char* bad = model_from(num_rows, num_cols, sense, obj_offset, c, col_lower, col_upper, row_lower,
+                                     row_upper, col_start, row_index, value, m))
+      return invalid(std::string("invalid model: ") + bad);
+    Options o;
+    if (const char* bad = to_options(opt, num_rows, num_cols, o)) return invalid(bad);
+    return server->server.submit(std::move(m), std::move(o));
+  } catch (const std::bad_alloc&) {
+    return invalid("out of memory");
+  } catch (const std::exception& e) {
+    return invalid(e.what());
+  }
+}
+
+extern "C" int ps26119_server_poll(ps26119_server* server, long long id, int wait, ps26119_result* result, double* x,
+                                   double* y, double* z, ps26119_request_times* times) {
+  if (!server) return -1;
+  Solution s;
+  b200::RequestTimes t;
+  const int r = server->server.take(id, wait != 0, s, t);
+  if (r != 1) return r;
+  if (result) {
+    clear(result);
+    fill(s, result);
+  }
+  auto out = [](double* dst, const std::vector<double>& v) {
+    if (dst && !v.empty()) std::memcpy(dst, v.data(), sizeof(double) * v.size());
+  };
+  out(x, s.x);
+  out(y, s.y);
+  out(z, s.z);
+  if (times) *times = ps26119_request_times{t.submitted, t.started, t.finished};
+  return 1;
+}
+
+extern "C" void ps26119_server_destroy(ps26119_server* server) { delete server; }

@@ -7,6 +7,8 @@
 // (src/pdhg/cpu_backend.cpp) bit for bit. Only reductions may reorder sums (fast mode).
 #pragma once
 
+#include <atomic>
+
 #include <cuda_runtime.h>
 
 #include <chrono>
@@ -284,15 +286,15 @@ inline int grid_for(std::int64_t n, int block = kBlock) {
 
 // Streaming multiprocessors of the current device (cached per device).
 inline int sm_count() {
-  static int cached[64] = {};
+  static std::atomic<int> cached[64] = {};
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
-  if (cached[dev] == 0) {
-    int n = 0;
-    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
-    cached[dev] = n;
+  int v = cached[dev].load(std::memory_order_relaxed);
+  if (v == 0) {
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) v = 148;
+    cached[dev].store(v, std::memory_order_relaxed);
   }
-  return cached[dev];
+  return v;
 }
 
 // Grid-stride helper over [0, n).

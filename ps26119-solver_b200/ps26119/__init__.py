@@ -83,6 +83,14 @@ class _Scenario(ctypes.Structure):  # ps26119_scenario
     _fields_ = [("obj", _D), ("col_lower", _D), ("col_upper", _D), ("row_lower", _D), ("row_upper", _D)]
 
 
+class _ServerOptions(ctypes.Structure):  # ps26119_server_options
+    _fields_ = [("slots", ctypes.c_int), ("hbm_budget_bytes", ctypes.c_double), ("dry_run_seconds", ctypes.c_double)]
+
+
+class _RequestTimes(ctypes.Structure):  # ps26119_request_times
+    _fields_ = [("submitted", ctypes.c_double), ("started", ctypes.c_double), ("finished", ctypes.c_double)]
+
+
 class _ScalingOptions(ctypes.Structure):  # ps26119_scaling_options
     _fields_ = [("geometric_mean_iterations", ctypes.c_int), ("geometric_mean_min_log10_range", ctypes.c_double),
                 ("ruiz_iterations", ctypes.c_int), ("pock_chambolle", ctypes.c_int),
@@ -103,7 +111,8 @@ EXPORTS = ["ps26119_version", "ps26119_default_options", "ps26119_solve_lp", "ps
            "ps26119_backend_dual_step", "ps26119_backend_r2h_primal", "ps26119_backend_r2h_dual",
            "ps26119_backend_fused_primal", "ps26119_backend_fused_dual", "ps26119_backend_kkt",
            "ps26119_backend_sync", "ps26119_backend_scaled_get", "ps26119_backend_scaled_structure",
-           "ps26119_backend_scalars", "ps26119_backend_norm2_estimate", "ps26119_dot_noalloc"]
+           "ps26119_backend_scalars", "ps26119_backend_norm2_estimate", "ps26119_dot_noalloc",
+           "ps26119_server_create", "ps26119_server_submit", "ps26119_server_poll", "ps26119_server_destroy"]
 
 _lib = None
 
@@ -163,6 +172,13 @@ def load(path: str | None = None):
     L.ps26119_backend_norm2_estimate.argtypes = [B, _D]
     L.ps26119_dot_noalloc.argtypes = [ctypes.c_longlong, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                       ctypes.c_void_p, ctypes.c_void_p]
+    L.ps26119_server_create.restype = ctypes.c_void_p
+    L.ps26119_server_create.argtypes = [P(_ServerOptions)]
+    L.ps26119_server_submit.restype = ctypes.c_longlong
+    L.ps26119_server_submit.argtypes = [ctypes.c_void_p] + _MODEL + [P(_Options), P(_Result)]
+    L.ps26119_server_poll.argtypes = [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_int, P(_Result), _D, _D, _D,
+                                      P(_RequestTimes)]
+    L.ps26119_server_destroy.argtypes = [ctypes.c_void_p]
     if path is None:
         _lib = L
     return L
@@ -295,6 +311,72 @@ def solve_lp(c, A, row_lower, row_upper, col_lower=None, col_upper=None, sense=1
     ray_p = pr if st == UNBOUNDED and n > 0 and not np.isnan(pr).any() else None
     return _result(st, res, x if have or ray_p is not None else None, y if have else None, z if have else None,
                    ray_d, ray_p)
+
+
+class Server:
+    """The request loop (ps26119_server_*): independent LPs admitted by slots and HBM budget,
+    solved concurrently on the GPU, each exactly as :func:`solve_lp` would solve it.
+
+    >>> with Server(slots=8) as srv:
+    ...     rid = srv.submit(lp)          # an object with the generators.Lp fields
+    ...     res, times = srv.result(rid)  # waits; times = (submitted, started, finished) seconds
+    """
+
+    def __init__(self, slots=8, hbm_budget_bytes=0.0, dry_run_seconds=0.0):
+        self.L = load()
+        o = _ServerOptions(int(slots), float(hbm_budget_bytes), float(dry_run_seconds))
+        self.h = self.L.ps26119_server_create(ctypes.byref(o))
+        if not self.h:
+            raise ValueError("ps26119_server_create refused the options")
+        self.shapes = {}
+
+    def submit(self, lp, algorithm="r2hpdhg", precision="fp64", tolerance=1e-8, time_limit=3600.0,
+               iteration_limit=0) -> int:
+        args, keep = _model_args(lp)
+        opt = _options(algorithm, precision, True, tolerance, time_limit, iteration_limit, 0, 1)
+        err = _Result()
+        rid = self.L.ps26119_server_submit(self.h, *args, ctypes.byref(opt), ctypes.byref(err))
+        del keep
+        if rid < 0:
+            raise ValueError(err.message.decode(errors="replace"))
+        self.shapes[rid] = (lp.num_rows, lp.num_cols)
+        return rid
+
+    def poll(self, rid, wait=False):
+        """(Result, (submitted, started, finished)) once request ``rid`` has finished, else None."""
+        m, n = self.shapes[rid]
+        res, t = _Result(), _RequestTimes()
+        x, y, z = np.full(n, np.nan), np.full(m, np.nan), np.full(n, np.nan)
+        r = self.L.ps26119_server_poll(self.h, rid, int(bool(wait)), ctypes.byref(res), _ptr(x), _ptr(y), _ptr(z),
+                                       ctypes.byref(t))
+        if r == 0:
+            return None
+        if r < 0:
+            raise KeyError(rid)
+        del self.shapes[rid]
+        have = res.status in (OPTIMAL, ITERATION_LIMIT, TIME_LIMIT)
+        return (_result(res.status, res, x if have else None, y if have else None, z if have else None),
+                (t.submitted, t.started, t.finished))
+
+    def result(self, rid):
+        return self.poll(rid, wait=True)
+
+    def close(self):
+        if self.h:
+            self.L.ps26119_server_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def solve_lp_device(m, n, sense, offset, ptrs, precision="fp64", tolerance=1e-8, time_limit=3600.0,
