@@ -124,9 +124,9 @@ def run_serve(args, rank, world, local):
                         time.sleep(pause)
                     ids.append(srv.submit(lp, precision=args.precision))
                 out = [srv.result(i) for i in ids]
-            bad = [r.status_name for r, _ in out if r.status != ps26119.OPTIMAL or r.check != "PASS"]
+            bad = [f"{r.status_name} ({r.message})" for r, _ in out if r.status != ps26119.OPTIMAL or r.check != "PASS"]
             if bad:
-                raise RuntimeError(f"served solves ended {sorted(set(bad))}")
+                raise RuntimeError(f"{len(bad)} served solves failed, e.g. {bad[:3]}")
             sub = np.array([t[0] for _, t in out])
             fin = np.array([t[2] for _, t in out])
             steps.append((fin.max() - sub.min(), fin - sub, [r.iterations for r, _ in out]))

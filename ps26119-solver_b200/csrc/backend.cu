@@ -186,7 +186,7 @@ class GpuBackendImpl final : public GpuBackend {
     p.add(K0 + L, 0, L, 0.0, SumOrder::kSeq, R + kD);
     p.add(K0 + 2 * L, 0, L, 0.0, SumOrder::kSeq, R + kRd2);
     p.add(K0 + 3 * L, m_, L, 0.0, SumOrder::kSeq, R + kP);
-    p.build(exact_, nullptr);
+    p.build(exact_, nullptr, st_);
     p.launch(st_);
     double h[kNumSlots];
     B200_CHECK(cudaMemcpyAsync(h, res_.get(), sizeof h, cudaMemcpyDeviceToHost, st_));
@@ -251,7 +251,7 @@ class GpuBackendImpl final : public GpuBackend {
     B200_LAUNCH_CHECK();
     SumPlan p;
     p.add(terms_.get(), 0, len, 0.0, SumOrder::kChunk64, out_.get());
-    p.build(exact_, nullptr);
+    p.build(exact_, nullptr, st_);
     p.launch(st_);
     double r = 0;
     B200_CHECK(cudaMemcpyAsync(&r, out_.get(), sizeof r, cudaMemcpyDeviceToHost, st_));

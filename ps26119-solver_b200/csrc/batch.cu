@@ -658,7 +658,7 @@ void BatchEngine::finish_slot(int t, BatchOutcome& so, Status st, const BKkt& kk
   launches_ += 5;
   SumPlan p;
   p.add(obj_t_.get(), 0, n, B_.offset, SumOrder::kSeq, obj_out_.get());
-  p.build(o_.exact, nullptr);
+  p.build(o_.exact, nullptr, st_);
   p.launch(st_);
   launches_ += p.kernel_count();
   so.x.resize(n), so.y.resize(m), so.z.resize(n);

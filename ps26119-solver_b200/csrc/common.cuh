@@ -17,7 +17,9 @@
 #include <cstdlib>
 #include <mutex>
 #include <new>
+#include <map>
 #include <set>
+#include <shared_mutex>
 #include <vector>
 #include <stdexcept>
 #include <string>
@@ -45,14 +47,45 @@ struct CudaError : std::runtime_error {
 
 #define B200_LAUNCH_CHECK() B200_CHECK(cudaGetLastError())
 
+// Stream capture and device-wide synchronisation exclude each other. CUDA rejects a device
+// synchronisation (cudaDeviceSynchronize, and the implicit one in cudaFree / cudaFreeHost) while
+// any stream of the device is being captured, and the rejected call invalidates that capture. So
+// with solves running on several host threads (the request loop), every capture in this library
+// holds this lock shared (CaptureScope) and every device-wide synchronising call holds it
+// exclusively (with_device_sync). A thread inside its own capture makes no such call:
+// with_device_sync then does nothing and returns false.
+inline std::shared_mutex& capture_mutex() {
+  static std::shared_mutex* m = new std::shared_mutex();  // never destroyed
+  return *m;
+}
+inline thread_local bool t_capturing = false;
+class CaptureScope {
+ public:
+  CaptureScope() : lk_(capture_mutex()) { t_capturing = true; }
+  ~CaptureScope() { t_capturing = false; }
+  CaptureScope(const CaptureScope&) = delete;
+  CaptureScope& operator=(const CaptureScope&) = delete;
+
+ private:
+  std::shared_lock<std::shared_mutex> lk_;
+};
+template <class F>
+inline bool with_device_sync(F&& f) {
+  if (t_capturing) return false;
+  std::unique_lock<std::shared_mutex> lk(capture_mutex());
+  f();
+  return true;
+}
+
 // A process-wide cache of device blocks. Solves allocate the same large buffers again and
 // again; cudaMalloc / cudaFree of gigabytes cost a device-wide synchronisation and, measured on
 // B200, from a few ms up to over a second per solve. Released blocks are kept (per device, by
 // size class: powers of two up to 1 MiB, multiples of 2 MiB above) and handed out again; at
-// most PS26119_DEVICE_CACHE_MB (default 8192) MiB stay cached, the rest is freed. Every
-// release in this library follows a synchronisation of the stream that used the block; as a
-// safety net the first reuse after a release synchronises the device once. On an allocation
-// failure the device's cached blocks are freed and the allocation is retried.
+// most PS26119_DEVICE_CACHE_MB (default 8192) MiB stay cached, the rest is freed. A block
+// released while kernels of its releasing thread may still use it (scoped temporaries of a
+// setup step) is handed out again only after a device synchronisation that began after the
+// release: solves on other threads and streams never see it in use. On an allocation failure
+// the device's cached blocks are freed and the allocation is retried.
 class DeviceBlockCache {
  public:
   static DeviceBlockCache& instance() {
@@ -68,23 +101,34 @@ class DeviceBlockCache {
     const std::size_t g = 2u << 20;
     return (bytes + g - 1) / g * g;
   }
+  // A released block may still be read or written by kernels its releasing thread enqueued
+  // (on any stream). Every release gets a generation number; a block is handed out again only
+  // once a device synchronisation that started after its release has completed (`synced_`).
   void* acquire(std::size_t bytes) {  // bytes: a size class
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) dev = 0;
     {
-      std::lock_guard<std::mutex> lock(mu_);
+      std::unique_lock<std::mutex> lock(mu_);
+      const std::uint64_t idle = synced_[dev];
+      long long ready = -1, pending = -1;
       for (std::size_t k = 0; k < free_.size(); ++k)
         if (free_[k].device == dev && free_[k].bytes == bytes) {
-          void* p = free_[k].p;
-          free_[k] = free_.back();
-          free_.pop_back();
-          cached_ -= bytes;
-          if (dirty_.count(dev)) {
-            dirty_.erase(dev);
-            (void)cudaDeviceSynchronize();
+          if (free_[k].gen <= idle) {
+            ready = static_cast<long long>(k);
+            break;
           }
-          return p;
+          if (pending < 0) pending = static_cast<long long>(k);
         }
+      if (ready >= 0) return take(static_cast<std::size_t>(ready));
+      if (pending >= 0 && !t_capturing) {  // reuse after one device synchronisation
+        void* p = take(static_cast<std::size_t>(pending));
+        const std::uint64_t upto = gen_;
+        lock.unlock();
+        with_device_sync([] { (void)cudaDeviceSynchronize(); });
+        lock.lock();
+        synced_[dev] = std::max(synced_[dev], upto);
+        return p;
+      }
     }
     void* p = nullptr;
     cudaError_t e = cudaMalloc(&p, bytes);
@@ -103,22 +147,21 @@ class DeviceBlockCache {
   void release(void* p, std::size_t bytes, int dev) {
     {
       std::lock_guard<std::mutex> lock(mu_);
-      if (cached_ + bytes <= limit_) {
-        free_.push_back({dev, bytes, p});
+      if (cached_ + bytes <= limit_ || t_capturing) {  // inside a capture: keep it, freeing would sync
+        free_.push_back({dev, bytes, p, ++gen_});
         cached_ += bytes;
-        dirty_.insert(dev);
         return;
       }
     }
-    cudaFree(p);  // never throws from a destructor
+    with_device_sync([p] { cudaFree(p); });  // never throws from a destructor
   }
   void trim(int dev) {  // frees this device's cached blocks
-    std::vector<void*> drop;
+    std::vector<Block> drop;
     {
       std::lock_guard<std::mutex> lock(mu_);
       for (std::size_t k = 0; k < free_.size();)
         if (free_[k].device == dev) {
-          drop.push_back(free_[k].p);
+          drop.push_back(free_[k]);
           cached_ -= free_[k].bytes;
           free_[k] = free_.back();
           free_.pop_back();
@@ -126,8 +169,15 @@ class DeviceBlockCache {
           ++k;
         }
     }
-    if (!drop.empty()) (void)cudaDeviceSynchronize();
-    for (void* p : drop) cudaFree(p);
+    if (drop.empty()) return;
+    const bool done = with_device_sync([&drop] {
+      (void)cudaDeviceSynchronize();
+      for (const Block& b : drop) cudaFree(b.p);
+    });
+    if (!done) {  // inside a capture of this thread: keep the blocks cached
+      std::lock_guard<std::mutex> lock(mu_);
+      for (const Block& b : drop) free_.push_back(b), cached_ += b.bytes;
+    }
   }
 
  private:
@@ -140,10 +190,19 @@ class DeviceBlockCache {
     int device;
     std::size_t bytes;
     void* p;
+    std::uint64_t gen;  // release generation
   };
+  void* take(std::size_t k) {  // with mu_ held
+    void* p = free_[k].p;
+    cached_ -= free_[k].bytes;
+    free_[k] = free_.back();
+    free_.pop_back();
+    return p;
+  }
   std::mutex mu_;
   std::vector<Block> free_;
-  std::set<int> dirty_;
+  std::map<int, std::uint64_t> synced_;  // per device: blocks released at or before this generation are idle
+  std::uint64_t gen_ = 0;
   std::size_t cached_ = 0, limit_ = 0;
 };
 
@@ -234,13 +293,13 @@ class PinnedBlockCache {
   void release(void* p, std::size_t bytes) {
     {
       std::lock_guard<std::mutex> lock(mu_);
-      if (cached_ + bytes <= (256u << 20)) {
+      if (cached_ + bytes <= (256u << 20) || t_capturing) {
         free_.push_back({bytes, p});
         cached_ += bytes;
         return;
       }
     }
-    cudaFreeHost(p);
+    with_device_sync([p] { cudaFreeHost(p); });
   }
 
  private:

@@ -282,13 +282,13 @@ void Engine::build_plans() {
   plan_obj_.add(O, 0, n, M_.offset, SumOrder::kSeq, R + kObjective);
   plan_chk_.add(O + n, 0, L, 0.0, SumOrder::kSeq, R + kChkDual);
   plan_chk_.add(O, 0, n, 0.0, SumOrder::kSeq, R + kChkPrimal);
-  plan_r0_.build(o_.exact, skip_r0_flag(params_.get()));
-  plan_res_.build(o_.exact, nullptr);
-  plan_kkt_.build(o_.exact, nullptr);
-  plan_ray1_.build(o_.exact, nullptr);
-  plan_ray2_.build(o_.exact, nullptr);
-  plan_obj_.build(o_.exact, nullptr);
-  plan_chk_.build(o_.exact, nullptr);
+  plan_r0_.build(o_.exact, skip_r0_flag(params_.get()), st_);
+  plan_res_.build(o_.exact, nullptr, st_);
+  plan_kkt_.build(o_.exact, nullptr, st_);
+  plan_ray1_.build(o_.exact, nullptr, st_);
+  plan_ray2_.build(o_.exact, nullptr, st_);
+  plan_obj_.build(o_.exact, nullptr, st_);
+  plan_chk_.build(o_.exact, nullptr, st_);
 }
 
 // The residual: dx = x̄ − x̂, adx = Ã dx, dy = ȳ − ŷ and the terms of the five dots.
@@ -371,6 +371,7 @@ void Engine::capture_epoch() {
   slab_prepare<T, EpiResY<T>, B200_STAGE_TMA != 0>();
   capturing_ = true;
   capture_count_ = 0;
+  auto capture_scope = std::make_unique<CaptureScope>();  // no device-wide syncs elsewhere meanwhile
   B200_CHECK(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
   auto step = [&](int s) {
     EpiPrimal<T> ep{v.x.get(), v.xh.get(), v.xb.get(), v.x0.get(), sp_.c<T>(), sp_.l<T>(), sp_.u<T>(), P, s, 0, 0, 0};
@@ -387,6 +388,7 @@ void Engine::capture_epoch() {
   for (int s = 1; s < K; ++s) step(s);
   B200_CHECK(cudaEventRecordWithFlags(ev_[3], st_, cudaEventRecordExternal));
   const cudaError_t e = cudaStreamEndCapture(st_, &g);
+  capture_scope.reset();
   capturing_ = false;
   B200_CHECK(e);
   B200_CHECK(cudaGraphInstantiate(&g_epoch_[idx], g, 0));
@@ -406,6 +408,7 @@ void Engine::capture_check(int variant) {
   slab_prepare<double, EpiRayRows, B200_STAGE_TMA != 0>();
   capturing_ = true;
   capture_count_ = 0;
+  auto capture_scope = std::make_unique<CaptureScope>();  // no device-wide syncs elsewhere meanwhile
   B200_CHECK(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
   clear_maxima();
   launch_residual<T>(true, nullptr, plan_res_);
@@ -420,6 +423,7 @@ void Engine::capture_check(int variant) {
   }
   B200_CHECK(cudaMemcpyAsync(hres_.get(), res_.get(), kNumSlots * sizeof(double), cudaMemcpyDeviceToHost, st_));
   const cudaError_t e = cudaStreamEndCapture(st_, &g);
+  capture_scope.reset();
   capturing_ = false;
   B200_CHECK(e);
   B200_CHECK(cudaGraphInstantiate(&g_check_[idx][variant], g, 0));
@@ -489,7 +493,7 @@ double Engine::initial_primal_weight() {  // engine.cpp:207-218
   SumPlan p;
   p.add(tm.get(), 0, m, 0.0, SumOrder::kSeq, s.get());
   p.add(tn.get(), 0, n, 0.0, SumOrder::kSeq, s.get() + 1);
-  p.build(o_.exact, nullptr);
+  p.build(o_.exact, nullptr, st_);
   p.launch(st_);
   double h[2];
   B200_CHECK(cudaMemcpyAsync(h, s.get(), sizeof h, cudaMemcpyDeviceToHost, st_));
@@ -869,6 +873,7 @@ void Engine::capture_pdlp_epoch(int phase) {
   slab_prepare<T, EpiPdlpDual<T>, B200_STAGE_TMA != 0>();
   capturing_ = true;
   capture_count_ = 0;
+  auto capture_scope = std::make_unique<CaptureScope>();  // no device-wide syncs elsewhere meanwhile
   B200_CHECK(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
   B200_CHECK(cudaEventRecordWithFlags(ev_[0], st_, cudaEventRecordExternal));
   for (int s = 0; s < K; ++s) {
@@ -887,6 +892,7 @@ void Engine::capture_pdlp_epoch(int phase) {
   B200_CHECK(cudaEventRecordWithFlags(ev_[2], st_, cudaEventRecordExternal));
   B200_CHECK(cudaEventRecordWithFlags(ev_[3], st_, cudaEventRecordExternal));
   const cudaError_t e = cudaStreamEndCapture(st_, &g);
+  capture_scope.reset();
   capturing_ = false;
   B200_CHECK(e);
   B200_CHECK(cudaGraphInstantiate(&g_pdlp_[idx][phase], g, 0));
@@ -910,6 +916,7 @@ void Engine::capture_pdlp_check(int phase, int variant) {
   slab_prepare<double, EpiRayRows, B200_STAGE_TMA != 0>();
   capturing_ = true;
   capture_count_ = 0;
+  auto capture_scope = std::make_unique<CaptureScope>();  // no device-wide syncs elsewhere meanwhile
   B200_CHECK(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
   clear_maxima();
   launch_kkt_scaled<T>(xc, yc);  // KKT of the current point -> res2_
@@ -933,6 +940,7 @@ void Engine::capture_pdlp_check(int phase, int variant) {
   B200_CHECK(cudaMemcpyAsync(hres_.get(), res_.get(), kNumSlots * sizeof(double), cudaMemcpyDeviceToHost, st_));
   B200_CHECK(cudaMemcpyAsync(hres2_.get(), res2_.get(), kNumSlots * sizeof(double), cudaMemcpyDeviceToHost, st_));
   const cudaError_t e = cudaStreamEndCapture(st_, &g);
+  capture_scope.reset();
   capturing_ = false;
   B200_CHECK(e);
   B200_CHECK(cudaGraphInstantiate(&g_pdlp_chk_[idx][phase][variant], g, 0));
@@ -997,7 +1005,7 @@ EngineResult Engine::run_pdlp(const DeviceOutputs& out) {
   hres2_.alloc(kNumSlots);
   plan_dist_.add(rt_.get(), 0, nn, 0.0, SumOrder::kChunk64, res_.get() + kPx);
   plan_dist_.add(rt_.get() + 2 * nn, 0, mm, 0.0, SumOrder::kChunk64, res_.get() + kPy);
-  plan_dist_.build(o_.exact, nullptr);
+  plan_dist_.build(o_.exact, nullptr, st_);
   mixed_now_ = o_.mixed;
   double omega = initial_primal_weight();
   if (mixed_now_) init_iterates<float>();
@@ -1149,7 +1157,9 @@ EngineResult run_engine(const DeviceModel& M, const EngineOptions& opt, const De
   if (!st) {
     // The caller's inputs may still be in flight on the legacy default stream: finish them,
     // then run on a stream of our own (capturable, unlike the legacy stream).
-    B200_CHECK(cudaDeviceSynchronize());
+    cudaError_t se = cudaSuccess;
+    with_device_sync([&se] { se = cudaDeviceSynchronize(); });
+    B200_CHECK(se);
     B200_CHECK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     own = true;
   }

@@ -241,8 +241,8 @@ struct ScaledDevice {
     SumPlan pal, pbn;
     pal.add(terms.get(), 0, n, 0.0, SumOrder::kSeq, out.get());
     pbn.add(terms.get(), 0, n, 0.0, SumOrder::kSeq, out.get() + 1);
-    pal.build(exact, nullptr);
-    pbn.build(exact, nullptr);
+    pal.build(exact, nullptr, st);
+    pbn.build(exact, nullptr, st);
     std::vector<double> alpha, beta;
     double theta = 0, theta_old = -1;
     int stagnant = 0;
@@ -343,7 +343,7 @@ struct ScaledDevice {
     SumPlan p;
     p.add(tmp_m.get(), 0, m, 0.0, SumOrder::kSeq, sums.get());
     p.add(tmp_n.get(), 0, n, 0.0, SumOrder::kSeq, sums.get() + 1);
-    p.build(exact, nullptr);
+    p.build(exact, nullptr, st);
     p.launch(st);
     double h[2];
     B200_CHECK(cudaMemcpyAsync(h, sums.get(), sizeof h, cudaMemcpyDeviceToHost, st));

@@ -107,7 +107,9 @@ class SumPlan {
     jobs_.push_back({terms, lo, hi, init, order, out});
   }
   // skip: optional device int; when non-zero at run time every kernel of the plan returns.
-  void build(bool exact, const int* skip) {
+  // st: the stream the plan is launched on; the segment descriptors are copied to the device on
+  // it, so they are in place before the plan's first launch on that stream.
+  void build(bool exact, const int* skip, cudaStream_t st) {
     exact_ = exact;
     skip_ = skip;
     std::vector<ChainSeg> phase1, phase2;
@@ -132,13 +134,13 @@ class SumPlan {
           ++slot;
         }
       }
-      upload(phase1, seg1_);
-      upload(phase2, seg2_);
+      upload(phase1, seg1_, st);
+      upload(phase2, seg2_, st);
       n1_ = static_cast<int>(phase1.size());
       n2_ = static_cast<int>(phase2.size());
     } else {
       for (const Job& j : jobs_) tree.push_back({j.t, j.lo, j.hi, j.init, j.out});
-      upload(tree, tseg_);
+      upload(tree, tseg_, st);
       nt_ = static_cast<int>(tree.size());
       partials_.alloc(static_cast<std::size_t>(nt_ > 0 ? nt_ : 1) * kTreeBlocks);
     }
@@ -174,10 +176,14 @@ class SumPlan {
     SumOrder order;
     double* out;
   };
+  // Stream-ordered copy from pageable memory: cudaMemcpyAsync stages the source before it
+  // returns, and the device copy lands before any later work on `st`. (A plain cudaMemcpy on the
+  // legacy stream may return before the copy lands and is not ordered with a non-blocking `st`.)
   template <class S>
-  static void upload(const std::vector<S>& v, DevBuf<unsigned char>& dst) {
+  static void upload(const std::vector<S>& v, DevBuf<unsigned char>& dst, cudaStream_t st) {
     dst.alloc(v.size() * sizeof(S) + 1);
-    if (!v.empty()) B200_CHECK(cudaMemcpy(dst.get(), v.data(), v.size() * sizeof(S), cudaMemcpyHostToDevice));
+    if (!v.empty())
+      B200_CHECK(cudaMemcpyAsync(dst.get(), v.data(), v.size() * sizeof(S), cudaMemcpyHostToDevice, st));
   }
   std::vector<Job> jobs_;
   bool exact_ = false;
