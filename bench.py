@@ -92,7 +92,7 @@ def run_serve(args, rank, world, local):
     torch.cuda.set_device(local)
     w = WORKLOADS[args.workload]
     reqs = make_requests(args.workload)
-    N, slots = len(reqs), w["slots"]
+    N, slots = len(reqs), args.serve_slots or w["slots"]
 
     def alone(lp, precision="fp64"):
         return ps26119.solve_lp(lp.c, (lp.col_start, lp.row_index, lp.value), lp.row_lower, lp.row_upper,
@@ -101,8 +101,12 @@ def run_serve(args, rank, world, local):
 
     alone(min(reqs, key=lambda lp: lp.num_rows))  # warm-up: first-call costs stay out
     S = min(N, args.serve_sample)
+    # a size-stratified sample: every (N/S)-th request in order of size, so that the sequential
+    # mean stands for the whole stream
+    by_size = sorted(range(N), key=lambda k: reqs[k].num_rows)
+    sample = [reqs[by_size[(2 * j + 1) * N // (2 * S)]] for j in range(S)]
     seq = []
-    for lp in reqs[:S]:
+    for lp in sample:
         t0 = time.perf_counter()
         r = alone(lp)
         seq.append(time.perf_counter() - t0)
@@ -129,9 +133,11 @@ def run_serve(args, rank, world, local):
                 raise RuntimeError(f"{len(bad)} served solves failed, e.g. {bad[:3]}")
             sub = np.array([t[0] for _, t in out])
             fin = np.array([t[2] for _, t in out])
-            steps.append((fin.max() - sub.min(), fin - sub, [r.iterations for r, _ in out]))
+            start = np.array([t[1] for _, t in out])
+            steps.append((fin.max() - sub.min(), fin - sub, [r.iterations for r, _ in out], fin - start))
     sec = max_over_ranks(float(np.mean([s[0] for s in steps])), world)
     lat = np.concatenate([s[1] for s in steps])
+    svc = np.concatenate([s[3] for s in steps])
     value = world * N / sec
     h2d = sum(lp.nnz * 12 + (lp.num_cols + 1) * 4 + lp.num_cols * 24 + lp.num_rows * 16 for lp in reqs)
     d2h = sum(lp.num_cols * 16 + lp.num_rows * 8 for lp in reqs)
@@ -144,11 +150,15 @@ def run_serve(args, rank, world, local):
         "config": {"workload": w["desc"], "requests": N, "slots": slots, "precision": args.precision,
                    "tolerance": 1e-8, "arrival_rate_per_s": rate, "rows": [int(lp.num_rows) for lp in reqs],
                    "entry": "ps26119_server_submit / ps26119_server_poll (host arrays)",
+                   "cuda_device_max_connections": os.environ.get("CUDA_DEVICE_MAX_CONNECTIONS"),
                    "parallelism": f"replicas x{world}", "l2": "many small LPs: L2-resident, latency-bound"},
         "latency_ms": {"p50": float(np.percentile(lat, 50) * 1e3), "p99": float(np.percentile(lat, 99) * 1e3),
-                       "mean": float(lat.mean() * 1e3)},
+                       "mean": float(lat.mean() * 1e3), "note": "submission to completion (queueing included)"},
+        "service_ms": {"p50": float(np.percentile(svc, 50) * 1e3), "p99": float(np.percentile(svc, 99) * 1e3),
+                       "note": "admission to completion"},
         "sequential_fp64": {"solves_per_s": 1.0 / t_seq, "speedup": value * t_seq / world,
-                            "sample": f"{S} of the requests solved one at a time, plain fp64, ps26119_solve_lp_ex"},
+                            "sample": f"{S} of the requests (stratified by size) solved one at a time, plain "
+                                      "fp64, ps26119_solve_lp_ex"},
         "iterations": steps[-1][2],
         "gpu_launches": None,
         "clocks": clocks.summary(),
@@ -631,7 +641,12 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--serve-sample", type=int, default=8, help="requests solved sequentially for the baseline")
+    ap.add_argument("--serve-slots", type=int, default=0, help="server slots (0: the workload's)")
     args = ap.parse_args()
+    if WORKLOADS[args.workload]["kind"] == "serve":
+        # one hardware work queue per slot (the default, 8, makes streams beyond 8 share queues);
+        # read when the CUDA context is created, so it is set before anything touches CUDA
+        os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
     rank, world, local = dist_setup()
     if args.impl == "reference":
         line = run_reference(args, rank, world)
