@@ -134,38 +134,86 @@ std::vector<double> Model::row_activity(const std::vector<double>& x) const {  /
   return ax;
 }
 
-std::uint64_t Model::fingerprint() const {  // model.cpp:20-85: FNV-1a over the canonical numbers
-  std::uint64_t h = 0xcbf29ce484222325ULL;
-  auto bytes = [&](const void* p, std::size_t n) {
-    const auto* b = static_cast<const unsigned char*>(p);
-    for (std::size_t i = 0; i < n; ++i) h ^= b[i], h *= 0x100000001b3ULL;
-  };
-  auto u64 = [&](std::uint64_t v) { bytes(&v, sizeof v); };
-  auto i64 = [&](std::int64_t v) { bytes(&v, sizeof v); };
-  auto f64 = [&](double v) {
+namespace {
+// FNV-1a over a byte stream, continued from state h.
+std::uint64_t fnv1a(std::uint64_t h, const std::vector<unsigned char>& bytes) {
+  for (unsigned char c : bytes) h ^= c, h *= 0x100000001b3ULL;
+  return h;
+}
+constexpr std::uint64_t kFnvOffset = 0xcbf29ce484222325ULL;
+
+// The canonical byte stream a fingerprint hashes (model.cpp:20-85): integers and doubles as
+// 8-byte little-endian words, −0 as +0, every NaN as the one quiet NaN.
+struct CanonicalBytes {
+  std::vector<unsigned char> buf;
+  void word(std::uint64_t v) {
+    const auto* b = reinterpret_cast<const unsigned char*>(&v);
+    buf.insert(buf.end(), b, b + sizeof v);
+  }
+  void i64(std::int64_t v) { word(static_cast<std::uint64_t>(v)); }
+  void f64(double v) {
     if (v == 0.0) v = 0.0;
     std::uint64_t bits;
     if (std::isnan(v)) bits = 0x7ff8000000000000ULL;
     else std::memcpy(&bits, &v, sizeof bits);
-    u64(bits);
-  };
-  auto f64s = [&](const std::vector<double>& v) {
-    u64(v.size());
-    for (double d : v) f64(d);
-  };
-  i64(num_rows), i64(num_cols), i64(sense), f64(obj_offset);
-  f64s(obj), f64s(col_lower), f64s(col_upper), f64s(row_lower), f64s(row_upper);
-  u64(value.size());
-  std::vector<std::pair<int, double>> col;
-  for (int j = 0; j < num_cols; ++j) {
-    col.clear();
-    for (int k = col_start[j]; k < col_start[j + 1]; ++k) col.emplace_back(row_index[k], value[k]);
-    std::sort(col.begin(), col.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
-    i64(static_cast<std::int64_t>(col.size()));
-    for (const auto& [i, v] : col) i64(i), f64(v);
+    word(bits);
   }
-  for (int j = 0; j < num_cols; ++j) i64(j < static_cast<int>(is_integer.size()) && is_integer[j] ? 1 : 0);
-  return h;
+  void f64s(const std::vector<double>& v) {
+    word(v.size());
+    for (double d : v) f64(d);
+  }
+};
+
+// Dimensions, sense, offset and the five vectors.
+void canonical_head(const Model& M, const std::vector<double>& obj, const std::vector<double>& cl,
+                    const std::vector<double>& cu, const std::vector<double>& rl, const std::vector<double>& ru,
+                    CanonicalBytes& out) {
+  out.i64(M.num_rows), out.i64(M.num_cols), out.i64(M.sense), out.f64(M.obj_offset);
+  out.f64s(obj), out.f64s(cl), out.f64s(cu), out.f64s(rl), out.f64s(ru);
+}
+// The matrix (each column's entries in row order) and the integrality flags.
+void canonical_tail(const Model& M, CanonicalBytes& out) {
+  out.word(M.value.size());
+  out.buf.reserve(out.buf.size() + 16 * M.value.size() + 16 * static_cast<std::size_t>(M.num_cols) + 16);
+  std::vector<std::pair<int, double>> col;
+  for (int j = 0; j < M.num_cols; ++j) {
+    col.clear();
+    for (int k = M.col_start[j]; k < M.col_start[j + 1]; ++k) col.emplace_back(M.row_index[k], M.value[k]);
+    std::sort(col.begin(), col.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+    out.i64(static_cast<std::int64_t>(col.size()));
+    for (const auto& [i, v] : col) out.i64(i), out.f64(v);
+  }
+  for (int j = 0; j < M.num_cols; ++j) out.i64(j < static_cast<int>(M.is_integer.size()) && M.is_integer[j] ? 1 : 0);
+}
+}  // namespace
+
+std::uint64_t Model::fingerprint() const {  // model.cpp:20-85: FNV-1a over the canonical numbers
+  CanonicalBytes head, tail;
+  canonical_head(*this, obj, col_lower, col_upper, row_lower, row_upper, head);
+  canonical_tail(*this, tail);
+  return fnv1a(fnv1a(kFnvOffset, head.buf), tail.buf);
+}
+
+// Fingerprints of the base model with each scenario's vectors (an empty vector keeps the
+// base's): the matrix part of the byte stream is built once, the scenarios are hashed on the
+// host's threads.
+std::vector<std::uint64_t> scenario_fingerprints(const Model& base, const std::vector<Scenario>& scenarios) {
+  CanonicalBytes tail;
+  canonical_tail(base, tail);
+  std::vector<std::uint64_t> out(scenarios.size());
+  parallel_ranges(static_cast<long long>(scenarios.size()), [&](long long kb, long long ke) {
+    for (long long k = kb; k < ke; ++k) {
+      const Scenario& s = scenarios[static_cast<std::size_t>(k)];
+      auto pick = [](const std::vector<double>& v, const std::vector<double>& d) -> const std::vector<double>& {
+        return v.empty() ? d : v;
+      };
+      CanonicalBytes head;
+      canonical_head(base, pick(s.obj, base.obj), pick(s.col_lower, base.col_lower), pick(s.col_upper, base.col_upper),
+                     pick(s.row_lower, base.row_lower), pick(s.row_upper, base.row_upper), head);
+      out[static_cast<std::size_t>(k)] = fnv1a(fnv1a(kFnvOffset, head.buf), tail.buf);
+    }
+  }, 2);
+  return out;
 }
 
 HostModelView Model::view() const {
@@ -968,28 +1016,16 @@ Solution solve(const Model& model, const Options& options) {  // solve.cpp:194-2
 }
 
 // ============================================================ batch (batch.cpp:129-441)
-namespace {
-std::string fingerprint_hex(const Model& m) {
-  char buf[17];
-  std::snprintf(buf, sizeof buf, "%016llx", static_cast<unsigned long long>(m.fingerprint()));
-  return buf;
-}
-}  // namespace
-
 std::vector<Solution> solve_batch(const Model& base, const std::vector<Scenario>& scenarios, const Options& options) {
   const auto t0 = clock_t_::now();
   const int K = static_cast<int>(scenarios.size());
   std::vector<Solution> out(K);
   {  // fingerprints of the scenario models (batch.cpp:113-127): the base with the scenario's vectors
-    Model w = base;
+    const std::vector<std::uint64_t> fp = scenario_fingerprints(base, scenarios);
     for (int k = 0; k < K; ++k) {
-      const Scenario& s = scenarios[k];
-      w.obj = s.obj.empty() ? base.obj : s.obj;
-      w.col_lower = s.col_lower.empty() ? base.col_lower : s.col_lower;
-      w.col_upper = s.col_upper.empty() ? base.col_upper : s.col_upper;
-      w.row_lower = s.row_lower.empty() ? base.row_lower : s.row_lower;
-      w.row_upper = s.row_upper.empty() ? base.row_upper : s.row_upper;
-      out[k].model_fingerprint = fingerprint_hex(w);
+      char buf[17];
+      std::snprintf(buf, sizeof buf, "%016llx", static_cast<unsigned long long>(fp[k]));
+      out[k].model_fingerprint = buf;
       out[k].engine = "r2hpdhg-batch";
       out[k].precision = "fp64";
     }

@@ -125,4 +125,7 @@ struct Scenario {
 // reference's batch is CPU-only; this is its replacement).
 std::vector<Solution> solve_batch(const Model& base, const std::vector<Scenario>& scenarios, const Options& options);
 
+// Model::fingerprint of the base model with each scenario's vectors (empty = the base's).
+std::vector<std::uint64_t> scenario_fingerprints(const Model& base, const std::vector<Scenario>& scenarios);
+
 }  // namespace b200
