@@ -26,6 +26,8 @@
 #include <string>
 
 #include "batch.hpp"
+
+#include <type_traits>
 #include "checks.cuh"
 #include "problem.cuh"
 
@@ -51,6 +53,28 @@ constexpr double kVerifyPrimal = 1e-6, kVerifyDual = 1e-6, kVerifyGap = 1e-6;
 // lane (slot t = g + s·G). Each (row, slot) sum is the reference's acc[k] += a·x[k] over the
 // row's nonzeros in order. Epi::kMax per-slot maxima are folded per warp and then into
 // atomic keys (order-independent and exact).
+// Latency: an epilogue with `Pre load(q, t)` has its operands loaded before the row walk, and
+// the walk loads kBatchNz (col, val) pairs, then their gathers, then adds them in order, so a
+// row costs two dependent round trips per kBatchNz nonzeros instead of two per nonzero.
+#ifndef B200_BATCH_NZ
+#define B200_BATCH_NZ 2
+#endif
+constexpr int kBatchNz = B200_BATCH_NZ;
+struct BNoPre {};
+template <class E>
+__device__ __forceinline__ auto bload(const E& e, long long q, int t, int) -> decltype(e.load(q, t)) {
+  return e.load(q, t);
+}
+template <class E>
+__device__ __forceinline__ BNoPre bload(const E&, long long, int, long) {
+  return BNoPre{};
+}
+template <class E, class P>
+__device__ __forceinline__ void bapply(const E& e, long long r, int t, long long q, double acc, double* mx, const P& p) {
+  if constexpr (std::is_same<P, BNoPre>::value) e(r, t, q, acc, mx);
+  else e(r, t, q, acc, mx, p);
+}
+
 template <int S, class Epi>
 __global__ void __launch_bounds__(256) k_bspmm(int rows, int W, int lg, const int* __restrict__ rp,
                                                const int* __restrict__ col, const double* __restrict__ val,
@@ -65,23 +89,43 @@ __global__ void __launch_bounds__(256) k_bspmm(int rows, int W, int lg, const in
 #pragma unroll
     for (int k = 0; k < NM; ++k) mx[s][k] = 0.0;
   for (long long r = gid; r < rows; r += ng) {
+    using Pre = decltype(bload(epi, 0LL, 0, 0));
+    Pre pre[S];
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+      const int t = g + s * G;
+      if (t < W) pre[s] = bload(epi, r * W + t, t, 0);
+    }
     double acc[S];
 #pragma unroll
     for (int s = 0; s < S; ++s) acc[s] = 0.0;
     const int b = rp[r], e = rp[r + 1];
-    for (int p = b; p < e; ++p) {
-      const double a = val[p];
-      const double* xr = X + static_cast<long long>(col[p]) * W;
+    for (int p = b; p < e; p += kBatchNz) {
+      int cc[kBatchNz];
+      double aa[kBatchNz];
 #pragma unroll
-      for (int s = 0; s < S; ++s) {
-        const int t = g + s * G;
-        if (t < W) acc[s] += a * xr[t];
+      for (int u = 0; u < kBatchNz; ++u) {
+        cc[u] = p + u < e ? col[p + u] : 0;
+        aa[u] = p + u < e ? val[p + u] : 0.0;
       }
+      double xv[kBatchNz][S];
+#pragma unroll
+      for (int u = 0; u < kBatchNz; ++u)
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+          const int t = g + s * G;
+          xv[u][s] = (p + u < e && t < W) ? X[static_cast<long long>(cc[u]) * W + t] : 0.0;
+        }
+#pragma unroll
+      for (int u = 0; u < kBatchNz; ++u)
+        if (p + u < e)
+#pragma unroll
+          for (int s = 0; s < S; ++s) acc[s] += aa[u] * xv[u][s];  // in CSR order
     }
 #pragma unroll
     for (int s = 0; s < S; ++s) {
       const int t = g + s * G;
-      if (t < W) epi(r, t, r * W + t, acc[s], mx[s]);
+      if (t < W) bapply(epi, r, t, r * W + t, acc[s], mx[s], pre[s]);
     }
   }
   if constexpr (Epi::kMax > 0) {
@@ -107,16 +151,25 @@ struct EpiBPrimal {
   const double *C, *L, *U, *X0, *tau;
   double *X, *XH, *XB;
   const long long* inner0;
-  int step;
+  int step, last;  // last: the epoch's last step
   double a2, b2;
-  __device__ void operator()(long long, int t, long long q, double aty, double*) const {
+  struct Pre {
+    double x, c, l, u, x0;
+  };
+  __device__ Pre load(long long q, int) const { return Pre{X[q], C[q], L[q], U[q], X0[q]}; }
+  __device__ void operator()(long long r, int t, long long q, double aty, double* mx) const {
+    (*this)(r, t, q, aty, mx, load(q, t));
+  }
+  __device__ void operator()(long long, int t, long long q, double aty, double*, const Pre& p) const {
     const long long in = inner0[t] + step;
     const double w = static_cast<double>(in + 1) / static_cast<double>(in + 2);
-    const double x = X[q];
-    const double h = ref_clamp(x - tau[t] * (C[q] - aty), L[q], U[q]);
-    XH[q] = h;
+    const double x = p.x;
+    const double h = ref_clamp(x - tau[t] * (p.c - aty), p.l, p.u);
+    // x̂ is read only by the residual, check and restart that follow the epoch's last step and
+    // the first step of a slot's Halpern cycle; on the other steps it is not stored
+    if (step == last || in == 0) XH[q] = h;
     XB[q] = 2 * h - x;
-    X[q] = w * (a2 * h + b2 * x) + (1 - w) * X0[q];
+    X[q] = w * (a2 * h + b2 * x) + (1 - w) * p.x0;
   }
 };
 // Dual step of every slot (batch.cpp:345-358), acc = (Ãx̄)_i.
@@ -125,18 +178,27 @@ struct EpiBDual {
   const double *RL, *RU, *Y0, *sigma;
   double *Y, *YH, *YB;
   const long long* inner0;
-  int step;
+  int step, last;
   double a2, b2;
-  __device__ void operator()(long long, int t, long long q, double ax, double*) const {
+  struct Pre {
+    double y, rl, ru, y0;
+  };
+  __device__ Pre load(long long q, int) const { return Pre{Y[q], RL[q], RU[q], Y0[q]}; }
+  __device__ void operator()(long long r, int t, long long q, double ax, double* mx) const {
+    (*this)(r, t, q, ax, mx, load(q, t));
+  }
+  __device__ void operator()(long long, int t, long long q, double ax, double*, const Pre& p) const {
     const long long in = inner0[t] + step;
     const double w = static_cast<double>(in + 1) / static_cast<double>(in + 2);
     const double sg = sigma[t];
-    const double y = Y[q];
+    const double y = p.y;
     const double v = ax - y / sg;
-    const double h = y - sg * ax + sg * ref_clamp(v, RL[q], RU[q]);
-    YH[q] = h;
-    YB[q] = 2 * h - y;
-    Y[q] = w * (a2 * h + b2 * y) + (1 - w) * Y0[q];
+    const double h = y - sg * ax + sg * ref_clamp(v, p.rl, p.ru);
+    if (step == last || in == 0) {  // ŷ, ȳ: read only after those steps (as x̂ above)
+      YH[q] = h;
+      YB[q] = 2 * h - y;
+    }
+    Y[q] = w * (a2 * h + b2 * y) + (1 - w) * p.y0;
   }
 };
 // Residual rows after adx = Ã·Δx (compute_residuals, batch.cpp:305-318): terms Δy², Δy·(AΔx)
@@ -392,7 +454,14 @@ class BatchEngine {
  public:
   BatchEngine(const HostModelView& base, const std::vector<BatchScenarioView>& sc, const std::vector<int>& sid,
               const EngineOptions& o, cudaStream_t st, std::chrono::steady_clock::time_point t0)
-      : B_(base), S_(sc), sid_(sid), o_(o), st_(st), t0_(t0) {}
+      : B_(base), S_(sc), sid_(sid), o_(o), st_(st), t0_(t0) {
+    for (auto& e : ev_) B200_CHECK(cudaEventCreate(&e));
+  }
+  ~BatchEngine() {
+    for (auto& e : ev_) cudaEventDestroy(e);
+  }
+  BatchEngine(const BatchEngine&) = delete;
+  BatchEngine& operator=(const BatchEngine&) = delete;
 
   void run(std::vector<BatchOutcome>& out);
 
@@ -414,6 +483,9 @@ class BatchEngine {
   std::vector<int> sid_;
   const EngineOptions& o_;
   cudaStream_t st_;
+  cudaEvent_t ev_[4] = {};  // SpMM time of an epoch: [0,1] step 0, [2,3] steps 1..K-1
+  double spmm_ms_ = 0.0;
+  long long spmm_launches_ = 0;
   std::chrono::steady_clock::time_point t0_;
   int m_ = 0, n_ = 0, W_ = 0;
   double eta_ = 1.0, setup_s_ = 0.0;
@@ -585,10 +657,10 @@ void BatchEngine::setup() {
 
 void BatchEngine::step(int s) {
   EpiBPrimal ep{nv_[C].get(), nv_[L].get(), nv_[U].get(), nv_[X0].get(), tau_.get(), nv_[X].get(), nv_[XH].get(),
-                nv_[XB].get(), inner0_.get(), s, 2 * o_.reflection, 1 - 2 * o_.reflection};
+                nv_[XB].get(), inner0_.get(), s, o_.check_every - 1, 2 * o_.reflection, 1 - 2 * o_.reflection};
   spmm(n_, cs_.get(), sp_.t_ri.get(), sp_.sat.get(), mv_[Y].get(), ep, false);
   EpiBDual ed{mv_[RL].get(), mv_[RU].get(), mv_[Y0].get(), sigma_.get(), mv_[Y].get(), mv_[YH].get(), mv_[YB].get(),
-              inner0_.get(), s, 2 * o_.reflection, 1 - 2 * o_.reflection};
+              inner0_.get(), s, o_.check_every - 1, 2 * o_.reflection, 1 - 2 * o_.reflection};
   spmm(m_, sp_.a_rp.get(), sp_.a_col.get(), sp_.sa.get(), nv_[XB].get(), ed, false);
 }
 
@@ -709,8 +781,13 @@ void BatchEngine::run(std::vector<BatchOutcome>& out) {
     B200_CHECK(cudaMemcpyAsync(tau_.get(), h_par_.get(), W_ * sizeof(double), cudaMemcpyHostToDevice, st_));
     B200_CHECK(cudaMemcpyAsync(sigma_.get(), h_par_.get() + W_, W_ * sizeof(double), cudaMemcpyHostToDevice, st_));
     B200_CHECK(cudaMemcpyAsync(inner0_.get(), h_inner_.get(), W_ * sizeof(long long), cudaMemcpyHostToDevice, st_));
+    B200_CHECK(cudaEventRecord(ev_[0], st_));
     for (int s = 0; s < Kc; ++s) {
       step(s);
+      if (s == 0) {
+        B200_CHECK(cudaEventRecord(ev_[1], st_));
+        B200_CHECK(cudaEventRecord(ev_[2], st_));  // moved past the r⁰ section below when there is one
+      }
       if (s == 0 && any_new) {  // r⁰ right after the epoch's first step (batch.cpp:359-366)
         launch_residual(false);
         ISegs g{};
@@ -719,8 +796,10 @@ void BatchEngine::run(std::vector<BatchOutcome>& out) {
         g.s[2] = {mv_[TCR].get(), m_, nullptr, 0, 0.0, kBCr0};
         g.n = 3;
         launch_sums(g);
+        B200_CHECK(cudaEventRecord(ev_[2], st_));
       }
     }
+    B200_CHECK(cudaEventRecord(ev_[3], st_));
     for (int t = 0; t < W_; ++t) inner[sid_[t]] += Kc;
     it += Kc;
     // ---- check: residual + restart distances, KKT of every slot, one download
@@ -743,6 +822,13 @@ void BatchEngine::run(std::vector<BatchOutcome>& out) {
     B200_CHECK(cudaMemcpyAsync(h_res_.get(), res_.get(), static_cast<std::size_t>(W_) * kRes * sizeof(double),
                                cudaMemcpyDeviceToHost, st_));
     B200_CHECK(cudaStreamSynchronize(st_));
+    {
+      float a = 0, b = 0;
+      B200_CHECK(cudaEventElapsedTime(&a, ev_[0], ev_[1]));
+      B200_CHECK(cudaEventElapsedTime(&b, ev_[2], ev_[3]));
+      spmm_ms_ += a + b;
+      spmm_launches_ += 2LL * Kc;
+    }
     // r⁰ of the slots that started this epoch, with the ω they ran with
     if (any_new)
       for (int t = 0; t < W_; ++t)
@@ -831,7 +917,11 @@ void BatchEngine::run(std::vector<BatchOutcome>& out) {
     if (o_.verbosity >= 2)
       std::fprintf(stderr, "batch it %lld  t %.2fs  running %d\n", it, elapsed(), W_);
   }
-  for (auto& so : out) so.kernel_launches = launches_;
+  for (auto& so : out) {
+    so.kernel_launches = launches_;
+    so.spmm_kernel_ms = spmm_ms_;
+    so.spmm_launches = spmm_launches_;
+  }
 }
 
 }  // namespace

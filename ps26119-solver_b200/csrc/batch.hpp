@@ -24,6 +24,8 @@ struct BatchOutcome {
   double objective = 0, dual_objective = 0, primal_residual = 0, dual_residual = 0, gap = 0;
   long long iterations = 0, iterations_to_fast = -1, kernel_launches = 0;
   double seconds = 0, setup_seconds = 0, seconds_to_fast = -1, primal_weight = 1;
+  double spmm_kernel_ms = 0;     // the batch's SpMM kernels (CUDA events), whole batch
+  long long spmm_launches = 0;
 };
 
 // Runs the scenarios listed in `slots` (indices into `scenarios`, all valid) on the device;

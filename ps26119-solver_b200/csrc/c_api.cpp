@@ -593,7 +593,11 @@ extern "C" int ps26119_solve_batch(int num_rows, int num_cols, int sense, double
     g_stats = ps26119_stats{};
     g_stats.kernel_launches = launches;
     g_stats.m = num_rows, g_stats.n = num_cols, g_stats.nnz = nnz;
-    if (num_scenarios > 0) g_stats.setup_seconds = sols[0].setup_seconds;
+    if (num_scenarios > 0) {
+      g_stats.setup_seconds = sols[0].setup_seconds;
+      g_stats.spmv_kernel_ms = sols[0].engine_result.iter_kernel_ms;
+      g_stats.spmv_kernel_launches = sols[0].engine_result.iter_kernel_launches;
+    }
     return 0;
   } catch (const std::bad_alloc&) {
     return fail(PS26119_NOT_SOLVED, "out of memory");

@@ -1087,6 +1087,8 @@ std::vector<Solution> solve_batch(const Model& base, const std::vector<Scenario>
       s.iterations_to_fast = r.iterations_to_fast;
       s.primal_weight = r.primal_weight;
       s.engine_result.kernel_launches = r.kernel_launches;
+      s.engine_result.iter_kernel_ms = r.spmm_kernel_ms;
+      s.engine_result.iter_kernel_launches = r.spmm_launches;
     }
   } catch (const std::bad_alloc&) {
     return fail_all("out of memory");
