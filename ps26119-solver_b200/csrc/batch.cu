@@ -157,9 +157,6 @@ struct EpiBPrimal {
     double x, c, l, u, x0;
   };
   __device__ Pre load(long long q, int) const { return Pre{X[q], C[q], L[q], U[q], X0[q]}; }
-  __device__ void operator()(long long r, int t, long long q, double aty, double* mx) const {
-    (*this)(r, t, q, aty, mx, load(q, t));
-  }
   __device__ void operator()(long long, int t, long long q, double aty, double*, const Pre& p) const {
     const long long in = inner0[t] + step;
     const double w = static_cast<double>(in + 1) / static_cast<double>(in + 2);
@@ -184,9 +181,6 @@ struct EpiBDual {
     double y, rl, ru, y0;
   };
   __device__ Pre load(long long q, int) const { return Pre{Y[q], RL[q], RU[q], Y0[q]}; }
-  __device__ void operator()(long long r, int t, long long q, double ax, double* mx) const {
-    (*this)(r, t, q, ax, mx, load(q, t));
-  }
   __device__ void operator()(long long, int t, long long q, double ax, double*, const Pre& p) const {
     const long long in = inner0[t] + step;
     const double w = static_cast<double>(in + 1) / static_cast<double>(in + 2);
