@@ -17,6 +17,10 @@
 //   ref_bound        certified_dual_bound with the implied-bounds switch and its term counts.
 //   ref_certificate  check_infeasibility_certificate / check_unboundedness_certificate
 //                    (src/core/certificates.cpp:14, 88).
+//   ref_presolve_file  the reference reader then ps26119::presolve (src/core/presolve.cpp:22-156)
+//                    on a model file: a digest of every presolve decision, in the serialisation
+//                    the library's `ps26119 info` prints (outcome, counts, maps, fixed values,
+//                    singletons, reduced fingerprint; 8-byte words, FNV-1a).
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -311,6 +315,61 @@ int ref_read_fingerprint(const char* path, char* fp, int cap, long long* dims) {
   std::snprintf(fp, static_cast<std::size_t>(cap), "%s", ok ? m.fingerprint_hex().c_str() : err.c_str());
   if (ok) dims[0] = m.num_rows, dims[1] = m.num_cols, dims[2] = static_cast<long long>(m.nnz());
   return ok ? 1 : 0;
+}
+
+// Digest of a PresolveResult; word order: outcome (0 reduced, 1 infeasible, 2 unchanged),
+// removed rows, removed cols, tightened bounds, |row_map| and entries, |col_map| and entries,
+// |fixed_value| and values (−0 as +0, NaN canonical), |singletons| and (row, col, a, set_lower,
+// set_upper) each, reduced fingerprint (0 unless reduced).
+int ref_presolve_file(const char* path, char* out, int cap, long long* counts) {
+  Model m;
+  const std::string p(path);
+  std::string err;
+  bool ok = false;
+  if (p.size() > 4 && p.compare(p.size() - 4, 4, ".lpm") == 0) {
+    const auto r = io::read_lpm(p, m);
+    ok = r.ok;
+    err = r.error;
+  } else {
+    ok = io::read_mps(p, m, err);
+  }
+  if (!ok) {
+    std::snprintf(out, static_cast<std::size_t>(cap), "%s", err.c_str());
+    return 0;
+  }
+  const PresolveResult r = presolve(m);
+  std::uint64_t h = 0xcbf29ce484222325ULL;
+  auto word = [&](std::uint64_t v) {
+    for (int k = 0; k < 8; ++k) h ^= (v >> (8 * k)) & 0xffu, h *= 0x100000001b3ULL;
+  };
+  auto f64 = [&](double v) {
+    if (v == 0.0) v = 0.0;
+    std::uint64_t bits;
+    if (std::isnan(v)) bits = 0x7ff8000000000000ULL;
+    else std::memcpy(&bits, &v, sizeof bits);
+    word(bits);
+  };
+  const int oc = r.outcome == PresolveResult::Outcome::Reduced ? 0 : r.outcome == PresolveResult::Outcome::Infeasible ? 1 : 2;
+  word(static_cast<std::uint64_t>(oc));
+  word(static_cast<std::uint64_t>(r.removed_rows)), word(static_cast<std::uint64_t>(r.removed_cols));
+  word(static_cast<std::uint64_t>(r.tightened_bounds));
+  word(r.row_map.size());
+  for (int i : r.row_map) word(static_cast<std::uint64_t>(static_cast<std::int64_t>(i)));
+  word(r.col_map.size());
+  for (int j : r.col_map) word(static_cast<std::uint64_t>(static_cast<std::int64_t>(j)));
+  word(r.fixed_value.size());
+  for (double v : r.fixed_value) f64(v);
+  word(r.singletons.size());
+  for (const auto& t : r.singletons) {
+    word(static_cast<std::uint64_t>(static_cast<std::int64_t>(t.row)));
+    word(static_cast<std::uint64_t>(static_cast<std::int64_t>(t.col)));
+    f64(t.a);
+    word(t.set_lower ? 1u : 0u), word(t.set_upper ? 1u : 0u);
+  }
+  word(oc == 0 ? r.reduced.fingerprint() : 0);
+  std::snprintf(out, static_cast<std::size_t>(cap), "%016llx", static_cast<unsigned long long>(h));
+  counts[0] = oc, counts[1] = r.removed_rows, counts[2] = r.removed_cols, counts[3] = r.tightened_bounds;
+  return 1;
 }
 
 // out[4] = finite, bound, unbounded_row_terms, unbounded_col_terms

@@ -90,6 +90,8 @@ def lib():
         L.ref_bound.argtypes = model + [_D, ctypes.c_int, _D]
         L.ref_read_fingerprint.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int,
                                            ctypes.POINTER(ctypes.c_longlong)]
+        L.ref_presolve_file.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int,
+                                        ctypes.POINTER(ctypes.c_longlong)]
         L.ref_certificate.argtypes = [ctypes.c_int] + model + [_D, _D, _D]
         L.ps26119_solve_lp.argtypes = None  # the reference's own C API, used by bench.py
         _lib = L
@@ -211,6 +213,17 @@ def read_fingerprint(path):
     dims = (ctypes.c_longlong * 3)()
     ok = L.ref_read_fingerprint(os.fsencode(path), buf, 512, dims)
     return (buf.value.decode(), tuple(dims)) if ok else (None, buf.value.decode())
+
+
+def presolve_file(path):
+    """The reference reader and ps26119::presolve on a model file: (digest hex, (outcome,
+    removed rows, removed cols, tightened bounds)) with outcome 0 reduced, 1 infeasible,
+    2 unchanged; or (None, error text)."""
+    L = lib()
+    buf = ctypes.create_string_buffer(512)
+    counts = (ctypes.c_longlong * 4)()
+    ok = L.ref_presolve_file(os.fsencode(path), buf, 512, counts)
+    return (buf.value.decode(), tuple(counts)) if ok else (None, buf.value.decode())
 
 
 def bound(lp, y, use_implied=True):

@@ -122,7 +122,23 @@ int cmd_info(int argc, char** argv) {
               free_cols, ints);
   std::printf("  nonzeros           %zu\n", m.nnz());
   std::printf("  fingerprint        %s\n", fingerprint_hex(m).c_str());
-  if (auto c = m.crossed_bounds(); !c.empty()) std::printf("  note               %s (infeasible)\n", c.c_str());
+  if (auto c = m.crossed_bounds(); !c.empty()) {
+    std::printf("  note               %s (infeasible)\n", c.c_str());
+    return 0;
+  }
+  // what the safe presolve (R1-R4) would do, and a digest of all its decisions
+  if (m.validate().empty()) {
+    const PresolveResult r = presolve(m);
+    const char* what = r.outcome == PresolveResult::Outcome::Reduced      ? "reduced"
+                       : r.outcome == PresolveResult::Outcome::Infeasible ? "infeasible"
+                                                                           : "unchanged";
+    std::printf("  presolve           %s: removed %d rows, %d columns, %d bounds tightened\n", what, r.removed_rows,
+                r.removed_cols, r.tightened_bounds);
+    if (r.outcome == PresolveResult::Outcome::Reduced)
+      std::printf("  reduced            %d rows, %d columns, %zu nonzeros\n", r.reduced.num_rows, r.reduced.num_cols,
+                  r.reduced.nnz());
+    std::printf("  presolve digest    %016llx\n", static_cast<unsigned long long>(presolve_digest(r)));
+  }
   return 0;
 }
 

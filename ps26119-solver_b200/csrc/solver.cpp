@@ -507,6 +507,21 @@ Solution postsolve(const Model& M, const PresolveResult& r, const Solution& red)
   return s;
 }
 
+std::uint64_t presolve_digest(const PresolveResult& r) {
+  CanonicalBytes b;
+  b.i64(r.outcome == PresolveResult::Outcome::Reduced ? 0 : r.outcome == PresolveResult::Outcome::Infeasible ? 1 : 2);
+  b.i64(r.removed_rows), b.i64(r.removed_cols), b.i64(r.tightened_bounds);
+  b.word(r.row_map.size());
+  for (int i : r.row_map) b.i64(i);
+  b.word(r.col_map.size());
+  for (int j : r.col_map) b.i64(j);
+  b.f64s(r.fixed_value);
+  b.word(r.singletons.size());
+  for (const auto& t : r.singletons) b.i64(t.row), b.i64(t.col), b.f64(t.a), b.i64(t.set_lower), b.i64(t.set_upper);
+  b.word(r.outcome == PresolveResult::Outcome::Reduced ? r.reduced.fingerprint() : 0);
+  return fnv1a(kFnvOffset, b.buf);
+}
+
 // Maps a Farkas vector of the reduced model to the original rows (presolve.cpp:195-207): kept
 // rows keep their multiplier; a column bound made by a removed singleton row moves onto that
 // row, newest singleton first, when λ_j = −(Aᵀr)_j points at it.

@@ -106,6 +106,11 @@ struct PresolveResult {
 PresolveResult presolve(const Model& model);
 Solution postsolve(const Model& original, const PresolveResult& r, const Solution& reduced);
 
+// One 64-bit FNV-1a digest of everything presolve decided: outcome, counts, row and column maps,
+// fixed values, singleton records (in order) and the reduced model's fingerprint. Two presolves
+// agree when their digests do (the CLI's `info` prints it).
+std::uint64_t presolve_digest(const PresolveResult& r);
+
 // The library entry point: never throws (solve.cpp:194-210).
 Solution solve(const Model& model, const Options& options);
 

@@ -1,0 +1,110 @@
+"""Presolve R1-R4 (csrc/solver.cpp presolve) against the reference's own presolve
+(src/core/presolve.cpp:22-156, run from oracle/_ref), on the CPU. Both sides read the same model
+file and digest every decision presolve makes: outcome, counts, row and column maps, fixed
+values, the singleton records in order, and the reduced model's fingerprint. `ps26119 info`
+prints the library's digest, reference.presolve_file the reference's. Equal digests mean the
+reduced model the engine solves and the postsolve data are the reference's, bit for bit."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from ps26119 import generators as g
+from conftest import REFERENCE_DATA
+from test_io import cli, write_mps
+
+
+def our_presolve(path):
+    r = cli("info", path)
+    assert r.returncode == 0, r.stdout + r.stderr
+    lines = [ln for ln in r.stdout.splitlines() if "presolve digest" in ln]
+    return lines[0].split()[-1] if lines else None, r.stdout
+
+
+def planted(seed):
+    """A small LP with every reduction planted: empty rows (feasible), empty columns (finite
+    and infinite best bounds, zero cost), fixed columns, and singleton rows that tighten lower
+    and upper bounds, some of them chained through columns that the reductions empty."""
+    rng = np.random.default_rng(seed)
+    m, n = 40, 30
+    A = np.where(rng.random((m, n)) < 0.15, rng.normal(size=(m, n)), 0.0)
+    A[[3, 17, 29], :] = 0.0                       # empty rows
+    A[:, [2, 11, 25]] = 0.0                       # empty columns
+    for i, j in ((5, 7), (8, 12), (21, 4), (33, 19), (36, 7)):   # singleton rows
+        A[i, :] = 0.0
+        A[i, j] = rng.choice([-1.0, 1.0]) * rng.uniform(0.5, 2.0)
+    x0 = rng.uniform(0.5, 4.0, n)
+    ax = A @ x0
+    rl, ru = ax - rng.uniform(0, 1, m), ax + rng.uniform(0, 1, m)
+    rl[[7, 15]] = -np.inf
+    ru[[9, 22]] = np.inf
+    rl[[3, 17]], ru[[3, 17]] = -1.0, 2.0          # 0 inside: removable
+    rl[29], ru[29] = 0.0, 0.0
+    cl, cu = np.zeros(n), np.full(n, 6.0)
+    cu[[1, 9]] = np.inf
+    cl[[6, 14, 27]] = cu[[6, 14, 27]] = x0[[6, 14, 27]]   # fixed columns
+    c = rng.normal(size=n)
+    c[2], c[11], c[25] = 1.0, -1.0, 0.0           # empty columns: lower, upper, zero cost
+    cu[11] = np.inf                                # best bound infinite: kept
+    return g.from_dense(c, A, rl, ru, cl, cu, offset=1.5)
+
+
+def infeasible_empty_row():
+    lp = planted(7)
+    rl, ru = lp.row_lower.copy(), lp.row_upper.copy()
+    rl[3], ru[3] = 1.0, 2.0  # an empty row that excludes 0
+    return lp.with_data(row_lower=rl, row_upper=ru)
+
+
+GENERATED = {
+    **{f"planted_{s}": (lambda s=s: planted(s)) for s in range(6)},
+    "infeasible_empty_row": infeasible_empty_row,
+    "random_m300": lambda: g.random_lp(300, seed=4),
+    "staircase_T3": lambda: g.staircase_lp(3, seed=2),
+}
+
+
+@pytest.mark.parametrize("name", sorted(GENERATED))
+def test_presolve_decisions_match_reference(ref, tmp_path, name):
+    lp = GENERATED[name]()
+    path = tmp_path / f"{name}.mps"
+    write_mps(lp, path)
+    want, counts = ref.presolve_file(str(path))
+    got, out = our_presolve(str(path))
+    assert want is not None, counts
+    assert got == want, (counts, out)
+
+
+def test_planted_models_exercise_every_rule(ref, tmp_path):
+    seen = set()
+    for s in range(6):
+        path = tmp_path / f"p{s}.mps"
+        write_mps(planted(s), path)
+        _, (outcome, rows, cols, tightened) = ref.presolve_file(str(path))
+        seen.add(outcome)
+        assert rows >= 3 + 5 and cols >= 2 + 3 and tightened >= 1  # one empty column is kept (infinite bound)
+    path = tmp_path / "inf.mps"
+    write_mps(infeasible_empty_row(), path)
+    seen.add(ref.presolve_file(str(path))[1][0])
+    assert seen == {0, 1}
+
+
+def _reference_files():
+    if not os.path.isdir(REFERENCE_DATA):
+        return []
+    out = []
+    for d in ("netlib_small", "examples", "hand"):
+        out += sorted(glob.glob(os.path.join(REFERENCE_DATA, d, "*.mps")) +
+                      glob.glob(os.path.join(REFERENCE_DATA, d, "*.lpm")))
+    return out
+
+
+@pytest.mark.parametrize("path", _reference_files(), ids=lambda p: os.path.relpath(p, REFERENCE_DATA))
+def test_presolve_on_reference_data_files(ref, path):
+    want, info = ref.presolve_file(path)
+    got, out = our_presolve(path)
+    if want is None:
+        assert got is None
+    else:
+        assert got == want, (info, out)
