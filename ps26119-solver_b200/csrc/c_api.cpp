@@ -136,7 +136,23 @@ int solve_host(int num_rows, int num_cols, int sense, double obj_offset, const d
   try {
     phase_log_begin(opt && opt->verbosity >= 1);
     auto t_model = std::chrono::steady_clock::now();
-    Model m;
+    // the calling thread's host copy of the model: its memory is reused by the next call on
+    // this thread (within the host reuse limit, host_keep), which then copies into pages that
+    // are already mapped instead of page-faulting fresh ones
+    struct ModelHolder {
+      Model m;
+      std::size_t accounted = 0;
+      ~ModelHolder() { host_keep(accounted, 0); }
+    };
+    static thread_local ModelHolder t_model_copy;
+    struct KeepModel {
+      ModelHolder& h;
+      ~KeepModel() {
+        if (!host_keep(h.accounted, capacity_bytes(h.m))) h.m = Model{};
+      }
+    } keep_model{t_model_copy};
+    Model& m = t_model_copy.m;
+    m.is_integer.clear();
     m.num_rows = num_rows;
     m.num_cols = num_cols;
     m.sense = sense;

@@ -13,6 +13,7 @@
 //                  with zero elimination
 #include "certify.hpp"
 #include "parallel.hpp"
+#include "solver.hpp"
 
 #include <algorithm>
 #include <cmath>
@@ -153,6 +154,23 @@ struct SafeSum {
 
 // The bound for multipliers y (already cleared where they point at an infinite row bound) and
 // column bounds [col_lo, col_up] (safe_bound.cpp:92-173).
+// The per-column term arrays and the cleared multipliers of this thread, kept between calls
+// within the host reuse limit (host_keep in solver.hpp).
+struct CertifyScratch {
+  std::vector<DD> col_term;
+  std::vector<char> col_inf;
+  std::vector<double> y;
+  std::size_t accounted = 0;
+  std::size_t bytes() const { return sizeof(DD) * col_term.capacity() + col_inf.capacity() + 8 * y.capacity(); }
+  void release() {
+    std::vector<DD>().swap(col_term);
+    std::vector<char>().swap(col_inf);
+    std::vector<double>().swap(y);
+  }
+  ~CertifyScratch() { host_keep(accounted, 0); }
+};
+thread_local CertifyScratch t_certify;
+
 SafeBound bound_with(const Model& M, const std::vector<double>& y, const std::vector<double>& col_lo,
                      const std::vector<double>& col_up) {
   SafeBound r;
@@ -160,8 +178,10 @@ SafeBound bound_with(const Model& M, const std::vector<double>& y, const std::ve
   const double sense = M.sense;
   if (static_cast<int>(y.size()) != m) return r;
   // per-column terms min over the enclosure [z_lo, z_hi] of z_j x_j, independent per column
-  std::vector<DD> col_term(static_cast<std::size_t>(n));
-  std::vector<char> col_inf(static_cast<std::size_t>(n), 0);
+  std::vector<DD>& col_term = t_certify.col_term;
+  std::vector<char>& col_inf = t_certify.col_inf;
+  col_term.assign(static_cast<std::size_t>(n), DD{});
+  col_inf.assign(static_cast<std::size_t>(n), 0);
   parallel_ranges(n, [&](long long jb, long long je) {
     std::vector<double> ex, scratch;
     ex.reserve(16);
@@ -245,7 +265,13 @@ SafeBound bound_with(const Model& M, const std::vector<double>& y, const std::ve
 SafeBound certified_dual_bound(const Model& M, const std::vector<double>& y_in, bool use_implied_bounds) {
   if (static_cast<int>(y_in.size()) != M.num_rows) return SafeBound{};
   // valid for ANY multipliers: clear those that point at an infinite row bound (safe_bound.cpp:178-187)
-  std::vector<double> y = y_in;
+  struct KeepScratch {
+    ~KeepScratch() {
+      if (!host_keep(t_certify.accounted, t_certify.bytes())) t_certify.release();
+    }
+  } keep;
+  std::vector<double>& y = t_certify.y;
+  y.assign(y_in.begin(), y_in.end());
   for (int i = 0; i < M.num_rows; ++i) {
     const double ym = M.sense * y[i];
     if ((ym > 0 && !std::isfinite(M.row_lower[i])) || (ym < 0 && !std::isfinite(M.row_upper[i]))) y[i] = 0.0;

@@ -10,6 +10,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <new>
@@ -316,8 +317,72 @@ bool within(double v, double lo, double up) {
 }
 }  // namespace
 
-PresolveResult presolve(const Model& M) {  // presolve.cpp:22-156 (LP: no integer columns here)
+namespace {
+// Presolve's per-thread scratch (kept between calls, within the host reuse limit).
+struct PresolveScratch {
+  std::vector<int> row_xor, row_cnt, col_cnt, new_row;
+  std::vector<double> rl, ru, cl, cu;
+  std::vector<char> row_alive, col_alive;
+  std::size_t accounted = 0;
+  std::size_t bytes() const {
+    return 4 * (row_xor.capacity() + row_cnt.capacity() + col_cnt.capacity() + new_row.capacity()) +
+           8 * (rl.capacity() + ru.capacity() + cl.capacity() + cu.capacity()) + row_alive.capacity() +
+           col_alive.capacity();
+  }
+  void release() {  // frees the memory (clear() alone keeps the capacity)
+    std::vector<int>().swap(row_xor), std::vector<int>().swap(row_cnt), std::vector<int>().swap(col_cnt);
+    std::vector<int>().swap(new_row);
+    std::vector<double>().swap(rl), std::vector<double>().swap(ru), std::vector<double>().swap(cl);
+    std::vector<double>().swap(cu);
+    std::vector<char>().swap(row_alive), std::vector<char>().swap(col_alive);
+  }
+  ~PresolveScratch() { host_keep(accounted, 0); }
+};
+thread_local PresolveScratch t_presolve;
+
+void clear_model(Model& R) {  // empties every vector, keeping its capacity
+  R.num_rows = R.num_cols = 0, R.sense = 1, R.obj_offset = 0.0;
+  R.obj.clear(), R.col_lower.clear(), R.col_upper.clear(), R.row_lower.clear(), R.row_upper.clear();
+  R.col_start.clear(), R.row_index.clear(), R.value.clear(), R.is_integer.clear();
+}
+}  // namespace
+
+std::size_t capacity_bytes(const Model& m) {
+  return 8 * (m.obj.capacity() + m.col_lower.capacity() + m.col_upper.capacity() + m.row_lower.capacity() +
+              m.row_upper.capacity() + m.value.capacity()) +
+         4 * (m.col_start.capacity() + m.row_index.capacity()) + m.is_integer.capacity();
+}
+
+bool host_keep(std::size_t& accounted, std::size_t bytes) {
+  static const std::size_t limit = [] {
+    const char* env = std::getenv("PS26119_HOST_REUSE_MB");
+    const long long mb = env ? std::atoll(env) : 2048;
+    return mb > 0 ? static_cast<std::size_t>(mb) << 20 : std::size_t{0};
+  }();
+  static std::mutex mu;
+  static std::size_t total = 0;
+  std::lock_guard<std::mutex> lock(mu);
+  total -= accounted;
+  accounted = 0;
+  if (bytes == 0 || total + bytes > limit) return false;
+  total += bytes;
+  accounted = bytes;
+  return true;
+}
+
+PresolveResult presolve(const Model& M) {
   PresolveResult r;
+  presolve_into(M, r);
+  return r;
+}
+
+void presolve_into(const Model& M, PresolveResult& r) {  // presolve.cpp:22-156 (LP: no integer columns here)
+  r.outcome = PresolveResult::Outcome::Unchanged;
+  r.message.clear();
+  r.removed_rows = r.removed_cols = r.tightened_bounds = 0;
+  r.row_map.clear(), r.col_map.clear(), r.singletons.clear();
+  clear_model(r.reduced);
+  PresolveScratch& S = t_presolve;
   const int m = M.num_rows, n = M.num_cols;
   // A singleton row's one remaining column is recovered as the XOR of the row's live column
   // indices (kept up to date as columns are removed), and its coefficient by a scan of that
@@ -325,7 +390,10 @@ PresolveResult presolve(const Model& M) {  // presolve.cpp:22-156 (LP: no intege
   // no row-wise copy of A.
   // One pass over the entries, threads over column ranges: XOR and count are commutative, so
   // relaxed integer atomics give the arrays of a sequential pass.
-  std::vector<int> row_xor(static_cast<std::size_t>(m), 0), row_cnt(static_cast<std::size_t>(m), 0);
+  std::vector<int>& row_xor = S.row_xor;
+  std::vector<int>& row_cnt = S.row_cnt;
+  row_xor.assign(static_cast<std::size_t>(m), 0);
+  row_cnt.assign(static_cast<std::size_t>(m), 0);
   parallel_ranges(n, [&](long long jb, long long je) {
     for (long long jj = jb; jj < je; ++jj) {
       const int j = static_cast<int>(jj);
@@ -336,24 +404,34 @@ PresolveResult presolve(const Model& M) {  // presolve.cpp:22-156 (LP: no intege
       }
     }
   });
-  std::vector<double> rl = M.row_lower, ru = M.row_upper, cl = M.col_lower, cu = M.col_upper;
-  std::vector<char> row_alive(m, 1), col_alive(n, 1);
-  std::vector<int> col_cnt(n);
+  std::vector<double>&rl = S.rl, &ru = S.ru, &cl = S.cl, &cu = S.cu;
+  rl.assign(M.row_lower.begin(), M.row_lower.end()), ru.assign(M.row_upper.begin(), M.row_upper.end());
+  cl.assign(M.col_lower.begin(), M.col_lower.end()), cu.assign(M.col_upper.begin(), M.col_upper.end());
+  std::vector<char>&row_alive = S.row_alive, &col_alive = S.col_alive;
+  row_alive.assign(static_cast<std::size_t>(m), 1), col_alive.assign(static_cast<std::size_t>(n), 1);
+  std::vector<int>& col_cnt = S.col_cnt;
+  col_cnt.resize(static_cast<std::size_t>(n));
   for (int j = 0; j < n; ++j) col_cnt[j] = M.col_start[j + 1] - M.col_start[j];
   r.fixed_value.assign(n, kNaN);
   double offset = M.obj_offset;
   auto infeasible = [&](const std::string& why) {
     r.outcome = PresolveResult::Outcome::Infeasible;
     r.message = why;
-    return r;
   };
+  // keeps the scratch for the next call on this thread, or frees it beyond the reuse limit
+  struct KeepScratch {
+    PresolveScratch& s;
+    ~KeepScratch() {
+      if (!host_keep(s.accounted, s.bytes())) s.release();
+    }
+  } keep{S};
   bool changed = true;
   while (changed) {
     changed = false;
     for (int i = 0; i < m; ++i) {  // rows: empty (R1) and singleton (R4)
       if (!row_alive[i]) continue;
       if (row_cnt[i] == 0) {
-        if (!within(0.0, rl[i], ru[i])) return infeasible("empty row " + std::to_string(i) + " excludes 0");
+        if (!within(0.0, rl[i], ru[i])) { infeasible("empty row " + std::to_string(i) + " excludes 0"); return; }
         row_alive[i] = 0;
         ++r.removed_rows;
         changed = true;
@@ -369,7 +447,7 @@ PresolveResult presolve(const Model& M) {  // presolve.cpp:22-156 (LP: no intege
         double nl = set_lower ? lo : cl[j], nu = set_upper ? hi : cu[j];
         if (nl > nu) {
           if (nl - nu > kFeasTol * (1 + std::fabs(nl)))
-            return infeasible("singleton row " + std::to_string(i) + " conflicts with the bounds of its column");
+            { infeasible("singleton row " + std::to_string(i) + " conflicts with the bounds of its column"); return; }
           nl = nu = 0.5 * (nl + nu);
         }
         cl[j] = nl;
@@ -412,10 +490,11 @@ PresolveResult presolve(const Model& M) {  // presolve.cpp:22-156 (LP: no intege
   }
   if (r.removed_rows == 0 && r.removed_cols == 0) {
     r.outcome = PresolveResult::Outcome::Unchanged;
-    return r;
+    return;
   }
   Model& R = r.reduced;
-  std::vector<int> new_row(m, -1);
+  std::vector<int>& new_row = S.new_row;
+  new_row.assign(static_cast<std::size_t>(m), -1);
   for (int i = 0; i < m; ++i)
     if (row_alive[i]) new_row[i] = static_cast<int>(r.row_map.size()), r.row_map.push_back(i);
   for (int j = 0; j < n; ++j)
@@ -470,7 +549,6 @@ PresolveResult presolve(const Model& M) {  // presolve.cpp:22-156 (LP: no intege
     R.row_upper.push_back(ru[i]);
   }
   r.outcome = PresolveResult::Outcome::Reduced;
-  return r;
 }
 
 Solution postsolve(const Model& M, const PresolveResult& r, const Solution& red) {  // presolve.cpp:158-193
@@ -706,7 +784,24 @@ Solution solve_impl(const Model& model, const Options& options) {
   if (!options.presolve || bad_warm || bad_warm_values || !model.validate().empty()) return solve_direct(model, options);
   if (auto why = model.crossed_bounds(); !why.empty()) return trivially_infeasible(options, why);
   const auto t0 = clock_t_::now();
-  PresolveResult pr = presolve(model);
+  // this thread's presolve result, its memory reused from the previous call (host_keep)
+  struct PresolveHolder {
+    PresolveResult r;
+    std::size_t accounted = 0;
+    ~PresolveHolder() { host_keep(accounted, 0); }
+  };
+  static thread_local PresolveHolder t_pr;
+  struct KeepResult {
+    PresolveHolder& h;
+    ~KeepResult() {
+      const PresolveResult& r = h.r;
+      const std::size_t bytes = capacity_bytes(r.reduced) + 4 * (r.row_map.capacity() + r.col_map.capacity()) +
+                                8 * r.fixed_value.capacity() + sizeof(PresolveResult::Singleton) * r.singletons.capacity();
+      if (!host_keep(h.accounted, bytes)) h.r = PresolveResult{};
+    }
+  } keep_result{t_pr};
+  PresolveResult& pr = t_pr.r;
+  presolve_into(model, pr);
   const double presolve_s = since(t0);
   phase_note("presolve", presolve_s);
   if (pr.outcome == PresolveResult::Outcome::Unchanged) {

@@ -104,6 +104,8 @@ struct PresolveResult {
   std::vector<Singleton> singletons;
 };
 PresolveResult presolve(const Model& model);
+// The same into `r`, reusing the capacity of its vectors (the dispatcher keeps one per thread).
+void presolve_into(const Model& model, PresolveResult& r);
 Solution postsolve(const Model& original, const PresolveResult& r, const Solution& reduced);
 
 // One 64-bit FNV-1a digest of everything presolve decided: outcome, counts, row and column maps,
@@ -113,6 +115,16 @@ std::uint64_t presolve_digest(const PresolveResult& r);
 
 // The library entry point: never throws (solve.cpp:194-210).
 Solution solve(const Model& model, const Options& options);
+
+// Host buffers kept between calls. A call on a large model spends more time page-faulting
+// fresh multi-hundred-megabyte vectors than copying into them, so the dispatcher keeps, per
+// thread, its model copy, presolve scratch and reduced model, and the certified bound's term
+// arrays, and reuses their memory on the next call. All threads together keep at most
+// PS26119_HOST_REUSE_MB MiB (default 2048; 0 keeps nothing); beyond that a thread frees its
+// buffers after the call. host_keep(accounted, bytes): a holder that has `accounted` bytes
+// counted asks to keep `bytes`; true: kept (and counted), false: the caller frees them.
+bool host_keep(std::size_t& accounted, std::size_t bytes);
+std::size_t capacity_bytes(const Model& m);
 
 // Host phase timings of one entry-point call: phase_log_begin(on) starts a log on this thread
 // (nothing is recorded when `on` is false), phase_note adds one phase, phase_log_end prints the
