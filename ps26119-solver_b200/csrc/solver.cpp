@@ -551,8 +551,31 @@ void presolve_into(const Model& M, PresolveResult& r) {  // presolve.cpp:22-156 
   r.outcome = PresolveResult::Outcome::Reduced;
 }
 
+namespace {
+// Every field of `s` except x, y and z: postsolve rebuilds those on the original model, so
+// copying the reduced ones (tens of MB on large models) would only be overwritten. The size
+// check makes a field added to Solution fail to compile here until it is copied too.
+Solution without_xyz(const Solution& s) {
+  static_assert(sizeof(Solution) == 640, "Solution changed: copy the new field in without_xyz");
+  Solution o;
+  o.status = s.status;
+  o.dual_ray = s.dual_ray, o.primal_ray = s.primal_ray;
+  o.objective = s.objective, o.dual_objective = s.dual_objective;
+  o.primal_residual = s.primal_residual, o.dual_residual = s.dual_residual, o.gap = s.gap;
+  o.iterations = s.iterations, o.seconds = s.seconds, o.setup_seconds = s.setup_seconds;
+  o.certified_bound = s.certified_bound, o.primal_weight = s.primal_weight;
+  o.check = s.check, o.check_primal = s.check_primal, o.check_dual = s.check_dual, o.check_gap = s.check_gap;
+  o.engine = s.engine, o.precision = s.precision, o.message = s.message;
+  o.engine_result = s.engine_result;
+  o.presolve_seconds = s.presolve_seconds;
+  o.model_fingerprint = s.model_fingerprint;
+  o.iterations_to_fast = s.iterations_to_fast;
+  return o;
+}
+}  // namespace
+
 Solution postsolve(const Model& M, const PresolveResult& r, const Solution& red) {  // presolve.cpp:158-193
-  Solution s = red;
+  Solution s = without_xyz(red);
   const int m = M.num_rows, n = M.num_cols;
   s.x.assign(n, 0.0);
   s.y.assign(m, 0.0);

@@ -6,6 +6,7 @@ prints the library's digest, reference.presolve_file the reference's. Equal dige
 reduced model the engine solves and the postsolve data are the reference's, bit for bit."""
 import glob
 import os
+import subprocess
 
 import numpy as np
 import pytest
@@ -108,3 +109,16 @@ def test_presolve_on_reference_data_files(ref, path):
         assert got is None
     else:
         assert got == want, (info, out)
+
+
+def test_presolve_without_host_buffer_reuse(ref, tmp_path):
+    # PS26119_HOST_REUSE_MB=0: presolve frees its scratch after every call; the decisions are
+    # the same as with the buffers kept
+    path = tmp_path / "p.mps"
+    write_mps(planted(3), path)
+    want, _ = ref.presolve_file(str(path))
+    from test_io import CLI
+    env = dict(os.environ, PS26119_HOST_REUSE_MB="0")
+    r = subprocess.run([CLI, "info", str(path)], capture_output=True, text=True, env=env, timeout=120)
+    got = [ln for ln in r.stdout.splitlines() if "presolve digest" in ln][0].split()[-1]
+    assert r.returncode == 0 and got == want
