@@ -173,7 +173,7 @@ int solve_host(int num_rows, int num_cols, int sense, double obj_offset, const d
     Options o;
     if (const char* bad = to_options(opt, num_rows, num_cols, o)) return phase_log_begin(false), invalid(bad);
     if (const char* bad = apply_engine_options(eo, o)) return phase_log_begin(false), invalid(bad);
-    const Solution s = solve(m, o);
+    Solution s = solve(m, o);
     fill(s, result);
     fill_stats(s, s.engine_result.iterations > 0 ? num_rows : 0, num_cols, nnz);
     g_stats.call_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - call_t0).count();
@@ -185,6 +185,7 @@ int solve_host(int num_rows, int num_cols, int sense, double obj_offset, const d
     out(z, s.z, num_cols);
     out(dual_ray, s.dual_ray, num_rows);
     out(primal_ray, s.primal_ray, num_cols);
+    pool_vector(std::move(s.x)), pool_vector(std::move(s.y)), pool_vector(std::move(s.z));  // for the next call
     phase_note("call", std::chrono::duration<double>(std::chrono::steady_clock::now() - call_t0).count());
     phase_log_end("solve_lp");
     return result->status;

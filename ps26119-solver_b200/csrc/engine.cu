@@ -1206,7 +1206,7 @@ EngineResult run_engine_host(const HostModelView& H, const EngineOptions& opt, H
   M.col_start = cs.get(), M.row_index = ri.get(), M.value = v.get();
   DeviceOutputs o{x.get(), y.get(), z.get(), dr.get(), pr.get()};
   EngineResult R = run_engine(M, opt, o, st);
-  out.x.resize(n), out.y.resize(m), out.z.resize(n);
+  out.x = pooled_vector(n), out.y = pooled_vector(m), out.z = pooled_vector(n);
   x.download(out.x.data(), n, st);
   y.download(out.y.data(), m, st);
   z.download(out.z.data(), n, st);

@@ -101,6 +101,11 @@ struct HostModelView {
 struct HostOutputs {
   std::vector<double> x, y, z, dual_ray, primal_ray;
 };
+// A per-thread pool of solution-sized host vectors (x, y, z), kept within the host reuse limit
+// (host_keep): pooled_vector(n) returns n zeros, in a pooled buffer's memory when one is large
+// enough (no fresh pages to fault in); pool_vector hands a finished vector's memory back.
+std::vector<double> pooled_vector(std::size_t n);
+void pool_vector(std::vector<double>&& v);
 EngineResult run_engine_host(const HostModelView& M, const EngineOptions& opt, HostOutputs& out);
 
 // Throws a runtime_error when no usable CUDA device exists (the C API reports it as

@@ -370,6 +370,44 @@ bool host_keep(std::size_t& accounted, std::size_t bytes) {
   return true;
 }
 
+namespace {
+struct VectorPool {
+  std::vector<std::vector<double>> free;
+  std::size_t accounted = 0;
+  std::size_t bytes() const {
+    std::size_t b = 0;
+    for (const auto& v : free) b += 8 * v.capacity();
+    return b;
+  }
+  ~VectorPool() { host_keep(accounted, 0); }
+};
+thread_local VectorPool t_vectors;
+}  // namespace
+
+std::vector<double> pooled_vector(std::size_t n) {
+  VectorPool& P = t_vectors;
+  long long best = -1;
+  for (std::size_t k = 0; k < P.free.size(); ++k)
+    if (P.free[k].capacity() >= n && (best < 0 || P.free[k].capacity() < P.free[static_cast<std::size_t>(best)].capacity()))
+      best = static_cast<long long>(k);
+  std::vector<double> v;
+  if (best >= 0) {
+    v.swap(P.free[static_cast<std::size_t>(best)]);
+    P.free.erase(P.free.begin() + best);
+    host_keep(P.accounted, P.bytes());
+  }
+  v.assign(n, 0.0);
+  return v;
+}
+
+void pool_vector(std::vector<double>&& v) {
+  if (v.capacity() < (std::size_t{1} << 16)) return;  // small ones are cheap to allocate
+  VectorPool& P = t_vectors;
+  P.free.push_back(std::move(v));
+  if (P.free.size() > 8) P.free.erase(P.free.begin());  // the 8 most recent
+  if (!host_keep(P.accounted, P.bytes())) std::vector<std::vector<double>>().swap(P.free);
+}
+
 PresolveResult presolve(const Model& M) {
   PresolveResult r;
   presolve_into(M, r);
@@ -577,8 +615,8 @@ Solution without_xyz(const Solution& s) {
 Solution postsolve(const Model& M, const PresolveResult& r, const Solution& red) {  // presolve.cpp:158-193
   Solution s = without_xyz(red);
   const int m = M.num_rows, n = M.num_cols;
-  s.x.assign(n, 0.0);
-  s.y.assign(m, 0.0);
+  s.x = pooled_vector(static_cast<std::size_t>(n));
+  s.y = pooled_vector(static_cast<std::size_t>(m));
   const bool have_x = red.x.size() == r.col_map.size();
   const bool have_y = red.y.size() == r.row_map.size();
   for (int j = 0; j < n; ++j)
@@ -594,7 +632,8 @@ Solution postsolve(const Model& M, const PresolveResult& r, const Solution& red)
     const double zm = M.sense * z;
     if ((zm > 0 && it->set_lower) || (zm < 0 && it->set_upper)) s.y[it->row] = z / it->a;
   }
-  s.z = M.obj;
+  s.z = pooled_vector(static_cast<std::size_t>(n));
+  std::copy(M.obj.begin(), M.obj.end(), s.z.begin());
   parallel_ranges(n, [&](long long jb, long long je) {  // each z_j in its own column order
     for (long long j = jb; j < je; ++j)
       for (int p = M.col_start[j]; p < M.col_start[j + 1]; ++p) s.z[j] -= M.value[p] * s.y[M.row_index[p]];
@@ -873,6 +912,12 @@ Solution solve_impl(const Model& model, const Options& options) {
     for (int i : pr.row_map) inner.warm_y.push_back(options.warm_y[i]);
   }
   Solution red;
+  struct PoolAtExit {  // the reduced solution's vectors go back to this thread's pool
+    Solution& s;
+    ~PoolAtExit() {
+      pool_vector(std::move(s.x)), pool_vector(std::move(s.y)), pool_vector(std::move(s.z));
+    }
+  } pool_red{red};
   if (pr.reduced.num_cols == 0 && pr.reduced.num_rows == 0) {
     red.status = Status::Optimal;
     red.engine = "presolve";
