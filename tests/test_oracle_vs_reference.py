@@ -10,6 +10,7 @@ import pytest
 
 import lps
 from ps26119 import generators as g
+from conftest import REFERENCE_DATA
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_runs.json")
 
@@ -125,12 +126,11 @@ def test_oracle_backend_ops_match_reference(ref, orc, precision):
         assert got[0][2] == got[1][2]
 
 
-@pytest.mark.skipif(not os.path.isdir(os.path.join(lps.os.sep, "root", "reference", "data")),
-                    reason="reference data not mounted")
+@pytest.mark.skipif(not os.path.isdir(REFERENCE_DATA), reason="reference data not mounted")
 def test_oracle_on_reference_netlib_fixtures(ref, orc):
     """The reference's small Netlib fixtures, read by path: the oracle reproduces the reference
     engine bit for bit and meets the published optima (data/netlib_small/optima.csv) to 1e-6."""
-    base = "/root/reference/data/netlib_small"
+    base = os.path.join(REFERENCE_DATA, "netlib_small")
     optima = {}
     for line in open(os.path.join(base, "optima.csv")).read().splitlines()[1:]:
         f = line.split(",")
