@@ -60,6 +60,25 @@ constexpr double kVerifyPrimal = 1e-6, kVerifyDual = 1e-6, kVerifyGap = 1e-6;
 #define B200_BATCH_NZ 2
 #endif
 constexpr int kBatchNz = B200_BATCH_NZ;
+// 1: the step epilogues load their streamed operands evict-first and store the block the next
+// kernel gathers (x̄, y) evict-last, so that it stays in L2 (as the single-LP kernels do).
+#ifndef B200_BATCH_HINTS
+#define B200_BATCH_HINTS 1
+#endif
+__device__ __forceinline__ double bstream(const double* p) {
+#if B200_BATCH_HINTS
+  return ld_stream(p);
+#else
+  return *p;
+#endif
+}
+__device__ __forceinline__ void bkeep(double* p, double v) {
+#if B200_BATCH_HINTS
+  st_keep(p, v);
+#else
+  *p = v;
+#endif
+}
 struct BNoPre {};
 template <class E>
 __device__ __forceinline__ auto bload(const E& e, long long q, int t, int) -> decltype(e.load(q, t)) {
@@ -156,7 +175,9 @@ struct EpiBPrimal {
   struct Pre {
     double x, c, l, u, x0;
   };
-  __device__ Pre load(long long q, int) const { return Pre{X[q], C[q], L[q], U[q], X0[q]}; }
+  __device__ Pre load(long long q, int) const {
+    return Pre{bstream(X + q), bstream(C + q), bstream(L + q), bstream(U + q), bstream(X0 + q)};
+  }
   __device__ void operator()(long long, int t, long long q, double aty, double*, const Pre& p) const {
     const long long in = inner0[t] + step;
     const double w = static_cast<double>(in + 1) / static_cast<double>(in + 2);
@@ -165,7 +186,7 @@ struct EpiBPrimal {
     // x̂ is read only by the residual, check and restart that follow the epoch's last step and
     // the first step of a slot's Halpern cycle; on the other steps it is not stored
     if (step == last || in == 0) XH[q] = h;
-    XB[q] = 2 * h - x;
+    bkeep(XB + q, 2 * h - x);  // gathered by the dual kernel next
     X[q] = w * (a2 * h + b2 * x) + (1 - w) * p.x0;
   }
 };
@@ -180,7 +201,7 @@ struct EpiBDual {
   struct Pre {
     double y, rl, ru, y0;
   };
-  __device__ Pre load(long long q, int) const { return Pre{Y[q], RL[q], RU[q], Y0[q]}; }
+  __device__ Pre load(long long q, int) const { return Pre{bstream(Y + q), bstream(RL + q), bstream(RU + q), bstream(Y0 + q)}; }
   __device__ void operator()(long long, int t, long long q, double ax, double*, const Pre& p) const {
     const long long in = inner0[t] + step;
     const double w = static_cast<double>(in + 1) / static_cast<double>(in + 2);
@@ -192,7 +213,7 @@ struct EpiBDual {
       YH[q] = h;
       YB[q] = 2 * h - y;
     }
-    Y[q] = w * (a2 * h + b2 * y) + (1 - w) * p.y0;
+    bkeep(Y + q, w * (a2 * h + b2 * y) + (1 - w) * p.y0);  // gathered by the primal kernel next
   }
 };
 // Residual rows after adx = Ã·Δx (compute_residuals, batch.cpp:305-318): terms Δy², Δy·(AΔx)
