@@ -126,3 +126,14 @@ def test_pointer_past_nnz_reports_the_decreasing_column(big):
 
 def test_valid_model_has_no_message(big):
     assert _message(big) == "" and sequential_first_error(big) == ""
+
+
+def test_calls_of_different_sizes_on_one_thread(big):
+    # The C API keeps the calling thread's model copy for its next call: models of other sizes,
+    # valid and invalid, must each be judged on their own data only.
+    small = g.random_lp(30, seed=5)
+    bad_small = _edit(small, value=lambda a: a.__setitem__(3, np.nan))
+    bad_big = _edit(big, row_index=lambda a: a.__setitem__(5, -2))
+    sequence = [big, bad_small, small, bad_big, small, big, bad_small]
+    for lp in sequence:
+        assert _message(lp) == sequential_first_error(lp)
