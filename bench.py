@@ -8,7 +8,7 @@
 One STEP is one cold solve of the seeded LP on the device: setup (structure, scaling, ‖Ã‖₂),
 L r²HPDHG iterations with their checks every 64 iterations, and the finish (unscaling, KKT,
 z = c − Aᵀy, in-process check). The full solve of this LP to 1e-8 takes 3,724,096 iterations
-(about nine minutes), so the default step caps the iterations at L = 6,400 and the metric is
+(about six minutes), so the default step caps the iterations at L = 6,400 and the metric is
 r²HPDHG iterations per second, whole job (time to 1e-8 = setup + iterations ÷ this rate).
 `--full` drops the cap: the step is a complete solve to 1e-8 KKT and the metric is solves/s
 (use it with --workload random10k: 249,088 iterations).
@@ -167,6 +167,17 @@ def run_serve(args, rank, world, local):
     }
 
 
+def cpu_model():
+    """The host CPU's model name (for the CPU baseline's record), or None."""
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
 def hbm_peak():
     """The measured HBM copy bandwidth (GB/s) and its source; the pool's earlier measurement,
     6,650 GB/s, when the measured file is absent."""
@@ -261,6 +272,7 @@ def run_batch(args, rank, world, local):
             rs = time.perf_counter() - t0
             rits = max(x["iterations"] for x in w)
             line["cpu_baseline"] = {"value": K * rits / rs, "unit": "scenario-iterations/s", "cores": cores,
+                                    "cpu_model": cpu_model(),
                                     "kind": "reference",
                                     "sample": f"reference solve_batch ({cores} threads), {rits} lockstep iterations "
                                               f"of {K} scenarios incl. setup in {rs:.1f} s"}
@@ -571,7 +583,7 @@ def reference_sample(args, lp, iterations, full):
     import reference
     cores = os.cpu_count() or 1
     if not reference.available():
-        return {"value": None, "unit": "iterations/s", "cores": cores, "kind": "reference",
+        return {"value": None, "unit": "iterations/s", "cores": cores, "cpu_model": cpu_model(), "kind": "reference",
                 "sample": "reference library not built"}
     s = reference.solve(lp, presolve=True, precision=args.precision, threads=0,
                         iteration_limit=args.cpu_sample_iterations)
@@ -579,7 +591,7 @@ def reference_sample(args, lp, iterations, full):
     its = full if args.full else iterations
     total = s.setup_seconds + per_iter * its
     return {"value": (1.0 if args.full else its) / total, "unit": "solves/s" if args.full else "iterations/s",
-            "cores": cores, "kind": "reference",
+            "cores": cores, "cpu_model": cpu_model(), "kind": "reference",
             "sample": f"reference ps26119::solve (r2hpdhg, presolve, {cores} threads): {s.iterations} iterations "
                       f"+ setup in {s.seconds:.1f} s ({per_iter * 1e3:.2f} ms/iteration, setup "
                       f"{s.setup_seconds:.2f} s), applied to {its} iterations"}
@@ -618,7 +630,7 @@ def run_reference(args, rank, world):
                 "data": "synthetic (seeded generator)",
                 "config": {"workload": WORKLOADS[args.workload]["desc"], "scenarios": K, "tolerance": 1e-8},
                 "impl": "reference",
-                "cpu_baseline": {"value": value, "unit": unit, "cores": cores, "kind": "reference", "sample": sample},
+                "cpu_baseline": {"value": value, "unit": unit, "cores": cores, "cpu_model": cpu_model(), "kind": "reference", "sample": sample},
                 "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     full = WORKLOADS[args.workload]["full_iterations"]
     its = full if args.full else args.iterations
@@ -642,7 +654,7 @@ def run_reference(args, rank, world):
                        "nnz": lp.nnz, "tolerance": 1e-8, "precision": args.precision,
                        "iterations_per_step": its},
             "impl": "reference",
-            "cpu_baseline": {"value": value, "unit": unit, "cores": cores, "kind": "reference", "sample": sample},
+            "cpu_baseline": {"value": value, "unit": unit, "cores": cores, "cpu_model": cpu_model(), "kind": "reference", "sample": sample},
             "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
