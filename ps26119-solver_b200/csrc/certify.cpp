@@ -105,26 +105,33 @@ double round_up(const DD& v, double err) {
 }
 bool may_underflow(const DD& p) { return p.hi != 0.0 && std::fabs(p.hi) < 1e-280; }
 
-// Exact sum as a nonoverlapping expansion (GROW-EXPANSION, zero elimination). false on a
-// non-finite value or an expansion longer than 64 components (the caller keeps its interval).
-bool grow_expansion(std::vector<double>& e, double b, std::vector<double>& scratch) {
-  if (b == 0.0) return true;
-  if (!std::isfinite(b)) return false;
-  scratch.clear();
-  double q = b;
-  for (double ei : e) {
-    const double sum = q + ei;
-    const double bv = sum - q;
-    const double av = sum - bv;
-    const double err = (q - av) + (ei - bv);
-    q = sum;
-    if (err != 0.0) scratch.push_back(err);
+// Exact sum as a nonoverlapping expansion (GROW-EXPANSION, zero elimination), in a fixed array
+// updated in place (component k is read before any write at an index ≤ k). grow() returns
+// false on a non-finite value or an expansion longer than 64 components (the caller then keeps
+// its interval).
+struct Expansion {
+  double c[66];
+  int n = 0;
+  bool grow(double b) {
+    if (b == 0.0) return true;
+    if (!std::isfinite(b)) return false;
+    double q = b;
+    int w = 0;
+    for (int k = 0; k < n; ++k) {
+      const double ei = c[k];
+      const double sum = q + ei;
+      const double bv = sum - q;
+      const double av = sum - bv;
+      const double err = (q - av) + (ei - bv);
+      q = sum;
+      if (err != 0.0) c[w++] = err;
+    }
+    n = w;
+    if (!std::isfinite(q)) return false;
+    if (q != 0.0) c[n++] = q;
+    return n <= 64;
   }
-  if (!std::isfinite(q)) return false;
-  if (q != 0.0) scratch.push_back(q);
-  e.swap(scratch);
-  return e.size() <= 64;
-}
+};
 
 // min over x ∈ [lo, hi] of z·x as an exact product; `inf` when it is −∞.
 DD min_term(double z, double lo, double hi, bool& inf) {
@@ -183,11 +190,11 @@ SafeBound bound_with(const Model& M, const std::vector<double>& y, const std::ve
   col_term.assign(static_cast<std::size_t>(n), DD{});
   col_inf.assign(static_cast<std::size_t>(n), 0);
   parallel_ranges(n, [&](long long jb, long long je) {
-    std::vector<double> ex, scratch;
-    ex.reserve(16);
-    scratch.reserve(17);
+    Expansion ex;
     for (long long jj = jb; jj < je; ++jj) {
       const int j = static_cast<int>(jj);
+      if (jj + 2 < je)  // the multipliers of the column after next: random reads, started early
+        for (int p = M.col_start[j + 2]; p < M.col_start[j + 3]; ++p) __builtin_prefetch(&y[M.row_index[p]]);
       DD z = dd_of(sense * M.obj[j]);
       double mag = 0.0;  // Σ|terms| after the first (exact) assignment
       int cnt = 0;
@@ -205,21 +212,21 @@ SafeBound bound_with(const Model& M, const std::vector<double>& y, const std::ve
       if (cnt > 0 && !uf) {
         // tighter, still rigorous: z exactly as an expansion (exact cancellation gives exactly 0,
         // a one-component expansion is an exact double, otherwise enclose its dd sum)
-        ex.clear();
-        bool ok = grow_expansion(ex, sense * M.obj[j], scratch);
+        ex.n = 0;
+        bool ok = ex.grow(sense * M.obj[j]);
         for (int p = M.col_start[j]; ok && p < M.col_start[j + 1]; ++p) {
           const DD prod = exact_product(M.value[p], sense * y[M.row_index[p]]);
-          ok = grow_expansion(ex, -prod.hi, scratch) && grow_expansion(ex, -prod.lo, scratch);
+          ok = ex.grow(-prod.hi) && ex.grow(-prod.lo);
         }
         if (ok) {
-          if (ex.empty()) {
+          if (ex.n == 0) {
             zlo = zhi = 0.0;
-          } else if (ex.size() == 1) {
-            zlo = zhi = ex[0];
+          } else if (ex.n == 1) {
+            zlo = zhi = ex.c[0];
           } else {
             DD v;
-            for (double c : ex) v = v + c;  // smallest component first
-            const double ev = static_cast<double>(ex.size() + 2) * kRel * std::fabs(value(v)) * 1.0000001;
+            for (int k = 0; k < ex.n; ++k) v = v + ex.c[k];  // smallest component first
+            const double ev = static_cast<double>(ex.n + 2) * kRel * std::fabs(value(v)) * 1.0000001;
             zlo = std::max(zlo, round_down(v, ev));
             zhi = std::min(zhi, round_up(v, ev));
           }
