@@ -424,6 +424,12 @@ const char* ps26119_backend_last_error(void) { return g_backend_error.c_str(); }
     g_backend_error = e.what();                           \
     return PS26119_NUMERICAL_ERROR;                       \
   }
+// inside B200_GUARD: a NULL host pointer argument is an invalid argument, not a crash
+#define B200_NEED(p)                            \
+  if (!(p)) {                                   \
+    g_backend_error = "NULL pointer argument";  \
+    return PS26119_INVALID_ARGUMENT;            \
+  }
 
 int ps26119_backend_new(ps26119_backend** out, int num_rows, int num_cols, int sense, double obj_offset,
                         const double* c, const double* col_lower, const double* col_upper, const double* row_lower,
@@ -434,11 +440,16 @@ int ps26119_backend_new(ps26119_backend** out, int num_rows, int num_cols, int s
   try {
     Model m;
     m.num_rows = num_rows, m.num_cols = num_cols, m.sense = sense, m.obj_offset = obj_offset;
-    if (num_rows < 0 || num_cols < 0 || !col_start) {
-      g_backend_error = "invalid dimensions or NULL col_start";
+    auto invalid = [](const char* why) {
+      g_backend_error = why;
       return PS26119_INVALID_ARGUMENT;
-    }
+    };
+    if (num_rows < 0 || num_cols < 0 || !col_start) return invalid("invalid dimensions or NULL col_start");
+    if (num_cols > 0 && (!c || !col_lower || !col_upper)) return invalid("column data is NULL");
+    if (num_rows > 0 && (!row_lower || !row_upper)) return invalid("row bounds are NULL");
     const int nnz = col_start[num_cols];
+    if (nnz < 0) return invalid("col_start[n] < 0");
+    if (nnz > 0 && (!row_index || !value)) return invalid("matrix arrays are NULL");
     m.obj.assign(c, c + num_cols);
     m.col_lower.assign(col_lower, col_lower + num_cols);
     m.col_upper.assign(col_upper, col_upper + num_cols);
@@ -489,16 +500,16 @@ int ps26119_backend_create(ps26119_backend* b, int dual) {
     return -1;
   }
 }
-int ps26119_backend_upload(ps26119_backend* b, int v, const double* src) { B200_GUARD(b->impl->upload(v, src)) }
-int ps26119_backend_download(ps26119_backend* b, int v, double* dst) { B200_GUARD(b->impl->download(v, dst)) }
+int ps26119_backend_upload(ps26119_backend* b, int v, const double* src) { B200_GUARD(B200_NEED(src); b->impl->upload(v, src)) }
+int ps26119_backend_download(ps26119_backend* b, int v, double* dst) { B200_GUARD(B200_NEED(dst); b->impl->download(v, dst)) }
 int ps26119_backend_fill(ps26119_backend* b, int v, double a) { B200_GUARD(b->impl->fill(v, a)) }
 int ps26119_backend_copy(ps26119_backend* b, int dst, int src) { B200_GUARD(b->impl->copy(dst, src)) }
 int ps26119_backend_axpby(ps26119_backend* b, double a, int x, double bb, int y) { B200_GUARD(b->impl->axpby(a, x, bb, y)) }
 int ps26119_backend_spmv(ps26119_backend* b, int x, int out) { B200_GUARD(b->impl->spmv(x, out)) }
 int ps26119_backend_spmv_t(ps26119_backend* b, int y, int out) { B200_GUARD(b->impl->spmv_t(y, out)) }
-int ps26119_backend_dot(ps26119_backend* b, int x, int y, double* out) { B200_GUARD(*out = b->impl->dot(x, y)) }
-int ps26119_backend_norm2(ps26119_backend* b, int x, double* out) { B200_GUARD(*out = b->impl->norm2(x)) }
-int ps26119_backend_diff_norm2(ps26119_backend* b, int x, int y, double* out) { B200_GUARD(*out = b->impl->diff_norm2(x, y)) }
+int ps26119_backend_dot(ps26119_backend* b, int x, int y, double* out) { B200_GUARD(B200_NEED(out); *out = b->impl->dot(x, y)) }
+int ps26119_backend_norm2(ps26119_backend* b, int x, double* out) { B200_GUARD(B200_NEED(out); *out = b->impl->norm2(x)) }
+int ps26119_backend_diff_norm2(ps26119_backend* b, int x, int y, double* out) { B200_GUARD(B200_NEED(out); *out = b->impl->diff_norm2(x, y)) }
 int ps26119_backend_primal_step(ps26119_backend* b, int x, int aty, double tau, int xh) {
   B200_GUARD(b->impl->primal_step(x, aty, tau, xh))
 }
@@ -521,7 +532,7 @@ int ps26119_backend_fused_dual(ps26119_backend* b, int xb, int y, int y0, double
                                int yb) {
   B200_GUARD(b->impl->fused_dual(xb, y, y0, sigma, w, rho, yh, yb))
 }
-int ps26119_backend_kkt(ps26119_backend* b, int xs, int ys, double* out) { B200_GUARD(b->impl->kkt(xs, ys, out)) }
+int ps26119_backend_kkt(ps26119_backend* b, int xs, int ys, double* out) { B200_GUARD(B200_NEED(out); b->impl->kkt(xs, ys, out)) }
 int ps26119_backend_sync(ps26119_backend* b) { B200_GUARD(b->impl->sync()) }
 long long ps26119_backend_scaled_get(ps26119_backend* b, int which, double* dst) {
   try {
@@ -539,8 +550,8 @@ long long ps26119_backend_scaled_structure(ps26119_backend* b, int which, int* r
     return -1;
   }
 }
-int ps26119_backend_scalars(ps26119_backend* b, double* out) { B200_GUARD(b->impl->scalars(out)) }
-int ps26119_backend_norm2_estimate(ps26119_backend* b, double* out) { B200_GUARD(*out = b->impl->norm2_estimate()) }
+int ps26119_backend_scalars(ps26119_backend* b, double* out) { B200_GUARD(B200_NEED(out); b->impl->scalars(out)) }
+int ps26119_backend_norm2_estimate(ps26119_backend* b, double* out) { B200_GUARD(B200_NEED(out); *out = b->impl->norm2_estimate()) }
 
 }  // extern "C"
 
@@ -748,7 +759,12 @@ extern "C" int ps26119_server_poll(ps26119_server* server, long long id, int wai
   if (!server) return -1;
   Solution s;
   b200::RequestTimes t;
-  const int r = server->server.take(id, wait != 0, s, t);
+  int r;
+  try {
+    r = server->server.take(id, wait != 0, s, t);
+  } catch (...) {  // no exception crosses the C boundary
+    return -1;
+  }
   if (r != 1) return r;
   if (result) {
     clear(result);

@@ -84,6 +84,31 @@ def test_invalid_arguments_never_reach_the_engine():
     assert st == ps26119.INVALID_ARGUMENT and b"invalid model" in res.message
 
 
+def test_backend_rejects_null_arguments_before_the_device():
+    """The plugin ABI checks its arrays and handles like the solve entry points do: a NULL
+    array or backend is INVALID_ARGUMENT with a message, never a crash or a device call."""
+    L = ps26119.load()
+    lp = lps.wyndor()
+    P = ps26119._ptr
+    f = lambda a: np.ascontiguousarray(a, dtype=np.float64)
+    i = lambda a: np.ascontiguousarray(a, dtype=np.int32)
+    arrays = [f(lp.c), f(lp.col_lower), f(lp.col_upper), f(lp.row_lower), f(lp.row_upper), i(lp.col_start),
+              i(lp.row_index), f(lp.value)]
+    for k, text in ((0, b"column data"), (3, b"row bounds"), (6, b"matrix arrays"), (7, b"matrix arrays")):
+        args = [P(a, ctypes.c_int) if a.dtype == np.int32 else P(a) for a in arrays]
+        args[k] = None
+        h = ctypes.c_void_p(1)
+        st = L.ps26119_backend_new(ctypes.byref(h), lp.num_rows, lp.num_cols, lp.sense, lp.offset, *args, None, 0)
+        assert st == ps26119.INVALID_ARGUMENT, k
+        assert not h.value, k
+        assert text in L.ps26119_backend_last_error(), (k, L.ps26119_backend_last_error())
+    out = ctypes.c_double()
+    assert L.ps26119_backend_dot(None, 0, 0, ctypes.byref(out)) == ps26119.INVALID_ARGUMENT
+    assert b"null backend" in L.ps26119_backend_last_error()
+    assert L.ps26119_backend_sync(None) == ps26119.INVALID_ARGUMENT
+    assert L.ps26119_backend_scaled_get(None, 0, None) == -1
+
+
 def test_cpu_engine_requests_are_refused_without_fallback():
     L = ps26119.load()
     o = ps26119._options("r2hpdhg", "fp64", False, 1e-8, 3600.0, 0, 0, 1)
