@@ -17,6 +17,7 @@
 #include "../../include/ps26119_backend.h"
 #include "certify.hpp"
 #include "io.hpp"
+#include "parallel.hpp"
 #include "solver.hpp"
 #include "serve.hpp"
 
@@ -157,14 +158,22 @@ int solve_host(int num_rows, int num_cols, int sense, double obj_offset, const d
     m.num_cols = num_cols;
     m.sense = sense;
     m.obj_offset = obj_offset;
-    m.obj.assign(c, c + num_cols);
-    m.col_lower.assign(col_lower, col_lower + num_cols);
-    m.col_upper.assign(col_upper, col_upper + num_cols);
-    m.row_lower.assign(row_lower, row_lower + num_rows);
-    m.row_upper.assign(row_upper, row_upper + num_rows);
-    m.col_start.assign(col_start, col_start + num_cols + 1);
-    m.row_index.assign(row_index, row_index + nnz);
-    m.value.assign(value, value + nnz);
+    // copied on the host threads: one thread's memcpy of a large model's arrays is several times
+    // slower than the memory allows
+    const std::size_t n = static_cast<std::size_t>(num_cols), rows = static_cast<std::size_t>(num_rows),
+                      k = static_cast<std::size_t>(nnz);
+    size_for_copy(m.obj, n), size_for_copy(m.col_lower, n), size_for_copy(m.col_upper, n);
+    size_for_copy(m.row_lower, rows), size_for_copy(m.row_upper, rows);
+    size_for_copy(m.col_start, n + 1), size_for_copy(m.row_index, k), size_for_copy(m.value, k);
+    const CopyJob copies[] = {{m.obj.data(), c, 8 * n},
+                              {m.col_lower.data(), col_lower, 8 * n},
+                              {m.col_upper.data(), col_upper, 8 * n},
+                              {m.row_lower.data(), row_lower, 8 * rows},
+                              {m.row_upper.data(), row_upper, 8 * rows},
+                              {m.col_start.data(), col_start, 4 * (n + 1)},
+                              {m.row_index.data(), row_index, 4 * k},
+                              {m.value.data(), value, 8 * k}};
+    parallel_copy(copies, sizeof copies / sizeof copies[0]);
     if (auto err = m.validate(); !err.empty()) {
       phase_log_begin(false);
       return invalid(("invalid model: " + err).c_str());

@@ -2,7 +2,7 @@
 // for the commands this library covers):
 //
 //   ps26119 --version
-//   ps26119 info  <file.mps|file.lpm>
+//   ps26119 info  <file.mps|file.lpm>...
 //   ps26119 convert <file.mps|file.lpm> <out.lpm>
 //   ps26119 solve <file.mps|file.lpm> [--algorithm auto|r2hpdhg|pdlp] [--precision fp64|mixed] [--gpu]
 //                 [--tol e] [--time-limit s] [--iteration-limit n] [--no-presolve] [--exact]
@@ -34,7 +34,7 @@ void usage(std::FILE* f) {
                "ps26119 (B200 engines) — LP solver on the GPU\n"
                "usage:\n"
                "  ps26119 --version\n"
-               "  ps26119 info  <file.mps|file.lpm>\n"
+               "  ps26119 info  <file.mps|file.lpm>...\n"
                "  ps26119 convert <file.mps|file.lpm> <out.lpm>\n"
                "  ps26119 solve <file.mps|file.lpm> [options]\n"
                "  ps26119 batch <base> <scenario>... [--out-dir d] [--tol e] [--time-limit s] [--iteration-limit n]\n"
@@ -93,14 +93,12 @@ bool load(const std::string& path, Model& m, ModelInfo& info) {
   return true;
 }
 
-int cmd_info(int argc, char** argv) {
-  if (argc < 1) {
-    usage(stderr);
-    return kExitUsage;
-  }
+// One file's summary. `r` is reused from file to file the way the solve path reuses its
+// presolve result on a thread, so a digest printed here is the one a repeated solve sees.
+int info_one(const char* path, PresolveResult& r) {
   Model m;
   ModelInfo info;
-  if (!load(argv[0], m, info)) return kExitRead;
+  if (!load(path, m, info)) return kExitRead;
   int eq = 0, ranged = 0, free_rows = 0, fixed = 0, boxed = 0, free_cols = 0, ints = 0;
   for (int i = 0; i < m.num_rows; ++i) {
     const double lo = m.row_lower[i], up = m.row_upper[i];
@@ -128,7 +126,7 @@ int cmd_info(int argc, char** argv) {
   }
   // what the safe presolve (R1-R4) would do, and a digest of all its decisions
   if (m.validate().empty()) {
-    const PresolveResult r = presolve(m);
+    presolve_into(m, r);
     const char* what = r.outcome == PresolveResult::Outcome::Reduced      ? "reduced"
                        : r.outcome == PresolveResult::Outcome::Infeasible ? "infeasible"
                                                                            : "unchanged";
@@ -139,6 +137,17 @@ int cmd_info(int argc, char** argv) {
                   r.reduced.nnz());
     std::printf("  presolve digest    %016llx\n", static_cast<unsigned long long>(presolve_digest(r)));
   }
+  return 0;
+}
+
+int cmd_info(int argc, char** argv) {
+  if (argc < 1) {
+    usage(stderr);
+    return kExitUsage;
+  }
+  PresolveResult r;
+  for (int k = 0; k < argc; ++k)
+    if (const int rc = info_one(argv[k], r)) return rc;
   return 0;
 }
 

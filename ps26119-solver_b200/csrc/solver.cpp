@@ -419,7 +419,14 @@ void presolve_into(const Model& M, PresolveResult& r) {  // presolve.cpp:22-156 
   r.message.clear();
   r.removed_rows = r.removed_cols = r.tightened_bounds = 0;
   r.row_map.clear(), r.col_map.clear(), r.singletons.clear();
-  clear_model(r.reduced);
+  // The reduced model is left as the last call built it (its vectors keep their sizes for the
+  // build below) and emptied on every way out that does not build it.
+  struct ClearUnlessReduced {
+    PresolveResult& r;
+    ~ClearUnlessReduced() {
+      if (r.outcome != PresolveResult::Outcome::Reduced) clear_model(r.reduced);
+    }
+  } clear_unless_reduced{r};
   PresolveScratch& S = t_presolve;
   const int m = M.num_rows, n = M.num_cols;
   // A singleton row's one remaining column is recovered as the XOR of the row's live column
@@ -537,54 +544,71 @@ void presolve_into(const Model& M, PresolveResult& r) {  // presolve.cpp:22-156 
     if (row_alive[i]) new_row[i] = static_cast<int>(r.row_map.size()), r.row_map.push_back(i);
   for (int j = 0; j < n; ++j)
     if (col_alive[j]) r.col_map.push_back(j);
+  // Every vector of R is sized here and overwritten in full: it keeps its size from the last
+  // call, so a repeated call writes each element once (no zero fill before the copy).
   R.sense = M.sense;
   R.obj_offset = offset;
   R.num_rows = static_cast<int>(r.row_map.size());
   R.num_cols = static_cast<int>(r.col_map.size());
-  R.col_start.reserve(r.col_map.size() + 1);
-  R.obj.reserve(r.col_map.size());
-  R.col_lower.reserve(r.col_map.size());
-  R.col_upper.reserve(r.col_map.size());
-  R.row_index.reserve(M.nnz());
-  R.value.reserve(M.nnz());
-  R.row_lower.reserve(r.row_map.size());
-  R.row_upper.reserve(r.row_map.size());
-  R.col_start.push_back(0);
+  R.is_integer.clear();
+  const int nk = R.num_cols;
+  size_for_copy(R.obj, r.col_map.size()), size_for_copy(R.col_lower, r.col_map.size());
+  size_for_copy(R.col_upper, r.col_map.size()), size_for_copy(R.col_start, r.col_map.size() + 1);
+  size_for_copy(R.row_lower, r.row_map.size()), size_for_copy(R.row_upper, r.row_map.size());
+  parallel_ranges(nk, [&](long long qb, long long qe) {  // the kept columns' data
+    for (long long q = qb; q < qe; ++q) {
+      const int j = r.col_map[static_cast<std::size_t>(q)];
+      R.obj[q] = M.obj[j], R.col_lower[q] = cl[j], R.col_upper[q] = cu[j];
+    }
+  });
+  parallel_ranges(R.num_rows, [&](long long qb, long long qe) {  // the kept rows' bounds
+    for (long long q = qb; q < qe; ++q) {
+      const int i = r.row_map[static_cast<std::size_t>(q)];
+      R.row_lower[q] = rl[i], R.row_upper[q] = ru[i];
+    }
+  });
+  R.col_start[0] = 0;
   if (r.removed_rows == 0) {
-    // row numbers unchanged: the kept columns are copied as they are, one block per run of kept
-    // columns whose entries are contiguous (removed columns without entries do not break a run)
-    const int nk = static_cast<int>(r.col_map.size());
+    // row numbers unchanged: the kept columns' entries are copied as they are, one block per
+    // run of kept columns whose entries are contiguous (removed columns without entries do not
+    // break a run); the blocks go in one parallel copy once every run's place is known
+    struct Run {
+      int k0, k1;
+      std::size_t at;
+    };
+    std::vector<Run> runs;
+    std::size_t at = 0;
     for (int q = 0; q < nk;) {
       int e = q + 1;
       while (e < nk && M.col_start[r.col_map[e]] == M.col_start[r.col_map[e - 1] + 1]) ++e;
       const int k0 = M.col_start[r.col_map[q]], k1 = M.col_start[r.col_map[e - 1] + 1];
-      const int base = static_cast<int>(R.value.size()) - k0;
-      R.row_index.insert(R.row_index.end(), M.row_index.begin() + k0, M.row_index.begin() + k1);
-      R.value.insert(R.value.end(), M.value.begin() + k0, M.value.begin() + k1);
-      for (int c = q; c < e; ++c) {
-        const int j = r.col_map[c];
-        R.obj.push_back(M.obj[j]);
-        R.col_lower.push_back(cl[j]);
-        R.col_upper.push_back(cu[j]);
-        R.col_start.push_back(M.col_start[j + 1] + base);
-      }
+      const int base = static_cast<int>(at) - k0;
+      runs.push_back({k0, k1, at});
+      for (int c = q; c < e; ++c) R.col_start[c + 1] = M.col_start[r.col_map[c] + 1] + base;
+      at += static_cast<std::size_t>(k1 - k0);
       q = e;
     }
+    size_for_copy(R.row_index, at), size_for_copy(R.value, at);
+    std::vector<CopyJob> jobs;
+    jobs.reserve(2 * runs.size());
+    for (const Run& u : runs) {
+      const std::size_t len = static_cast<std::size_t>(u.k1 - u.k0);
+      jobs.push_back({R.row_index.data() + u.at, M.row_index.data() + u.k0, 4 * len});
+      jobs.push_back({R.value.data() + u.at, M.value.data() + u.k0, 8 * len});
+    }
+    parallel_copy(jobs.data(), jobs.size());
   } else {
-    for (int j : r.col_map) {
-      R.obj.push_back(M.obj[j]);
-      R.col_lower.push_back(cl[j]);
-      R.col_upper.push_back(cu[j]);
+    R.row_index.clear(), R.value.clear();
+    R.row_index.reserve(M.nnz());
+    R.value.reserve(M.nnz());
+    for (int q = 0; q < nk; ++q) {
+      const int j = r.col_map[q];
       for (int p = M.col_start[j]; p < M.col_start[j + 1]; ++p) {
         const int i = M.row_index[p];
         if (new_row[i] >= 0) R.row_index.push_back(new_row[i]), R.value.push_back(M.value[p]);
       }
-      R.col_start.push_back(static_cast<int>(R.value.size()));
+      R.col_start[q + 1] = static_cast<int>(R.value.size());
     }
-  }
-  for (int i : r.row_map) {
-    R.row_lower.push_back(rl[i]);
-    R.row_upper.push_back(ru[i]);
   }
   r.outcome = PresolveResult::Outcome::Reduced;
 }

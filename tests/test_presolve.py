@@ -58,8 +58,33 @@ def infeasible_empty_row():
     return lp.with_data(row_lower=rl, row_upper=ru)
 
 
+def columns_only(seed, m=50, n=40):
+    """Fixed and empty columns only: every row keeps at least three entries in the kept
+    columns, so no row is removed and the reduced matrix is the kept columns copied as they
+    are (the case of large random LPs, whose empty columns are the only reduction)."""
+    rng = np.random.default_rng(seed)
+    A = np.where(rng.random((m, n)) < 0.3, rng.normal(size=(m, n)), 0.0)
+    fixed, empty = [3, 8, n - 7], [5, n - 10, n - 1]
+    A[:, empty] = 0.0
+    kept = [j for j in range(n) if j not in fixed and j not in empty]
+    for i in range(m):
+        for j in kept[i % 7::7][:3]:
+            if A[i, j] == 0.0:
+                A[i, j] = rng.choice([-1.0, 1.0]) * rng.uniform(0.5, 2.0)
+    x0 = rng.uniform(0.5, 4.0, n)
+    ax = A @ x0
+    rl, ru = ax - rng.uniform(0, 1, m), ax + rng.uniform(0, 1, m)
+    cl, cu = np.zeros(n), np.full(n, 6.0)
+    cl[fixed] = cu[fixed] = x0[fixed]
+    c = rng.normal(size=n)
+    c[empty] = [1.0, -1.0, 0.0]
+    return g.from_dense(c, A, rl, ru, cl, cu, offset=-0.5)
+
+
 GENERATED = {
     **{f"planted_{s}": (lambda s=s: planted(s)) for s in range(6)},
+    **{f"columns_only_{s}": (lambda s=s: columns_only(s)) for s in range(2)},
+    "columns_only_large": lambda: columns_only(5, m=400, n=300),
     "infeasible_empty_row": infeasible_empty_row,
     "random_m300": lambda: g.random_lp(300, seed=4),
     "staircase_T3": lambda: g.staircase_lp(3, seed=2),
@@ -122,3 +147,29 @@ def test_presolve_without_host_buffer_reuse(ref, tmp_path):
     r = subprocess.run([CLI, "info", str(path)], capture_output=True, text=True, env=env, timeout=120)
     got = [ln for ln in r.stdout.splitlines() if "presolve digest" in ln][0].split()[-1]
     assert r.returncode == 0 and got == want
+
+
+def test_columns_only_models_remove_no_rows(ref, tmp_path):
+    for name in ("columns_only_0", "columns_only_1", "columns_only_large"):
+        path = tmp_path / f"{name}.mps"
+        write_mps(GENERATED[name](), path)
+        _, (outcome, rows, cols, _) = ref.presolve_file(str(path))
+        assert outcome == 0 and rows == 0 and cols >= 3, (name, outcome, rows, cols)
+
+
+def test_presolve_reuses_its_result_across_models(ref, tmp_path):
+    # One process presolves a sequence of models into one reused result, the way repeated solves
+    # on a thread do: larger and smaller models, reductions with and without removed rows, an
+    # unchanged and an infeasible model in between. Every digest equals the reference's.
+    order = ["columns_only_large", "planted_0", "columns_only_0", "infeasible_empty_row", "columns_only_1",
+             "random_m300", "planted_4", "staircase_T3", "columns_only_large", "planted_0"]
+    paths, want = [], []
+    for k, name in enumerate(order):
+        path = tmp_path / f"{k}_{name}.mps"
+        write_mps(GENERATED[name](), path)
+        paths.append(str(path))
+        want.append(ref.presolve_file(str(path))[0])
+    r = cli("info", *paths)
+    assert r.returncode == 0, r.stdout + r.stderr
+    got = [ln.split()[-1] for ln in r.stdout.splitlines() if "presolve digest" in ln]
+    assert got == want, list(zip(order, got, want))
