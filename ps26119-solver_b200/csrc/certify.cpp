@@ -124,11 +124,13 @@ struct Expansion {
       const double av = sum - bv;
       const double err = (q - av) + (ei - bv);
       q = sum;
-      if (err != 0.0) c[w++] = err;
+      c[w] = err;  // kept only when nonzero; stored either way (no branch on the data)
+      w += err != 0.0;
     }
     n = w;
     if (!std::isfinite(q)) return false;
-    if (q != 0.0) c[n++] = q;
+    c[n] = q;  // n ≤ 64 here: the array has room
+    n += q != 0.0;
     return n <= 64;
   }
 };
