@@ -21,6 +21,9 @@
 //                    on a model file: a digest of every presolve decision, in the serialisation
 //                    the library's `ps26119 info` prints (outcome, counts, maps, fixed values,
 //                    singletons, reduced fingerprint; 8-byte words, FNV-1a).
+//   ref_postsolve_file the reference reader, presolve, then postsolve (src/core/presolve.cpp:158-193)
+//                    of a given reduced (x, y): the original x, y, z and objective.
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -369,6 +372,37 @@ int ref_presolve_file(const char* path, char* out, int cap, long long* counts) {
   word(oc == 0 ? r.reduced.fingerprint() : 0);
   std::snprintf(out, static_cast<std::size_t>(cap), "%016llx", static_cast<unsigned long long>(h));
   counts[0] = oc, counts[1] = r.removed_rows, counts[2] = r.removed_cols, counts[3] = r.tightened_bounds;
+  return 1;
+}
+
+// Reads a model file, presolves it and postsolves the reduced point (red_x: nx values, red_y:
+// ny values; a size that does not match the reduced model means "no point", as in the
+// reference). x and z hold n values, y m values; sizes[0..2] receive the sizes of x, y and z
+// after postsolve (0 for a cleared vector). Returns 1, or 0 when the file does not read or
+// presolve does not reduce the model.
+int ref_postsolve_file(const char* path, const double* red_x, long long nx, const double* red_y, long long ny,
+                       double* x, double* y, double* z, double* objective, long long* sizes) {
+  Model m;
+  const std::string p(path);
+  std::string err;
+  bool ok = false;
+  if (p.size() > 4 && p.compare(p.size() - 4, 4, ".lpm") == 0) ok = io::read_lpm(p, m).ok;
+  else ok = io::read_mps(p, m, err);
+  if (!ok) return 0;
+  const PresolveResult r = presolve(m);
+  if (r.outcome != PresolveResult::Outcome::Reduced) return 0;
+  Solution red;
+  red.status = Status::Optimal;
+  red.x.assign(red_x, red_x + nx);
+  red.y.assign(red_y, red_y + ny);
+  const Solution s = postsolve(m, r, red);
+  std::copy(s.x.begin(), s.x.end(), x);
+  std::copy(s.y.begin(), s.y.end(), y);
+  std::copy(s.z.begin(), s.z.end(), z);
+  *objective = s.objective;
+  sizes[0] = static_cast<long long>(s.x.size());
+  sizes[1] = static_cast<long long>(s.y.size());
+  sizes[2] = static_cast<long long>(s.z.size());
   return 1;
 }
 

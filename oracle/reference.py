@@ -92,6 +92,8 @@ def lib():
                                            ctypes.POINTER(ctypes.c_longlong)]
         L.ref_presolve_file.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int,
                                         ctypes.POINTER(ctypes.c_longlong)]
+        L.ref_postsolve_file.argtypes = [ctypes.c_char_p, _D, ctypes.c_longlong, _D, ctypes.c_longlong, _D, _D, _D,
+                                         _D, ctypes.POINTER(ctypes.c_longlong)]
         L.ref_certificate.argtypes = [ctypes.c_int] + model + [_D, _D, _D]
         L.ps26119_solve_lp.argtypes = None  # the reference's own C API, used by bench.py
         _lib = L
@@ -224,6 +226,22 @@ def presolve_file(path):
     counts = (ctypes.c_longlong * 4)()
     ok = L.ref_presolve_file(os.fsencode(path), buf, 512, counts)
     return (buf.value.decode(), tuple(counts)) if ok else (None, buf.value.decode())
+
+
+def postsolve_file(path, num_rows, num_cols, red_x, red_y):
+    """The reference reader, presolve and postsolve (reference src/core/presolve.cpp:158-193) of
+    the reduced point (red_x, red_y) on a model file with num_rows × num_cols: (x, y, z,
+    objective), each vector empty when postsolve cleared it; None when presolve does not reduce."""
+    L = lib()
+    red_x = np.ascontiguousarray(red_x, dtype=np.float64)
+    red_y = np.ascontiguousarray(red_y, dtype=np.float64)
+    x, y, z = np.zeros(num_cols), np.zeros(num_rows), np.zeros(num_cols)
+    obj = np.zeros(1)
+    sizes = (ctypes.c_longlong * 3)()
+    if not L.ref_postsolve_file(os.fsencode(path), _d(red_x), len(red_x), _d(red_y), len(red_y), _d(x), _d(y), _d(z),
+                                _d(obj), sizes):
+        return None
+    return x[:sizes[0]], y[:sizes[1]], z[:sizes[2]], float(obj[0])
 
 
 def bound(lp, y, use_implied=True):

@@ -384,7 +384,10 @@ struct VectorPool {
 thread_local VectorPool t_vectors;
 }  // namespace
 
-std::vector<double> pooled_vector(std::size_t n) {
+namespace {
+// n elements in the smallest pooled buffer that holds them (a fresh vector when none does);
+// the values are unspecified: the caller overwrites every one
+std::vector<double> pooled_storage(std::size_t n) {
   VectorPool& P = t_vectors;
   long long best = -1;
   for (std::size_t k = 0; k < P.free.size(); ++k)
@@ -396,7 +399,15 @@ std::vector<double> pooled_vector(std::size_t n) {
     P.free.erase(P.free.begin() + best);
     host_keep(P.accounted, P.bytes());
   }
-  v.assign(n, 0.0);
+  size_for_copy(v, n);
+  return v;
+}
+}  // namespace
+
+std::vector<double> pooled_vector(std::size_t n) {
+  std::vector<double> v = pooled_storage(n);
+  parallel_ranges(static_cast<long long>(n), [&](long long b, long long e) { std::fill(v.data() + b, v.data() + e, 0.0); },
+                  1LL << 18);
   return v;
 }
 
@@ -643,12 +654,19 @@ Solution postsolve(const Model& M, const PresolveResult& r, const Solution& red)
   s.y = pooled_vector(static_cast<std::size_t>(m));
   const bool have_x = red.x.size() == r.col_map.size();
   const bool have_y = red.y.size() == r.row_map.size();
-  for (int j = 0; j < n; ++j)
-    if (!std::isnan(r.fixed_value[j])) s.x[j] = r.fixed_value[j];
+  // element-wise writes to distinct entries (the maps are one-to-one), on the host threads
+  parallel_ranges(n, [&](long long jb, long long je) {
+    for (long long j = jb; j < je; ++j)
+      if (!std::isnan(r.fixed_value[j])) s.x[j] = r.fixed_value[j];
+  });
   if (have_x)
-    for (std::size_t c = 0; c < r.col_map.size(); ++c) s.x[r.col_map[c]] = red.x[c];
+    parallel_ranges(static_cast<long long>(r.col_map.size()), [&](long long cb, long long ce) {
+      for (long long c = cb; c < ce; ++c) s.x[r.col_map[c]] = red.x[c];
+    });
   if (have_y)
-    for (std::size_t q = 0; q < r.row_map.size(); ++q) s.y[r.row_map[q]] = red.y[q];
+    parallel_ranges(static_cast<long long>(r.row_map.size()), [&](long long qb, long long qe) {
+      for (long long q = qb; q < qe; ++q) s.y[r.row_map[q]] = red.y[q];
+    });
   for (auto it = r.singletons.rbegin(); it != r.singletons.rend(); ++it) {
     const int j = it->col;
     double z = M.obj[j];
@@ -656,11 +674,13 @@ Solution postsolve(const Model& M, const PresolveResult& r, const Solution& red)
     const double zm = M.sense * z;
     if ((zm > 0 && it->set_lower) || (zm < 0 && it->set_upper)) s.y[it->row] = z / it->a;
   }
-  s.z = pooled_vector(static_cast<std::size_t>(n));
-  std::copy(M.obj.begin(), M.obj.end(), s.z.begin());
+  s.z = pooled_storage(static_cast<std::size_t>(n));
   parallel_ranges(n, [&](long long jb, long long je) {  // each z_j in its own column order
-    for (long long j = jb; j < je; ++j)
-      for (int p = M.col_start[j]; p < M.col_start[j + 1]; ++p) s.z[j] -= M.value[p] * s.y[M.row_index[p]];
+    for (long long j = jb; j < je; ++j) {
+      double z = M.obj[j];
+      for (int p = M.col_start[j]; p < M.col_start[j + 1]; ++p) z -= M.value[p] * s.y[M.row_index[p]];
+      s.z[j] = z;
+    }
   });
   s.objective = M.objective_value(s.x);
   if (!have_x) {

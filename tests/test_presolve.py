@@ -173,3 +173,84 @@ def test_presolve_reuses_its_result_across_models(ref, tmp_path):
     assert r.returncode == 0, r.stdout + r.stderr
     got = [ln.split()[-1] for ln in r.stdout.splitlines() if "presolve digest" in ln]
     assert got == want, list(zip(order, got, want))
+
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+PKG = os.path.join(ROOT, "ps26119-solver_b200")
+
+
+@pytest.fixture(scope="module")
+def postsolve_probe(tmp_path_factory):
+    """tests/native/postsolve_probe.cpp linked with the library's host objects (compiled from
+    the library's sources when the build's objects are absent)."""
+    csrc = os.path.join(PKG, "csrc")
+    units = ("solver.cpp", "certify.cpp", "io.cpp")
+    objs = [os.path.join(PKG, "_build", u + ".o") for u in units]
+    if not all(os.path.exists(o) for o in objs):
+        objs = [os.path.join(csrc, u) for u in units]
+    exe = str(tmp_path_factory.mktemp("probe") / "postsolve_probe")
+    cmd = ["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-I", csrc, "-I", "/usr/local/cuda/include",
+           os.path.join(ROOT, "tests", "native", "postsolve_probe.cpp"), *objs, "-o", exe, "-lpthread"]
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    return exe
+
+
+def _read_probe(path, count):
+    raw = open(path, "rb").read()
+    out, at = [], 0
+    for _ in range(count):
+        sizes = np.frombuffer(raw, dtype=np.int64, count=3, offset=at)
+        at += 24
+        if sizes[0] < 0:
+            out.append(None)
+            continue
+        vecs = []
+        for s in sizes:
+            vecs.append(np.frombuffer(raw, dtype=np.float64, count=int(s), offset=at))
+            at += 8 * int(s)
+        obj = float(np.frombuffer(raw, dtype=np.float64, count=1, offset=at)[0])
+        at += 8
+        out.append((*vecs, obj))
+    assert at == len(raw)
+    return out
+
+
+def _same_bits(a, b):
+    return a.shape == b.shape and np.array_equal(np.asarray(a).view(np.uint64), np.asarray(b).view(np.uint64))
+
+
+def test_postsolve_matches_reference(ref, tmp_path, postsolve_probe):
+    """postsolve (csrc/solver.cpp) against the reference's (src/core/presolve.cpp:158-193) on the
+    same presolved models and seeded reduced points: x, y, z and the objective bit for bit. The
+    points include ones without x or without y (postsolve then clears what depends on them).
+    The jobs run in one process with one reused presolve result, as repeated solves do, and the
+    50,000-row LP runs the threaded passes."""
+    rng = np.random.default_rng(11)
+    models = {name: GENERATED[name]() for name in ("planted_0", "planted_2", "planted_5", "columns_only_0",
+                                                     "columns_only_large", "staircase_T3")}
+    models["random_m50000"] = g.random_lp(50_000, seed=8)
+    args, want, names = [], [], []
+    for k, (name, lp) in enumerate(models.items()):
+        path = str(tmp_path / f"{name}.mps")
+        write_mps(lp, path)
+        _, (outcome, rows, cols, _) = ref.presolve_file(path)
+        assert outcome == 0, name
+        m, n = lp.num_rows - rows, lp.num_cols - cols
+        for variant in ("xy", "x", "y"):
+            rx = rng.normal(size=n) if "x" in variant else np.zeros(0)
+            ry = rng.normal(size=m) * 3 if "y" in variant else np.zeros(0)
+            fx, fy = tmp_path / f"{k}_{variant}_x.bin", tmp_path / f"{k}_{variant}_y.bin"
+            rx.tofile(fx), ry.tofile(fy)
+            args += [path, str(fx), str(fy)]
+            want.append(ref.postsolve_file(path, lp.num_rows, lp.num_cols, rx, ry))
+            names.append((name, variant))
+    out = tmp_path / "out.bin"
+    r = subprocess.run([postsolve_probe, str(out), *args], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    got = _read_probe(out, len(want))
+    for (name, variant), w, o in zip(names, want, got):
+        assert w is not None and o is not None, (name, variant)
+        for q, label in enumerate(("x", "y", "z")):
+            assert _same_bits(o[q], w[q]), (name, variant, label)
+        assert _same_bits(np.array([o[3]]), np.array([w[3]])) or (np.isnan(o[3]) and np.isnan(w[3])), (name, variant)
