@@ -323,15 +323,17 @@ struct PresolveScratch {
   std::vector<int> row_xor, row_cnt, col_cnt, new_row;
   std::vector<double> rl, ru, cl, cu;
   std::vector<char> row_alive, col_alive;
+  std::vector<int> pairs;  // (row, column) of every entry, grouped by row block (row_tags)
   std::size_t accounted = 0;
   std::size_t bytes() const {
-    return 4 * (row_xor.capacity() + row_cnt.capacity() + col_cnt.capacity() + new_row.capacity()) +
+    return 4 * (row_xor.capacity() + row_cnt.capacity() + col_cnt.capacity() + new_row.capacity() +
+                pairs.capacity()) +
            8 * (rl.capacity() + ru.capacity() + cl.capacity() + cu.capacity()) + row_alive.capacity() +
            col_alive.capacity();
   }
   void release() {  // frees the memory (clear() alone keeps the capacity)
     std::vector<int>().swap(row_xor), std::vector<int>().swap(row_cnt), std::vector<int>().swap(col_cnt);
-    std::vector<int>().swap(new_row);
+    std::vector<int>().swap(new_row), std::vector<int>().swap(pairs);
     std::vector<double>().swap(rl), std::vector<double>().swap(ru), std::vector<double>().swap(cl);
     std::vector<double>().swap(cu);
     std::vector<char>().swap(row_alive), std::vector<char>().swap(col_alive);
@@ -339,6 +341,78 @@ struct PresolveScratch {
   ~PresolveScratch() { host_keep(accounted, 0); }
 };
 thread_local PresolveScratch t_presolve;
+
+// Per row: the number of entries and the XOR of their column indices. Both are commutative, so
+// any order of the entries gives the arrays of a sequential pass. With several host threads the
+// entries are first bucketed by block of 2^14 rows (each thread counts, then places, the entries
+// of its own column range), then each block is applied by one thread with plain stores into
+// rows that fit in its cache: atomics on random rows would serialise the cache misses instead.
+void row_tags(const Model& M, std::vector<int>& row_xor, std::vector<int>& row_cnt, std::vector<int>& pairs) {
+  const int m = M.num_rows, n = M.num_cols;
+  row_xor.assign(static_cast<std::size_t>(m), 0);
+  row_cnt.assign(static_cast<std::size_t>(m), 0);
+  const long long nnz = static_cast<long long>(M.nnz());
+  const int T = nnz < (1LL << 18) ? 1 : static_cast<int>(std::min(32u, std::max(1u, std::thread::hardware_concurrency())));
+  if (T == 1) {
+    for (int j = 0; j < n; ++j)
+      for (int k = M.col_start[j]; k < M.col_start[j + 1]; ++k) row_xor[M.row_index[k]] ^= j, ++row_cnt[M.row_index[k]];
+    return;
+  }
+  constexpr int kShift = 14;
+  const int nb = (m >> kShift) + 1;
+  std::vector<long long> at(static_cast<std::size_t>(T) * nb, 0);  // chunk c's next slot in block b: at[c·nb + b]
+  std::vector<long long> start(static_cast<std::size_t>(nb) + 1, 0);
+  auto cols = [&](long long c, int& jb, int& je) {
+    jb = static_cast<int>(static_cast<long long>(n) * c / T), je = static_cast<int>(static_cast<long long>(n) * (c + 1) / T);
+  };
+  parallel_ranges(
+      T,
+      [&](long long cb, long long ce) {
+        for (long long c = cb; c < ce; ++c) {
+          int jb, je;
+          cols(c, jb, je);
+          long long* h = &at[static_cast<std::size_t>(c) * nb];
+          for (int k = M.col_start[jb]; k < M.col_start[je]; ++k) ++h[M.row_index[k] >> kShift];
+        }
+      },
+      1);
+  long long pos = 0;  // blocks in order, and inside a block the chunks in order
+  for (int b = 0; b < nb; ++b) {
+    start[b] = pos;
+    for (int c = 0; c < T; ++c) {
+      const long long cnt = at[static_cast<std::size_t>(c) * nb + b];
+      at[static_cast<std::size_t>(c) * nb + b] = pos;
+      pos += cnt;
+    }
+  }
+  start[nb] = pos;
+  size_for_copy(pairs, static_cast<std::size_t>(2 * nnz));
+  parallel_ranges(
+      T,
+      [&](long long cb, long long ce) {
+        for (long long c = cb; c < ce; ++c) {
+          int jb, je;
+          cols(c, jb, je);
+          long long* h = &at[static_cast<std::size_t>(c) * nb];
+          for (int j = jb; j < je; ++j)
+            for (int k = M.col_start[j]; k < M.col_start[j + 1]; ++k) {
+              const int i = M.row_index[k];
+              const long long q = h[i >> kShift]++;
+              pairs[2 * q] = i, pairs[2 * q + 1] = j;
+            }
+        }
+      },
+      1);
+  parallel_ranges(
+      nb,
+      [&](long long bb, long long be) {
+        for (long long q = start[bb]; q < start[be]; ++q) {
+          const int i = pairs[2 * q];
+          row_xor[i] ^= pairs[2 * q + 1], ++row_cnt[i];
+        }
+      },
+      1);
+}
 
 void clear_model(Model& R) {  // empties every vector, keeping its capacity
   R.num_rows = R.num_cols = 0, R.sense = 1, R.obj_offset = 0.0;
@@ -444,22 +518,9 @@ void presolve_into(const Model& M, PresolveResult& r) {  // presolve.cpp:22-156 
   // indices (kept up to date as columns are removed), and its coefficient by a scan of that
   // column: the same (j, a) the reference finds by walking the row (presolve.cpp:60-66), with
   // no row-wise copy of A.
-  // One pass over the entries, threads over column ranges: XOR and count are commutative, so
-  // relaxed integer atomics give the arrays of a sequential pass.
   std::vector<int>& row_xor = S.row_xor;
   std::vector<int>& row_cnt = S.row_cnt;
-  row_xor.assign(static_cast<std::size_t>(m), 0);
-  row_cnt.assign(static_cast<std::size_t>(m), 0);
-  parallel_ranges(n, [&](long long jb, long long je) {
-    for (long long jj = jb; jj < je; ++jj) {
-      const int j = static_cast<int>(jj);
-      for (int k = M.col_start[j]; k < M.col_start[j + 1]; ++k) {
-        const int i = M.row_index[k];
-        __atomic_fetch_xor(&row_xor[i], j, __ATOMIC_RELAXED);
-        __atomic_fetch_add(&row_cnt[i], 1, __ATOMIC_RELAXED);
-      }
-    }
-  });
+  row_tags(M, row_xor, row_cnt, S.pairs);
   std::vector<double>&rl = S.rl, &ru = S.ru, &cl = S.cl, &cu = S.cu;
   rl.assign(M.row_lower.begin(), M.row_lower.end()), ru.assign(M.row_upper.begin(), M.row_upper.end());
   cl.assign(M.col_lower.begin(), M.col_lower.end()), cu.assign(M.col_upper.begin(), M.col_upper.end());

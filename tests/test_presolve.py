@@ -81,10 +81,43 @@ def columns_only(seed, m=50, n=40):
     return g.from_dense(c, A, rl, ru, cl, cu, offset=-0.5)
 
 
+def planted_sparse(seed, m=60_000):
+    """A random sparse LP large enough for the threaded presolve passes (360,000 entries), with
+    empty rows, singleton rows (equalities among them, which fix their column and start chains)
+    and fixed columns planted in it."""
+    base = g.random_lp(m, seed=seed)
+    rng = np.random.default_rng(seed + 100)
+    n = base.num_cols
+    cols = np.repeat(np.arange(n), np.diff(base.col_start))
+    rows, vals = base.row_index.astype(np.int64), base.value.copy()
+    empty = rng.choice(m, 60, replace=False)
+    single = rng.choice(np.setdiff1d(np.arange(m), empty), 300, replace=False)
+    keep = ~np.isin(rows, empty)
+    first = {}  # a singleton row keeps its entry of smallest column
+    for k in np.nonzero(np.isin(rows, single))[0]:
+        first.setdefault(int(rows[k]), k)
+    keep &= ~np.isin(rows, single) | np.isin(np.arange(len(rows)), list(first.values()))
+    rows, cols, vals = rows[keep], cols[keep], vals[keep]
+    x0 = base.meta["x0"]
+    b = np.bincount(rows, weights=vals * x0[cols], minlength=m)
+    rl, ru = b.copy(), b.copy()
+    rl[empty], ru[empty] = -1.0, 2.0
+    loose = single[:150]  # half the singletons are inequalities that tighten one bound
+    rl[loose] = b[loose] - np.abs(b[loose]) * 0.5 - 0.1
+    ru[loose] = np.inf
+    cl, cu = base.col_lower.copy(), base.col_upper.copy()
+    fixed = rng.choice(n, 100, replace=False)
+    cl[fixed] = cu[fixed] = x0[fixed]
+    cs, ri, v = g.csc_from_triplets(m, n, rows, cols, vals)
+    return base.with_data(row_lower=rl, row_upper=ru, col_lower=cl, col_upper=cu, col_start=cs, row_index=ri,
+                          value=v, name="planted-sparse")
+
+
 GENERATED = {
     **{f"planted_{s}": (lambda s=s: planted(s)) for s in range(6)},
     **{f"columns_only_{s}": (lambda s=s: columns_only(s)) for s in range(2)},
     "columns_only_large": lambda: columns_only(5, m=400, n=300),
+    "planted_sparse": lambda: planted_sparse(3),
     "infeasible_empty_row": infeasible_empty_row,
     "random_m300": lambda: g.random_lp(300, seed=4),
     "staircase_T3": lambda: g.staircase_lp(3, seed=2),
@@ -225,11 +258,12 @@ def test_postsolve_matches_reference(ref, tmp_path, postsolve_probe):
     same presolved models and seeded reduced points: x, y, z and the objective bit for bit. The
     points include ones without x or without y (postsolve then clears what depends on them).
     The jobs run in one process with one reused presolve result, as repeated solves do, and the
-    50,000-row LP runs the threaded passes."""
+    two large LPs run the threaded passes."""
     rng = np.random.default_rng(11)
     models = {name: GENERATED[name]() for name in ("planted_0", "planted_2", "planted_5", "columns_only_0",
                                                      "columns_only_large", "staircase_T3")}
     models["random_m50000"] = g.random_lp(50_000, seed=8)
+    models["planted_sparse"] = GENERATED["planted_sparse"]()
     args, want, names = [], [], []
     for k, (name, lp) in enumerate(models.items()):
         path = str(tmp_path / f"{name}.mps")
