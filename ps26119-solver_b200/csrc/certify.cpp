@@ -280,11 +280,14 @@ SafeBound certified_dual_bound(const Model& M, const std::vector<double>& y_in, 
     }
   } keep;
   std::vector<double>& y = t_certify.y;
-  y.assign(y_in.begin(), y_in.end());
-  for (int i = 0; i < M.num_rows; ++i) {
-    const double ym = M.sense * y[i];
-    if ((ym > 0 && !std::isfinite(M.row_lower[i])) || (ym < 0 && !std::isfinite(M.row_upper[i]))) y[i] = 0.0;
-  }
+  size_for_copy(y, y_in.size());
+  parallel_ranges(M.num_rows, [&](long long ib, long long ie) {  // element-wise, on the host threads
+    for (long long i = ib; i < ie; ++i) {
+      const double ym = M.sense * y_in[i];
+      const bool clear = (ym > 0 && !std::isfinite(M.row_lower[i])) || (ym < 0 && !std::isfinite(M.row_upper[i]));
+      y[i] = clear ? 0.0 : y_in[i];
+    }
+  });
   SafeBound r = bound_with(M, y, M.col_lower, M.col_upper);
   if (use_implied_bounds && r.unbounded_col_terms > 0 && r.unbounded_row_terms == 0) {
     const ImpliedBounds ib = implied_bounds(M);
