@@ -522,14 +522,22 @@ void presolve_into(const Model& M, PresolveResult& r) {  // presolve.cpp:22-156 
   std::vector<int>& row_cnt = S.row_cnt;
   row_tags(M, row_xor, row_cnt, S.pairs);
   std::vector<double>&rl = S.rl, &ru = S.ru, &cl = S.cl, &cu = S.cu;
-  rl.assign(M.row_lower.begin(), M.row_lower.end()), ru.assign(M.row_upper.begin(), M.row_upper.end());
-  cl.assign(M.col_lower.begin(), M.col_lower.end()), cu.assign(M.col_upper.begin(), M.col_upper.end());
+  size_for_copy(rl, M.row_lower.size()), size_for_copy(ru, M.row_upper.size());
+  size_for_copy(cl, M.col_lower.size()), size_for_copy(cu, M.col_upper.size());
+  const CopyJob bounds[] = {{rl.data(), M.row_lower.data(), 8 * rl.size()},
+                            {ru.data(), M.row_upper.data(), 8 * ru.size()},
+                            {cl.data(), M.col_lower.data(), 8 * cl.size()},
+                            {cu.data(), M.col_upper.data(), 8 * cu.size()}};
+  parallel_copy(bounds, 4);
   std::vector<char>&row_alive = S.row_alive, &col_alive = S.col_alive;
-  row_alive.assign(static_cast<std::size_t>(m), 1), col_alive.assign(static_cast<std::size_t>(n), 1);
+  row_alive.assign(static_cast<std::size_t>(m), 1);
   std::vector<int>& col_cnt = S.col_cnt;
-  col_cnt.resize(static_cast<std::size_t>(n));
-  for (int j = 0; j < n; ++j) col_cnt[j] = M.col_start[j + 1] - M.col_start[j];
-  r.fixed_value.assign(n, kNaN);
+  size_for_copy(col_alive, static_cast<std::size_t>(n)), size_for_copy(col_cnt, static_cast<std::size_t>(n));
+  size_for_copy(r.fixed_value, static_cast<std::size_t>(n));
+  parallel_ranges(n, [&](long long jb, long long je) {
+    for (long long j = jb; j < je; ++j)
+      col_alive[j] = 1, col_cnt[j] = M.col_start[j + 1] - M.col_start[j], r.fixed_value[j] = kNaN;
+  });
   double offset = M.obj_offset;
   auto infeasible = [&](const std::string& why) {
     r.outcome = PresolveResult::Outcome::Infeasible;
