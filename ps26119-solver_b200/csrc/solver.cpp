@@ -324,16 +324,17 @@ struct PresolveScratch {
   std::vector<double> rl, ru, cl, cu;
   std::vector<char> row_alive, col_alive;
   std::vector<int> pairs;  // (row, column) of every entry, grouped by row block (row_tags)
+  std::vector<int> cand;   // the rows or columns a presolve loop acts on
   std::size_t accounted = 0;
   std::size_t bytes() const {
     return 4 * (row_xor.capacity() + row_cnt.capacity() + col_cnt.capacity() + new_row.capacity() +
-                pairs.capacity()) +
+                pairs.capacity() + cand.capacity()) +
            8 * (rl.capacity() + ru.capacity() + cl.capacity() + cu.capacity()) + row_alive.capacity() +
            col_alive.capacity();
   }
   void release() {  // frees the memory (clear() alone keeps the capacity)
     std::vector<int>().swap(row_xor), std::vector<int>().swap(row_cnt), std::vector<int>().swap(col_cnt);
-    std::vector<int>().swap(new_row), std::vector<int>().swap(pairs);
+    std::vector<int>().swap(new_row), std::vector<int>().swap(pairs), std::vector<int>().swap(cand);
     std::vector<double>().swap(rl), std::vector<double>().swap(ru), std::vector<double>().swap(cl);
     std::vector<double>().swap(cu);
     std::vector<char>().swap(row_alive), std::vector<char>().swap(col_alive);
@@ -341,6 +342,32 @@ struct PresolveScratch {
   ~PresolveScratch() { host_keep(accounted, 0); }
 };
 thread_local PresolveScratch t_presolve;
+
+// The indices i in [0, count) with pred(i), in increasing order, into `out`; pred is evaluated
+// on the host threads (it must only read).
+template <class Pred>
+void select_in_order(int count, Pred pred, std::vector<int>& out) {
+  out.clear();
+  const int T = count < 65536 ? 1 : static_cast<int>(std::min(32u, std::max(1u, std::thread::hardware_concurrency())));
+  if (T == 1) {
+    for (int i = 0; i < count; ++i)
+      if (pred(i)) out.push_back(i);
+    return;
+  }
+  std::vector<std::vector<int>> part(static_cast<std::size_t>(T));
+  parallel_ranges(
+      T,
+      [&](long long cb, long long ce) {
+        for (long long c = cb; c < ce; ++c) {
+          const int ib = static_cast<int>(static_cast<long long>(count) * c / T);
+          const int ie = static_cast<int>(static_cast<long long>(count) * (c + 1) / T);
+          for (int i = ib; i < ie; ++i)
+            if (pred(i)) part[static_cast<std::size_t>(c)].push_back(i);
+        }
+      },
+      1);
+  for (const auto& p : part) out.insert(out.end(), p.begin(), p.end());
+}
 
 // Per row: the number of entries and the XOR of their column indices. Both are commutative, so
 // any order of the entries gives the arrays of a sequential pass. With several host threads the
@@ -550,10 +577,16 @@ void presolve_into(const Model& M, PresolveResult& r) {  // presolve.cpp:22-156 
       if (!host_keep(s.accounted, s.bytes())) s.release();
     }
   } keep{S};
+  // Within the row loop of a pass no row's count or liveness changes but the row's own, and
+  // within the column loop no column's bounds, count or liveness changes but the column's own.
+  // So each loop's candidates are known when it starts: they are found on the host threads and
+  // then processed one by one in index order, the order of a full sequential scan.
+  std::vector<int>& cand = S.cand;
   bool changed = true;
   while (changed) {
     changed = false;
-    for (int i = 0; i < m; ++i) {  // rows: empty (R1) and singleton (R4)
+    select_in_order(m, [&](int i) { return row_alive[i] && row_cnt[i] <= 1; }, cand);
+    for (const int i : cand) {  // rows: empty (R1) and singleton (R4)
       if (!row_alive[i]) continue;
       if (row_cnt[i] == 0) {
         if (!within(0.0, rl[i], ru[i])) { infeasible("empty row " + std::to_string(i) + " excludes 0"); return; }
@@ -585,7 +618,8 @@ void presolve_into(const Model& M, PresolveResult& r) {  // presolve.cpp:22-156 
         changed = true;
       }
     }
-    for (int j = 0; j < n; ++j) {  // columns: fixed (R2) and empty (R3)
+    select_in_order(n, [&](int j) { return col_alive[j] && (cl[j] == cu[j] || col_cnt[j] == 0); }, cand);
+    for (const int j : cand) {  // columns: fixed (R2) and empty (R3)
       if (!col_alive[j]) continue;
       double v;
       if (cl[j] == cu[j]) {

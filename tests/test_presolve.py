@@ -81,10 +81,10 @@ def columns_only(seed, m=50, n=40):
     return g.from_dense(c, A, rl, ru, cl, cu, offset=-0.5)
 
 
-def planted_sparse(seed, m=60_000):
-    """A random sparse LP large enough for the threaded presolve passes (360,000 entries), with
-    empty rows, singleton rows (equalities among them, which fix their column and start chains)
-    and fixed columns planted in it."""
+def planted_sparse(seed, m=70_000):
+    """A random sparse LP large enough for the threaded presolve passes (about 420,000 entries),
+    with empty rows, singleton rows (equalities among them, which fix their column and start
+    chains) and fixed columns planted in it."""
     base = g.random_lp(m, seed=seed)
     rng = np.random.default_rng(seed + 100)
     n = base.num_cols
