@@ -13,7 +13,8 @@
 //   ref_backend_*    pdhg::make_cpu_backend() ops (src/pdhg/cpu_backend.cpp:31-215), the
 //                    op-by-op comparison that tests/unit/test_gpu.cpp:33-95 performs.
 //   ref_check        core::check_solution (src/core/solution_checker.cpp:61) and
-//                    certified_dual_bound (src/core/safe_bound.cpp:178).
+//                    certified_dual_bound (src/core/safe_bound.cpp:178); ref_check_file the
+//                    same on a model file read by the reference's readers.
 //   ref_bound        certified_dual_bound with the implied-bounds switch and its term counts.
 //   ref_certificate  check_infeasibility_certificate / check_unboundedness_certificate
 //                    (src/core/certificates.cpp:14, 88).
@@ -299,6 +300,28 @@ void ref_check(int m, int n, int sense, double offset, const double* c, const do
   out[4] = r.primal_objective;
   out[5] = r.dual_objective;
   out[6] = certified_dual_bound(M, yv, true).bound;
+}
+
+// ref_check on the model read from a file by the reference's readers (x: n values, y: m
+// values of that model). Returns 1, or 0 when the file does not read.
+int ref_check_file(const char* path, const double* x, const double* y, double* out) {
+  Model M;
+  const std::string p(path);
+  std::string err;
+  bool ok = false;
+  if (p.size() > 4 && p.compare(p.size() - 4, 4, ".lpm") == 0) ok = io::read_lpm(p, M).ok;
+  else ok = io::read_mps(p, M, err);
+  if (!ok) return 0;
+  const std::vector<double> xv(x, x + M.num_cols), yv(y, y + M.num_rows);
+  const CheckReport r = check_solution(M, xv, yv);
+  out[0] = r.passed() ? 1.0 : 0.0;
+  out[1] = r.max_primal_violation;
+  out[2] = r.max_dual_violation;
+  out[3] = r.relative_gap;
+  out[4] = r.primal_objective;
+  out[5] = r.dual_objective;
+  out[6] = certified_dual_bound(M, yv, true).bound;
+  return 1;
 }
 
 // The reference's readers: fingerprint of the model read from `path` (.lpm or .mps), dims[3] =

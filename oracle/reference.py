@@ -92,6 +92,7 @@ def lib():
                                            ctypes.POINTER(ctypes.c_longlong)]
         L.ref_presolve_file.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int,
                                         ctypes.POINTER(ctypes.c_longlong)]
+        L.ref_check_file.argtypes = [ctypes.c_char_p, _D, _D, _D]
         L.ref_postsolve_file.argtypes = [ctypes.c_char_p, _D, ctypes.c_longlong, _D, ctypes.c_longlong, _D, _D, _D,
                                          _D, ctypes.POINTER(ctypes.c_longlong)]
         L.ref_certificate.argtypes = [ctypes.c_int] + model + [_D, _D, _D]
@@ -205,6 +206,17 @@ def check(lp, x, y):
     del keep
     return {"passed": bool(out[0]), "primal": out[1], "dual": out[2], "gap": out[3], "primal_objective": out[4],
             "dual_objective": out[5], "certified_bound": out[6]}
+
+
+def check_file(path, x, y):
+    """check() on the model read from a file by the reference's readers: the 7 values
+    (passed, primal, dual, gap, primal objective, dual objective, certified bound) as an array,
+    or None when the file does not read."""
+    L = lib()
+    out = np.zeros(7)
+    ok = L.ref_check_file(os.fsencode(path), _d(np.ascontiguousarray(x, dtype=np.float64)),
+                          _d(np.ascontiguousarray(y, dtype=np.float64)), _d(out))
+    return out if ok else None
 
 
 def read_fingerprint(path):

@@ -7,6 +7,7 @@
 #include "parallel.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -128,10 +129,108 @@ double Model::objective_value(const std::vector<double>& x) const {  // model.cp
   return v;
 }
 
+namespace {
+// Host threads for an O(nnz) pass over a model with `nnz` entries (one below 2^18 entries).
+int pass_threads(long long nnz) {
+  return nnz < (1LL << 18) ? 1 : static_cast<int>(std::min(32u, std::max(1u, std::thread::hardware_concurrency())));
+}
+
+// Groups the entries of the column-major matrix by block of 2^kRowShift rows, for passes that
+// update rows without atomics. Chunk c (one per thread) is the column range [n·c/T, n·(c+1)/T).
+// Every entry gets a slot; the slots of block b are [start[b], start[b+1]), and inside a block
+// chunk 0's entries come first, then chunk 1's, and so on, each chunk's in column order. So the
+// entries of any one row are in increasing column order, the order of a sequential column-major
+// pass. place(q, i, j, k) is called once for entry k (row i, column j) with its slot q, on the
+// thread of the entry's chunk.
+constexpr int kRowShift = 14;  // 16,384 rows: a block's rows fit in one core's cache
+template <class Place>
+void bucket_rows(const Model& M, int T, std::vector<long long>& start, Place place) {
+  const int m = M.num_rows, n = M.num_cols;
+  const int nb = (m >> kRowShift) + 1;
+  std::vector<long long> at(static_cast<std::size_t>(T) * nb, 0);  // chunk c's next slot in block b: at[c·nb + b]
+  auto cols = [&](long long c, int& jb, int& je) {
+    jb = static_cast<int>(static_cast<long long>(n) * c / T), je = static_cast<int>(static_cast<long long>(n) * (c + 1) / T);
+  };
+  parallel_ranges(
+      T,
+      [&](long long cb, long long ce) {
+        for (long long c = cb; c < ce; ++c) {
+          int jb, je;
+          cols(c, jb, je);
+          long long* h = &at[static_cast<std::size_t>(c) * nb];
+          for (int k = M.col_start[jb]; k < M.col_start[je]; ++k) ++h[M.row_index[k] >> kRowShift];
+        }
+      },
+      1);
+  start.assign(static_cast<std::size_t>(nb) + 1, 0);
+  long long pos = 0;  // blocks in order, and inside a block the chunks in order
+  for (int b = 0; b < nb; ++b) {
+    start[b] = pos;
+    for (int c = 0; c < T; ++c) {
+      const long long cnt = at[static_cast<std::size_t>(c) * nb + b];
+      at[static_cast<std::size_t>(c) * nb + b] = pos;
+      pos += cnt;
+    }
+  }
+  start[nb] = pos;
+  parallel_ranges(
+      T,
+      [&](long long cb, long long ce) {
+        for (long long c = cb; c < ce; ++c) {
+          int jb, je;
+          cols(c, jb, je);
+          long long* h = &at[static_cast<std::size_t>(c) * nb];
+          for (int j = jb; j < je; ++j)
+            for (int k = M.col_start[j]; k < M.col_start[j + 1]; ++k) {
+              const int i = M.row_index[k];
+              place(h[i >> kRowShift]++, i, j, k);
+            }
+        }
+      },
+      1);
+}
+
+// The bucketed entries of row_activity (row, product), kept per thread between calls within the
+// host reuse limit.
+struct ActivityScratch {
+  std::vector<int> row;
+  std::vector<double> prod;
+  std::size_t accounted = 0;
+  ~ActivityScratch() { host_keep(accounted, 0); }
+};
+thread_local ActivityScratch t_activity;
+}  // namespace
+
 std::vector<double> Model::row_activity(const std::vector<double>& x) const {  // model.cpp:175-180
-  std::vector<double> ax(num_rows, 0.0);
-  for (int j = 0; j < num_cols; ++j)
-    for (int k = col_start[j]; k < col_start[j + 1]; ++k) ax[row_index[k]] += value[k] * x[j];
+  std::vector<double> ax = pooled_vector(static_cast<std::size_t>(num_rows));  // zeros
+  const int T = pass_threads(static_cast<long long>(nnz()));
+  if (T == 1) {
+    for (int j = 0; j < num_cols; ++j)
+      for (int k = col_start[j]; k < col_start[j + 1]; ++k) ax[row_index[k]] += value[k] * x[j];
+    return ax;
+  }
+  // Each product is formed as in the sequential pass, and each row adds its products in
+  // increasing column order (bucket_rows), so every ax[i] has the sequential pass's bits.
+  ActivityScratch& S = t_activity;
+  struct Keep {
+    ActivityScratch& s;
+    ~Keep() {
+      if (!host_keep(s.accounted, 4 * s.row.capacity() + 8 * s.prod.capacity()))
+        std::vector<int>().swap(s.row), std::vector<double>().swap(s.prod);
+    }
+  } keep{S};
+  size_for_copy(S.row, nnz()), size_for_copy(S.prod, nnz());
+  std::vector<long long> start;
+  bucket_rows(*this, T, start, [&](long long q, int i, int j, int k) {
+    S.row[q] = i;
+    S.prod[q] = value[k] * x[j];
+  });
+  parallel_ranges(
+      static_cast<long long>(start.size()) - 1,
+      [&](long long bb, long long be) {
+        for (long long q = start[bb]; q < start[be]; ++q) ax[S.row[q]] += S.prod[q];
+      },
+      1);
   return ax;
 }
 
@@ -228,6 +327,8 @@ HostModelView Model::view() const {
 
 // ============================================================ check (solution_checker.cpp)
 namespace {
+std::vector<double> pooled_storage(std::size_t n);  // defined with the vector pool below
+
 struct DualTerm {
   double violation, contribution, complementarity;
 };
@@ -260,37 +361,67 @@ CheckReport check_solution(const Model& lp, const std::vector<double>& x, const 
     return rep;
   };
   if (static_cast<int>(x.size()) != n || static_cast<int>(row_dual.size()) != m) return reject();
-  for (double v : x)
-    if (!std::isfinite(v)) return reject();
-  for (double v : row_dual)
-    if (!std::isfinite(v)) return reject();
-  const std::vector<double> ax = lp.row_activity(x);
-  for (int i = 0; i < m; ++i)
-    rep.max_primal_violation = std::max(rep.max_primal_violation, bound_violation(ax[i], lp.row_lower[i], lp.row_upper[i]));
-  for (int j = 0; j < n; ++j)
-    rep.max_primal_violation = std::max(rep.max_primal_violation, bound_violation(x[j], lp.col_lower[j], lp.col_upper[j]));
-  std::vector<double> y(m);
-  for (int i = 0; i < m; ++i) y[i] = sense * row_dual[i];
-  std::vector<double> aty(n, 0.0);
-  for (int j = 0; j < n; ++j)
-    for (int k = lp.col_start[j]; k < lp.col_start[j + 1]; ++k) aty[j] += lp.value[k] * y[lp.row_index[k]];
-  double dual_obj_min = 0.0, primal_obj_min = 0.0, c_scale = 1.0;
-  for (int j = 0; j < n; ++j) c_scale = std::max(c_scale, std::fabs(lp.obj[j]));
-  for (int i = 0; i < m; ++i) {
-    const DualTerm t = evaluate_multiplier(y[i], lp.row_lower[i], lp.row_upper[i], ax[i]);
-    rep.max_dual_violation = std::max(rep.max_dual_violation, t.violation / c_scale);
-    rep.max_complementarity = std::max(rep.max_complementarity, t.complementarity);
-    dual_obj_min += t.contribution;
-  }
-  for (int j = 0; j < n; ++j) {
-    const double c = sense * lp.obj[j];
-    const double d = c - aty[j];
-    const DualTerm t = evaluate_multiplier(d, lp.col_lower[j], lp.col_upper[j], x[j]);
-    rep.max_dual_violation = std::max(rep.max_dual_violation, t.violation / c_scale);
-    rep.max_complementarity = std::max(rep.max_complementarity, t.complementarity);
-    dual_obj_min += t.contribution;
-    primal_obj_min += c * x[j];
-  }
+  // Element-wise work runs on the host threads: each element's terms are those of the
+  // sequential pass, maxima combine exactly in any order, and the two sums are taken afterwards
+  // in the sequential pass's order (rows, then columns).
+  std::atomic<bool> finite{true};
+  parallel_ranges(std::max<long long>(n, m), [&](long long b, long long e) {
+    bool ok = true;
+    for (long long k = b; k < e; ++k)
+      ok = ok && (k >= n || std::isfinite(x[k])) && (k >= m || std::isfinite(row_dual[k]));
+    if (!ok) finite.store(false, std::memory_order_relaxed);
+  });
+  if (!finite.load()) return reject();
+  std::mutex mu;
+  auto fold = [&mu](double& into, double v) {  // with mu held
+    into = std::max(into, v);
+  };
+  double c_scale = 1.0;
+  parallel_ranges(n, [&](long long jb, long long je) {  // column bound violations and max |c_j|
+    double pv = 0.0, cs = 1.0;
+    for (long long j = jb; j < je; ++j) {
+      pv = std::max(pv, bound_violation(x[j], lp.col_lower[j], lp.col_upper[j]));
+      cs = std::max(cs, std::fabs(lp.obj[j]));
+    }
+    std::lock_guard<std::mutex> lock(mu);
+    fold(rep.max_primal_violation, pv), fold(c_scale, cs);
+  });
+  std::vector<double> ax = lp.row_activity(x);
+  std::vector<double> row_term = pooled_storage(static_cast<std::size_t>(m));
+  parallel_ranges(m, [&](long long ib, long long ie) {  // row violations and multiplier terms
+    double pv = 0.0, dv = 0.0, cp = 0.0;
+    for (long long i = ib; i < ie; ++i) {
+      pv = std::max(pv, bound_violation(ax[i], lp.row_lower[i], lp.row_upper[i]));
+      const DualTerm t = evaluate_multiplier(sense * row_dual[i], lp.row_lower[i], lp.row_upper[i], ax[i]);
+      dv = std::max(dv, t.violation / c_scale);
+      cp = std::max(cp, t.complementarity);
+      row_term[i] = t.contribution;
+    }
+    std::lock_guard<std::mutex> lock(mu);
+    fold(rep.max_primal_violation, pv), fold(rep.max_dual_violation, dv), fold(rep.max_complementarity, cp);
+  });
+  std::vector<double> col_term = pooled_storage(static_cast<std::size_t>(n));
+  std::vector<double> obj_term = pooled_storage(static_cast<std::size_t>(n));
+  parallel_ranges(n, [&](long long jb, long long je) {  // reduced costs and their terms
+    double dv = 0.0, cp = 0.0;
+    for (long long j = jb; j < je; ++j) {
+      double aty = 0.0;  // (Aᵀ·sense·y)_j in the column's entry order
+      for (int k = lp.col_start[j]; k < lp.col_start[j + 1]; ++k) aty += lp.value[k] * (sense * row_dual[lp.row_index[k]]);
+      const double c = sense * lp.obj[j];
+      const DualTerm t = evaluate_multiplier(c - aty, lp.col_lower[j], lp.col_upper[j], x[j]);
+      dv = std::max(dv, t.violation / c_scale);
+      cp = std::max(cp, t.complementarity);
+      col_term[j] = t.contribution;
+      obj_term[j] = c * x[j];
+    }
+    std::lock_guard<std::mutex> lock(mu);
+    fold(rep.max_dual_violation, dv), fold(rep.max_complementarity, cp);
+  });
+  double dual_obj_min = 0.0, primal_obj_min = 0.0;
+  for (int i = 0; i < m; ++i) dual_obj_min += row_term[i];
+  for (int j = 0; j < n; ++j) dual_obj_min += col_term[j], primal_obj_min += obj_term[j];
+  pool_vector(std::move(ax)), pool_vector(std::move(row_term)), pool_vector(std::move(col_term));
+  pool_vector(std::move(obj_term));
   rep.primal_objective = sense * primal_obj_min + lp.obj_offset;
   rep.dual_objective = sense * dual_obj_min + lp.obj_offset;
   rep.relative_gap = std::fabs(rep.primal_objective - rep.dual_objective) /
@@ -371,67 +502,24 @@ void select_in_order(int count, Pred pred, std::vector<int>& out) {
 
 // Per row: the number of entries and the XOR of their column indices. Both are commutative, so
 // any order of the entries gives the arrays of a sequential pass. With several host threads the
-// entries are first bucketed by block of 2^14 rows (each thread counts, then places, the entries
-// of its own column range), then each block is applied by one thread with plain stores into
-// rows that fit in its cache: atomics on random rows would serialise the cache misses instead.
+// entries are bucketed by row block (bucket_rows), then each block is applied by one thread
+// with plain stores into rows that fit in its cache: atomics on random rows would serialise the
+// cache misses instead.
 void row_tags(const Model& M, std::vector<int>& row_xor, std::vector<int>& row_cnt, std::vector<int>& pairs) {
   const int m = M.num_rows, n = M.num_cols;
   row_xor.assign(static_cast<std::size_t>(m), 0);
   row_cnt.assign(static_cast<std::size_t>(m), 0);
-  const long long nnz = static_cast<long long>(M.nnz());
-  const int T = nnz < (1LL << 18) ? 1 : static_cast<int>(std::min(32u, std::max(1u, std::thread::hardware_concurrency())));
+  const int T = pass_threads(static_cast<long long>(M.nnz()));
   if (T == 1) {
     for (int j = 0; j < n; ++j)
       for (int k = M.col_start[j]; k < M.col_start[j + 1]; ++k) row_xor[M.row_index[k]] ^= j, ++row_cnt[M.row_index[k]];
     return;
   }
-  constexpr int kShift = 14;
-  const int nb = (m >> kShift) + 1;
-  std::vector<long long> at(static_cast<std::size_t>(T) * nb, 0);  // chunk c's next slot in block b: at[c·nb + b]
-  std::vector<long long> start(static_cast<std::size_t>(nb) + 1, 0);
-  auto cols = [&](long long c, int& jb, int& je) {
-    jb = static_cast<int>(static_cast<long long>(n) * c / T), je = static_cast<int>(static_cast<long long>(n) * (c + 1) / T);
-  };
+  size_for_copy(pairs, 2 * M.nnz());
+  std::vector<long long> start;
+  bucket_rows(M, T, start, [&](long long q, int i, int j, int) { pairs[2 * q] = i, pairs[2 * q + 1] = j; });
   parallel_ranges(
-      T,
-      [&](long long cb, long long ce) {
-        for (long long c = cb; c < ce; ++c) {
-          int jb, je;
-          cols(c, jb, je);
-          long long* h = &at[static_cast<std::size_t>(c) * nb];
-          for (int k = M.col_start[jb]; k < M.col_start[je]; ++k) ++h[M.row_index[k] >> kShift];
-        }
-      },
-      1);
-  long long pos = 0;  // blocks in order, and inside a block the chunks in order
-  for (int b = 0; b < nb; ++b) {
-    start[b] = pos;
-    for (int c = 0; c < T; ++c) {
-      const long long cnt = at[static_cast<std::size_t>(c) * nb + b];
-      at[static_cast<std::size_t>(c) * nb + b] = pos;
-      pos += cnt;
-    }
-  }
-  start[nb] = pos;
-  size_for_copy(pairs, static_cast<std::size_t>(2 * nnz));
-  parallel_ranges(
-      T,
-      [&](long long cb, long long ce) {
-        for (long long c = cb; c < ce; ++c) {
-          int jb, je;
-          cols(c, jb, je);
-          long long* h = &at[static_cast<std::size_t>(c) * nb];
-          for (int j = jb; j < je; ++j)
-            for (int k = M.col_start[j]; k < M.col_start[j + 1]; ++k) {
-              const int i = M.row_index[k];
-              const long long q = h[i >> kShift]++;
-              pairs[2 * q] = i, pairs[2 * q + 1] = j;
-            }
-        }
-      },
-      1);
-  parallel_ranges(
-      nb,
+      static_cast<long long>(start.size()) - 1,
       [&](long long bb, long long be) {
         for (long long q = start[bb]; q < start[be]; ++q) {
           const int i = pairs[2 * q];
@@ -1121,17 +1209,24 @@ Solution solve_impl(const Model& model, const Options& options) {
     // model with its own norms. check_solution's measures are not the same test, so the KKT
     // statistics are recomputed here exactly as kkt_general defines them.
     const int m = model.num_rows, n = model.num_cols;
-    std::vector<double> ax = std::vector<double>(m, 0.0), aty(n, 0.0), ymin(s.y);
-    for (double& v : ymin) v *= model.sense;
-    // A·x row-sequential in column order (kkt_general's CSR product): walking the columns in
-    // increasing order and adding into each row adds every row's terms in exactly that order.
-    for (int j = 0; j < n; ++j)
-      for (int k = model.col_start[j]; k < model.col_start[j + 1]; ++k) ax[model.row_index[k]] += model.value[k] * s.x[j];
-    for (int j = 0; j < n; ++j) {
-      double acc = 0;
-      for (int k = model.col_start[j]; k < model.col_start[j + 1]; ++k) acc += model.value[k] * ymin[model.row_index[k]];
-      aty[j] = acc;
-    }
+    std::vector<double> aty = pooled_storage(static_cast<std::size_t>(n)), ymin = pooled_storage(s.y.size());
+    parallel_ranges(m, [&](long long ib, long long ie) {
+      for (long long i = ib; i < ie; ++i) ymin[i] = s.y[i] * model.sense;
+    });
+    // A·x row-sequential in column order (kkt_general's CSR product): row_activity adds every
+    // row's terms in increasing column order, exactly that order.
+    std::vector<double> ax = model.row_activity(s.x);
+    struct GiveBack {  // the three buffers go back to the pool on every return below
+      std::vector<double>&a, &b, &c;
+      ~GiveBack() { pool_vector(std::move(a)), pool_vector(std::move(b)), pool_vector(std::move(c)); }
+    } give_back{ax, aty, ymin};
+    parallel_ranges(n, [&](long long jb, long long je) {
+      for (long long j = jb; j < je; ++j) {
+        double acc = 0;
+        for (int k = model.col_start[j]; k < model.col_start[j + 1]; ++k) acc += model.value[k] * ymin[model.row_index[k]];
+        aty[j] = acc;
+      }
+    });
     double rp2 = 0, rd2 = 0, b2 = 0, c2 = 0, p = 0, d = 0, cinf = 0, pmax = 0, dmax = 0;
     auto ev = [](double v, double lo, double up) {
       if (v < lo) return (lo - v) / (1.0 + std::fabs(lo));

@@ -46,3 +46,24 @@ def orc():
     if not oracle.available():
         pytest.skip("oracle/liboracle.so not built (make -C oracle oracle)")
     return oracle
+
+
+@pytest.fixture(scope="session")
+def host_probe(tmp_path_factory):
+    """tests/native/host_probe.cpp linked with the library's host objects (compiled from the
+    library's sources when the build's objects are absent): the library's presolve, postsolve,
+    check_solution and certified bound on model files, on the CPU."""
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    pkg = os.path.join(root, "ps26119-solver_b200")
+    csrc = os.path.join(pkg, "csrc")
+    units = ("solver.cpp", "certify.cpp", "io.cpp")
+    objs = [os.path.join(pkg, "_build", u + ".o") for u in units]
+    if not all(os.path.exists(o) for o in objs):
+        objs = [os.path.join(csrc, u) for u in units]
+    exe = str(tmp_path_factory.mktemp("probe") / "host_probe")
+    cmd = ["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-I", csrc, "-I", "/usr/local/cuda/include",
+           os.path.join(root, "tests", "native", "host_probe.cpp"), *objs, "-o", exe, "-lpthread"]
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    return exe
