@@ -130,10 +130,10 @@ double Model::objective_value(const std::vector<double>& x) const {  // model.cp
 }
 
 namespace {
+// The host threads a pass may use (as parallel_ranges: at most 32).
+int host_threads() { return static_cast<int>(std::min(32u, std::max(1u, std::thread::hardware_concurrency()))); }
 // Host threads for an O(nnz) pass over a model with `nnz` entries (one below 2^18 entries).
-int pass_threads(long long nnz) {
-  return nnz < (1LL << 18) ? 1 : static_cast<int>(std::min(32u, std::max(1u, std::thread::hardware_concurrency())));
-}
+int pass_threads(long long nnz) { return nnz < (1LL << 18) ? 1 : host_threads(); }
 
 // Groups the entries of the column-major matrix by block of 2^kRowShift rows, for passes that
 // update rows without atomics. Chunk c (one per thread) is the column range [n·c/T, n·(c+1)/T).
@@ -474,12 +474,36 @@ struct PresolveScratch {
 };
 thread_local PresolveScratch t_presolve;
 
+// An ordered scan of [0, len) in T chunks on the host threads: count(b, e) returns the number of
+// items chunk [b, e) will write, size(total) is called once with the sum, then fill(b, e, at)
+// writes the chunk's items starting at `at`, the number of items of the chunks before it.
+template <class Count, class Size, class Fill>
+void ordered_scan(long long len, int T, Count count, Size size, Fill fill) {
+  if (len < T) T = static_cast<int>(std::max<long long>(len, 1));
+  std::vector<long long> at(static_cast<std::size_t>(T) + 1, 0);
+  auto lo = [&](long long c) { return len * c / T; };
+  parallel_ranges(
+      T,
+      [&](long long cb, long long ce) {
+        for (long long c = cb; c < ce; ++c) at[static_cast<std::size_t>(c) + 1] = count(lo(c), lo(c + 1));
+      },
+      1);
+  for (int c = 0; c < T; ++c) at[static_cast<std::size_t>(c) + 1] += at[static_cast<std::size_t>(c)];
+  size(at[static_cast<std::size_t>(T)]);
+  parallel_ranges(
+      T,
+      [&](long long cb, long long ce) {
+        for (long long c = cb; c < ce; ++c) fill(lo(c), lo(c + 1), at[static_cast<std::size_t>(c)]);
+      },
+      1);
+}
+
 // The indices i in [0, count) with pred(i), in increasing order, into `out`; pred is evaluated
 // on the host threads (it must only read).
 template <class Pred>
 void select_in_order(int count, Pred pred, std::vector<int>& out) {
   out.clear();
-  const int T = count < 65536 ? 1 : static_cast<int>(std::min(32u, std::max(1u, std::thread::hardware_concurrency())));
+  const int T = count < 65536 ? 1 : host_threads();
   if (T == 1) {
     for (int i = 0; i < count; ++i)
       if (pred(i)) out.push_back(i);
@@ -740,12 +764,37 @@ void presolve_into(const Model& M, PresolveResult& r) {  // presolve.cpp:22-156 
     return;
   }
   Model& R = r.reduced;
+  // The maps and the reduced matrix are built by ordered scans on the host threads: each chunk
+  // counts its items, the chunks' offsets are their counts' prefix sums, and each chunk then
+  // writes its items from its offset, so the output is that of one sequential pass.
   std::vector<int>& new_row = S.new_row;
-  new_row.assign(static_cast<std::size_t>(m), -1);
-  for (int i = 0; i < m; ++i)
-    if (row_alive[i]) new_row[i] = static_cast<int>(r.row_map.size()), r.row_map.push_back(i);
-  for (int j = 0; j < n; ++j)
-    if (col_alive[j]) r.col_map.push_back(j);
+  size_for_copy(new_row, static_cast<std::size_t>(m));
+  ordered_scan(
+      m, m < 65536 ? 1 : host_threads(),
+      [&](long long b, long long e) {
+        long long k = 0;
+        for (long long i = b; i < e; ++i) k += row_alive[i] != 0;
+        return k;
+      },
+      [&](long long total) { size_for_copy(r.row_map, static_cast<std::size_t>(total)); },
+      [&](long long b, long long e, long long at) {
+        for (long long i = b; i < e; ++i) {
+          new_row[i] = row_alive[i] ? static_cast<int>(at) : -1;
+          if (row_alive[i]) r.row_map[at++] = static_cast<int>(i);
+        }
+      });
+  ordered_scan(
+      n, n < 65536 ? 1 : host_threads(),
+      [&](long long b, long long e) {
+        long long k = 0;
+        for (long long j = b; j < e; ++j) k += col_alive[j] != 0;
+        return k;
+      },
+      [&](long long total) { size_for_copy(r.col_map, static_cast<std::size_t>(total)); },
+      [&](long long b, long long e, long long at) {
+        for (long long j = b; j < e; ++j)
+          if (col_alive[j]) r.col_map[at++] = static_cast<int>(j);
+      });
   // Every vector of R is sized here and overwritten in full: it keeps its size from the last
   // call, so a repeated call writes each element once (no zero fill before the copy).
   R.sense = M.sense;
@@ -769,49 +818,37 @@ void presolve_into(const Model& M, PresolveResult& r) {  // presolve.cpp:22-156 
       R.row_lower[q] = rl[i], R.row_upper[q] = ru[i];
     }
   });
+  // The kept columns' entries in kept rows, renumbered. With no row removed, every entry of a
+  // kept column is kept under its own row number.
+  const bool all_rows = r.removed_rows == 0;
   R.col_start[0] = 0;
-  if (r.removed_rows == 0) {
-    // row numbers unchanged: the kept columns' entries are copied as they are, one block per
-    // run of kept columns whose entries are contiguous (removed columns without entries do not
-    // break a run); the blocks go in one parallel copy once every run's place is known
-    struct Run {
-      int k0, k1;
-      std::size_t at;
-    };
-    std::vector<Run> runs;
-    std::size_t at = 0;
-    for (int q = 0; q < nk;) {
-      int e = q + 1;
-      while (e < nk && M.col_start[r.col_map[e]] == M.col_start[r.col_map[e - 1] + 1]) ++e;
-      const int k0 = M.col_start[r.col_map[q]], k1 = M.col_start[r.col_map[e - 1] + 1];
-      const int base = static_cast<int>(at) - k0;
-      runs.push_back({k0, k1, at});
-      for (int c = q; c < e; ++c) R.col_start[c + 1] = M.col_start[r.col_map[c] + 1] + base;
-      at += static_cast<std::size_t>(k1 - k0);
-      q = e;
-    }
-    size_for_copy(R.row_index, at), size_for_copy(R.value, at);
-    std::vector<CopyJob> jobs;
-    jobs.reserve(2 * runs.size());
-    for (const Run& u : runs) {
-      const std::size_t len = static_cast<std::size_t>(u.k1 - u.k0);
-      jobs.push_back({R.row_index.data() + u.at, M.row_index.data() + u.k0, 4 * len});
-      jobs.push_back({R.value.data() + u.at, M.value.data() + u.k0, 8 * len});
-    }
-    parallel_copy(jobs.data(), jobs.size());
-  } else {
-    R.row_index.clear(), R.value.clear();
-    R.row_index.reserve(M.nnz());
-    R.value.reserve(M.nnz());
-    for (int q = 0; q < nk; ++q) {
-      const int j = r.col_map[q];
-      for (int p = M.col_start[j]; p < M.col_start[j + 1]; ++p) {
-        const int i = M.row_index[p];
-        if (new_row[i] >= 0) R.row_index.push_back(new_row[i]), R.value.push_back(M.value[p]);
-      }
-      R.col_start[q + 1] = static_cast<int>(R.value.size());
-    }
-  }
+  ordered_scan(
+      nk, pass_threads(static_cast<long long>(M.nnz())),
+      [&](long long qb, long long qe) {
+        long long k = 0;
+        for (long long q = qb; q < qe; ++q) {
+          const int j = r.col_map[static_cast<std::size_t>(q)];
+          if (all_rows) {
+            k += M.col_start[j + 1] - M.col_start[j];
+          } else {
+            for (int p = M.col_start[j]; p < M.col_start[j + 1]; ++p) k += new_row[M.row_index[p]] >= 0;
+          }
+        }
+        return k;
+      },
+      [&](long long total) {
+        size_for_copy(R.row_index, static_cast<std::size_t>(total)), size_for_copy(R.value, static_cast<std::size_t>(total));
+      },
+      [&](long long qb, long long qe, long long at) {
+        for (long long q = qb; q < qe; ++q) {
+          const int j = r.col_map[static_cast<std::size_t>(q)];
+          for (int p = M.col_start[j]; p < M.col_start[j + 1]; ++p) {
+            const int i = all_rows ? M.row_index[p] : new_row[M.row_index[p]];
+            if (i >= 0) R.row_index[at] = i, R.value[at] = M.value[p], ++at;
+          }
+          R.col_start[q + 1] = static_cast<int>(at);
+        }
+      });
   r.outcome = PresolveResult::Outcome::Reduced;
 }
 

@@ -118,6 +118,7 @@ GENERATED = {
     **{f"columns_only_{s}": (lambda s=s: columns_only(s)) for s in range(2)},
     "columns_only_large": lambda: columns_only(5, m=400, n=300),
     "planted_sparse": lambda: planted_sparse(3),
+    "random_m70000": lambda: g.random_lp(70_000, seed=6),  # empty columns only, threaded copy
     "infeasible_empty_row": infeasible_empty_row,
     "random_m300": lambda: g.random_lp(300, seed=4),
     "staircase_T3": lambda: g.staircase_lp(3, seed=2),
