@@ -1,10 +1,18 @@
 // parallel_copy_check.cpp — test driver for csrc/parallel.hpp: parallel_copy against memcpy on
 // random job lists (empty jobs, small ones, and ones above the 4 MiB threading threshold), with
 // guard bytes on both sides of every destination; size_for_copy keeps or replaces a buffer as
-// documented. Prints "ok" and exits 0, or names the first mismatch and exits 1.
+// documented; parallel_ranges covers every index exactly once when sections run from several
+// threads at once (all but one fall back to threads of their own), when a section is started
+// inside another, and in a child process made by fork() after the pool has started. Prints "ok"
+// and exits 0, or names the first failure and exits 1.
+#include <sys/wait.h>
+#include <unistd.h>
+
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <random>
+#include <thread>
 #include <vector>
 
 #include "parallel.hpp"
@@ -47,6 +55,46 @@ int main() {
   size_for_copy(v, 1000);  // larger: a new buffer of exactly that size
   if (v.size() != 1000) {
     std::printf("size_for_copy beyond capacity\n");
+    return 1;
+  }
+  // every index of [0, n) visited exactly once by a section
+  auto covers = [](long long n) {
+    std::vector<std::atomic<int>> seen(static_cast<std::size_t>(n));
+    for (auto& a : seen) a.store(0);
+    parallel_ranges(n, [&](long long b, long long e) {
+      for (long long i = b; i < e; ++i) seen[static_cast<std::size_t>(i)].fetch_add(1);
+    });
+    for (auto& a : seen)
+      if (a.load() != 1) return false;
+    return true;
+  };
+  std::atomic<int> bad{0};
+  std::vector<std::thread> callers;
+  for (int c = 0; c < 4; ++c)
+    callers.emplace_back([&] {
+      for (int k = 0; k < 50; ++k)
+        if (!covers(70000 + 977 * k)) ++bad;
+    });
+  for (auto& t : callers) t.join();
+  if (bad.load()) {
+    std::printf("concurrent sections\n");
+    return 1;
+  }
+  std::atomic<long long> inner{0};
+  parallel_ranges(100000, [&](long long b, long long e) {  // a section inside a section
+    (void)b, (void)e;
+    parallel_ranges(70000, [&](long long ib, long long ie) { inner += ie - ib; });
+  });
+  const long long T = std::min<long long>(std::max(1u, std::thread::hardware_concurrency()), 32);
+  if (inner.load() != 70000 * T) {
+    std::printf("nested sections: %lld\n", inner.load());
+    return 1;
+  }
+  const pid_t pid = fork();
+  if (pid == 0) _exit(covers(123457) && covers(70001) ? 0 : 1);  // the child's own pool
+  int status = 0;
+  if (pid < 0 || waitpid(pid, &status, 0) != pid || !WIFEXITED(status) || WEXITSTATUS(status) != 0) {
+    std::printf("sections in a forked child\n");
     return 1;
   }
   std::printf("ok\n");

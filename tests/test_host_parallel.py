@@ -1,6 +1,7 @@
-"""The host threading helpers (csrc/parallel.hpp) that the C API's model copy, presolve and
-postsolve use: tests/native/parallel_copy_check.cpp, compiled here, checks parallel_copy
-byte for byte against memcpy. CPU only."""
+"""The host threading helpers (csrc/parallel.hpp) that the C API's model copy, presolve,
+postsolve and the checks use: tests/native/parallel_copy_check.cpp, compiled here, checks
+parallel_copy byte for byte against memcpy, and that the worker pool behind parallel_ranges
+covers every index once with concurrent callers, nested sections and a forked child. CPU only."""
 import os
 import subprocess
 
