@@ -143,6 +143,9 @@ int pass_threads(long long nnz) { return nnz < (1LL << 18) ? 1 : host_threads();
 // pass. place(q, i, j, k) is called once for entry k (row i, column j) with its slot q, on the
 // thread of the entry's chunk.
 constexpr int kRowShift = 14;  // 16,384 rows: a block's rows fit in one core's cache
+// Bucketing holds 8-12 bytes per entry; above this many entries the passes that use it fall
+// back to forms without scratch (atomics, or one sequential pass).
+constexpr long long kBucketMaxEntries = 1LL << 28;
 template <class Place>
 void bucket_rows(const Model& M, int T, std::vector<long long>& start, Place place) {
   const int m = M.num_rows, n = M.num_cols;
@@ -204,7 +207,7 @@ thread_local ActivityScratch t_activity;
 std::vector<double> Model::row_activity(const std::vector<double>& x) const {  // model.cpp:175-180
   std::vector<double> ax = pooled_vector(static_cast<std::size_t>(num_rows));  // zeros
   const int T = pass_threads(static_cast<long long>(nnz()));
-  if (T == 1) {
+  if (T == 1 || static_cast<long long>(nnz()) > kBucketMaxEntries) {
     for (int j = 0; j < num_cols; ++j)
       for (int k = col_start[j]; k < col_start[j + 1]; ++k) ax[row_index[k]] += value[k] * x[j];
     return ax;
@@ -537,6 +540,16 @@ void row_tags(const Model& M, std::vector<int>& row_xor, std::vector<int>& row_c
   if (T == 1) {
     for (int j = 0; j < n; ++j)
       for (int k = M.col_start[j]; k < M.col_start[j + 1]; ++k) row_xor[M.row_index[k]] ^= j, ++row_cnt[M.row_index[k]];
+    return;
+  }
+  if (static_cast<long long>(M.nnz()) > kBucketMaxEntries) {  // no scratch: relaxed integer atomics
+    parallel_ranges(n, [&](long long jb, long long je) {
+      for (long long j = jb; j < je; ++j)
+        for (int k = M.col_start[j]; k < M.col_start[j + 1]; ++k) {
+          __atomic_fetch_xor(&row_xor[M.row_index[k]], static_cast<int>(j), __ATOMIC_RELAXED);
+          __atomic_fetch_add(&row_cnt[M.row_index[k]], 1, __ATOMIC_RELAXED);
+        }
+    });
     return;
   }
   size_for_copy(pairs, 2 * M.nnz());
