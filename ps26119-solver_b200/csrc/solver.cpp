@@ -144,8 +144,12 @@ int pass_threads(long long nnz) { return nnz < (1LL << 18) ? 1 : host_threads();
 // thread of the entry's chunk.
 constexpr int kRowShift = 14;  // 16,384 rows: a block's rows fit in one core's cache
 // Bucketing holds 8-12 bytes per entry; above this many entries the passes that use it fall
-// back to forms without scratch (atomics, or one sequential pass).
-constexpr long long kBucketMaxEntries = 1LL << 28;
+// back to forms without scratch (atomics, or one sequential pass). The tests build a copy with
+// a small limit to run those forms on small models.
+#ifndef PS26119_BUCKET_MAX_ENTRIES
+#define PS26119_BUCKET_MAX_ENTRIES (1LL << 28)
+#endif
+constexpr long long kBucketMaxEntries = PS26119_BUCKET_MAX_ENTRIES;
 template <class Place>
 void bucket_rows(const Model& M, int T, std::vector<long long>& start, Place place) {
   const int m = M.num_rows, n = M.num_cols;

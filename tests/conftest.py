@@ -48,22 +48,34 @@ def orc():
     return oracle
 
 
-@pytest.fixture(scope="session")
-def host_probe(tmp_path_factory):
-    """tests/native/host_probe.cpp linked with the library's host objects (compiled from the
-    library's sources when the build's objects are absent): the library's presolve, postsolve,
-    check_solution and certified bound on model files, on the CPU."""
+def _build_host_probe(out_dir, defines=()):
     import subprocess
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     pkg = os.path.join(root, "ps26119-solver_b200")
     csrc = os.path.join(pkg, "csrc")
     units = ("solver.cpp", "certify.cpp", "io.cpp")
     objs = [os.path.join(pkg, "_build", u + ".o") for u in units]
-    if not all(os.path.exists(o) for o in objs):
+    if defines or not all(os.path.exists(o) for o in objs):
         objs = [os.path.join(csrc, u) for u in units]
-    exe = str(tmp_path_factory.mktemp("probe") / "host_probe")
-    cmd = ["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-I", csrc, "-I", "/usr/local/cuda/include",
-           os.path.join(root, "tests", "native", "host_probe.cpp"), *objs, "-o", exe, "-lpthread"]
+    exe = str(out_dir / "host_probe")
+    cmd = ["g++", "-O2", "-std=c++17", "-ffp-contract=off", *[f"-D{d}" for d in defines], "-I", csrc, "-I",
+           "/usr/local/cuda/include", os.path.join(root, "tests", "native", "host_probe.cpp"), *objs, "-o", exe,
+           "-lpthread"]
     r = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr
     return exe
+
+
+@pytest.fixture(scope="session")
+def host_probe(tmp_path_factory):
+    """tests/native/host_probe.cpp linked with the library's host objects (compiled from the
+    library's sources when the build's objects are absent): the library's presolve, postsolve,
+    check_solution and certified bound on model files, on the CPU."""
+    return _build_host_probe(tmp_path_factory.mktemp("probe"))
+
+
+@pytest.fixture(scope="session")
+def host_probe_no_buckets(tmp_path_factory):
+    """The host probe built from the library's sources with the row-block bucketing limited to
+    4,096 entries, so that larger models take the passes' forms without scratch."""
+    return _build_host_probe(tmp_path_factory.mktemp("probe_nb"), defines=("PS26119_BUCKET_MAX_ENTRIES=4096",))

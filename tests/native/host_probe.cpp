@@ -8,6 +8,9 @@
 //     vectors are reused from job to job, as repeated solves on one thread reuse them. For each
 //     job out.bin receives the sizes of x, y and z (int64 each), then x, y, z and the objective
 //     (float64); a job whose model presolve does not reduce writes three sizes of -1 only.
+//   host_probe digest <out.txt> <model>...
+//     presolve of each model into one reused result: its digest (as `ps26119 info` prints it),
+//     one line per model.
 //   host_probe check <out.bin> (<model> <x.bin> <y.bin>)...
 //     check_solution and certified_dual_bound (with implied bounds) of the point on the
 //     model: per job 7 float64 — passed, max primal violation, max dual violation, relative
@@ -99,12 +102,35 @@ static int check_jobs(std::FILE* out, int argc, char** argv) {
   return 0;
 }
 
+static int digest_jobs(std::FILE* out, int argc, char** argv) {
+  PresolveResult pr;
+  for (int a = 0; a < argc; ++a) {
+    Model M;
+    ModelInfo info;
+    std::string err;
+    if (!read_model(argv[a], M, info, err)) {
+      std::fprintf(stderr, "%s: %s\n", argv[a], err.c_str());
+      return 3;
+    }
+    presolve_into(M, pr);
+    std::fprintf(out, "%016llx\n", static_cast<unsigned long long>(presolve_digest(pr)));
+  }
+  return 0;
+}
+
 int main(int argc, char** argv) {
+  const std::string cmd = argc > 1 ? argv[1] : "";
+  if (cmd == "digest" && argc >= 4) {
+    std::FILE* out = std::fopen(argv[2], "w");
+    if (!out) return 3;
+    const int rc = digest_jobs(out, argc - 3, argv + 3);
+    std::fclose(out);
+    return rc;
+  }
   if (argc < 6 || (argc - 3) % 3 != 0) {
-    std::fprintf(stderr, "usage: host_probe postsolve|check <out.bin> (<model> <a.bin> <b.bin>)...\n");
+    std::fprintf(stderr, "usage: host_probe digest <out.txt> <model>... | postsolve|check <out.bin> (<model> <a.bin> <b.bin>)...\n");
     return 2;
   }
-  const std::string cmd = argv[1];
   std::FILE* out = std::fopen(argv[2], "wb");
   if (!out) return 3;
   const int rc = cmd == "postsolve" ? postsolve_jobs(out, argc - 3, argv + 3)

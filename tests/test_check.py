@@ -23,6 +23,15 @@ def _points(lp, rng):
 
 
 def test_check_and_bound_match_reference(ref, tmp_path, host_probe):
+    _compare(ref, tmp_path, host_probe)
+
+
+def test_check_without_row_buckets(ref, tmp_path, host_probe_no_buckets):
+    # above the bucketing limit the row activity is one sequential pass; same bits
+    _compare(ref, tmp_path, host_probe_no_buckets)
+
+
+def _compare(ref, tmp_path, host_probe):
     rng = np.random.default_rng(21)
     models = {name: GENERATED[name]() for name in ("planted_0", "planted_3", "columns_only_1", "staircase_T3",
                                                      "infeasible_empty_row")}

@@ -273,3 +273,20 @@ def test_postsolve_matches_reference(ref, tmp_path, postsolve_probe):
         for q, label in enumerate(("x", "y", "z")):
             assert _same_bits(o[q], w[q]), (name, variant, label)
         assert _same_bits(np.array([o[3]]), np.array([w[3]])) or (np.isnan(o[3]) and np.isnan(w[3])), (name, variant)
+
+
+def test_presolve_without_row_buckets(ref, tmp_path, host_probe_no_buckets):
+    # above the bucketing limit the row counts and XORs take relaxed integer atomics instead;
+    # a probe built with a 4,096-entry limit runs that form on the large models
+    names = ["planted_sparse", "random_m70000", "planted_2"]
+    paths = []
+    for name in names:
+        path = str(tmp_path / f"{name}.mps")
+        write_mps(GENERATED[name](), path)
+        paths.append(path)
+    out = tmp_path / "digests.txt"
+    r = subprocess.run([host_probe_no_buckets, "digest", str(out), *paths], capture_output=True, text=True,
+                       timeout=600)
+    assert r.returncode == 0, r.stderr
+    got = open(out).read().split()
+    assert got == [ref.presolve_file(p)[0] for p in paths]
