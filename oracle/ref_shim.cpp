@@ -24,6 +24,8 @@
 //                    singletons, reduced fingerprint; 8-byte words, FNV-1a).
 //   ref_postsolve_file the reference reader, presolve, then postsolve (src/core/presolve.cpp:158-193)
 //                    of a given reduced (x, y): the original x, y, z and objective.
+//   ref_kkt_file     the presolve wrapper's KKT test of a point on the original model
+//                    (original_kkt, src/core/solve.cpp:77-84; pdhg::kkt_general).
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -426,6 +428,30 @@ int ref_postsolve_file(const char* path, const double* red_x, long long nx, cons
   sizes[0] = static_cast<long long>(s.x.size());
   sizes[1] = static_cast<long long>(s.y.size());
   sizes[2] = static_cast<long long>(s.z.size());
+  return 1;
+}
+
+// pdhg::kkt_general (src/pdhg/cpu_backend.cpp:225-284) of (x, sense·y) on the model read from a
+// file, as original_kkt (src/core/solve.cpp:77-84) forms it: out[8] = primal residual, dual
+// residual, primal objective, dual objective, b norm, c norm, primal max rel, dual max rel;
+// out[8] = converged(eps). Returns 1, or 0 when the file does not read.
+int ref_kkt_file(const char* path, const double* x, const double* y, double eps, double* out) {
+  Model M;
+  const std::string p(path);
+  std::string err;
+  bool ok = false;
+  if (p.size() > 4 && p.compare(p.size() - 4, 4, ".lpm") == 0) ok = io::read_lpm(p, M).ok;
+  else ok = io::read_mps(p, M, err);
+  if (!ok) return 0;
+  const la::Csr<double> A = la::csr_from_model(M), At = la::csr_transpose_from_model(M);
+  const pdhg::LpView lp{M.num_rows, M.num_cols, M.sense, M.obj.data(), M.col_lower.data(), M.col_upper.data(),
+                        M.row_lower.data(), M.row_upper.data()};
+  std::vector<double> ymin(y, y + M.num_rows);
+  for (double& v : ymin) v *= M.sense;
+  const pdhg::KktStats k = pdhg::kkt_general(A, At, lp, std::vector<double>(x, x + M.num_cols), ymin);
+  const double vals[9] = {k.primal_residual, k.dual_residual, k.primal_obj, k.dual_obj, k.b_norm, k.c_norm,
+                          k.primal_max_rel, k.dual_max_rel, k.converged(eps) ? 1.0 : 0.0};
+  std::copy(vals, vals + 9, out);
   return 1;
 }
 

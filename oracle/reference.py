@@ -93,6 +93,7 @@ def lib():
         L.ref_presolve_file.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int,
                                         ctypes.POINTER(ctypes.c_longlong)]
         L.ref_check_file.argtypes = [ctypes.c_char_p, _D, _D, _D]
+        L.ref_kkt_file.argtypes = [ctypes.c_char_p, _D, _D, ctypes.c_double, _D]
         L.ref_postsolve_file.argtypes = [ctypes.c_char_p, _D, ctypes.c_longlong, _D, ctypes.c_longlong, _D, _D, _D,
                                          _D, ctypes.POINTER(ctypes.c_longlong)]
         L.ref_certificate.argtypes = [ctypes.c_int] + model + [_D, _D, _D]
@@ -216,6 +217,17 @@ def check_file(path, x, y):
     out = np.zeros(7)
     ok = L.ref_check_file(os.fsencode(path), _d(np.ascontiguousarray(x, dtype=np.float64)),
                           _d(np.ascontiguousarray(y, dtype=np.float64)), _d(out))
+    return out if ok else None
+
+
+def kkt_file(path, x, y, eps):
+    """original_kkt (reference src/core/solve.cpp:77-84) of (x, y) on the model read from a
+    file: the 8 KktStats values and converged(eps) as an array of 9, or None when the file does
+    not read."""
+    L = lib()
+    out = np.zeros(9)
+    ok = L.ref_kkt_file(os.fsencode(path), _d(np.ascontiguousarray(x, dtype=np.float64)),
+                        _d(np.ascontiguousarray(y, dtype=np.float64)), float(eps), _d(out))
     return out if ok else None
 
 

@@ -440,6 +440,110 @@ CheckReport check_solution(const Model& lp, const std::vector<double>& x, const 
   return rep;
 }
 
+bool OriginalKkt::converged(double eps) const {  // termination.h:51-55 (obj_shift 0)
+  const double rprim = primal_residual / (1.0 + b_norm), rdual = dual_residual / (1.0 + c_norm);
+  const double gap = std::fabs(primal_obj - dual_obj) / (1.0 + std::fabs(primal_obj) + std::fabs(dual_obj));
+  if (std::max({rprim, rdual, gap}) > eps) return false;
+  if (eps >= 1e-6) return true;  // tolerances.h:34-36, the verifier's 1e-6
+  return primal_max_rel <= 1e-6 && dual_max_rel <= 1e-6 && gap <= 1e-6;
+}
+
+OriginalKkt original_kkt(const Model& model, const std::vector<double>& x, const std::vector<double>& y) {
+  // kkt_general (cpu_backend.cpp:225-284) on the original model with multipliers sense·y.
+  // Element-wise terms are computed on the host threads; every sum is then taken in the
+  // reference's order (rows, then columns), adding exactly the terms it adds, and the maxima
+  // combine exactly in any order.
+  const int m = model.num_rows, n = model.num_cols;
+  // A·x row-sequential in column order (kkt_general's CSR product): row_activity adds every
+  // row's terms in increasing column order, exactly that order.
+  std::vector<double> ax = model.row_activity(x);
+  // per row: viol², max(|lo|,|up|)², the dual objective term and the dual residual term (each
+  // with a flag: whether the reference adds it)
+  std::vector<double> r_viol = pooled_storage(static_cast<std::size_t>(m)), r_b = pooled_storage(static_cast<std::size_t>(m));
+  std::vector<double> r_d = pooled_storage(static_cast<std::size_t>(m)), r_rd = pooled_storage(static_cast<std::size_t>(m));
+  // per column: c_j², c_j·x_j, the dual residual term and the dual objective term (flagged)
+  std::vector<double> c_c = pooled_storage(static_cast<std::size_t>(n)), c_p = pooled_storage(static_cast<std::size_t>(n));
+  std::vector<double> c_rd = pooled_storage(static_cast<std::size_t>(n)), c_d = pooled_storage(static_cast<std::size_t>(n));
+  std::vector<char> r_flag(static_cast<std::size_t>(m)), c_flag(static_cast<std::size_t>(n));  // bit 0: d, bit 1: rd
+  std::mutex mu;
+  double pmax = 0, dmax = 0, cinf = 0;
+  auto ev = [](double v, double lo, double up) {
+    if (v < lo) return (lo - v) / (1.0 + std::fabs(lo));
+    if (v > up) return (v - up) / (1.0 + std::fabs(up));
+    return 0.0;
+  };
+  parallel_ranges(m, [&](long long ib, long long ie) {
+    double pm = 0, dm = 0;
+    for (long long i = ib; i < ie; ++i) {
+      const double lo = model.row_lower[i], up = model.row_upper[i];
+      const double viol = ax[i] < lo ? lo - ax[i] : (ax[i] > up ? ax[i] - up : 0.0);
+      r_viol[i] = viol * viol;
+      pm = std::max(pm, ev(ax[i], lo, up));
+      const double bl = std::isfinite(lo) ? std::fabs(lo) : 0.0, bu = std::isfinite(up) ? std::fabs(up) : 0.0;
+      r_b[i] = std::max(bl, bu) * std::max(bl, bu);
+      const double yi = y[i] * model.sense;
+      char f = 0;
+      if (yi > 0) {
+        if (std::isfinite(lo)) r_d[i] = yi * lo, f = 1;
+        else r_rd[i] = yi * yi, f = 2, dm = std::max(dm, yi);
+      } else if (yi < 0) {
+        if (std::isfinite(up)) r_d[i] = yi * up, f = 1;
+        else r_rd[i] = yi * yi, f = 2, dm = std::max(dm, -yi);
+      }
+      r_flag[i] = f;
+    }
+    std::lock_guard<std::mutex> lock(mu);
+    pmax = std::max(pmax, pm), dmax = std::max(dmax, dm);
+  });
+  parallel_ranges(n, [&](long long jb, long long je) {
+    double pm = 0, dm = 0, ci = 0;
+    for (long long j = jb; j < je; ++j) {
+      double aty = 0;  // (Aᵀ·sense·y)_j in the column's entry order (the transpose's CSR product)
+      for (int k = model.col_start[j]; k < model.col_start[j + 1]; ++k)
+        aty += model.value[k] * (y[model.row_index[k]] * model.sense);
+      const double cj = model.sense * model.obj[j];
+      c_c[j] = cj * cj;
+      ci = std::max(ci, std::fabs(cj));
+      c_p[j] = cj * x[j];
+      pm = std::max(pm, ev(x[j], model.col_lower[j], model.col_upper[j]));
+      const double lam = cj - aty, lo = model.col_lower[j], up = model.col_upper[j];
+      double z;
+      if (std::isfinite(lo) && std::isfinite(up)) z = lam;
+      else if (std::isfinite(lo)) z = std::max(lam, 0.0);
+      else if (std::isfinite(up)) z = std::min(lam, 0.0);
+      else z = 0.0;
+      c_rd[j] = (lam - z) * (lam - z);
+      dm = std::max(dm, std::fabs(lam - z));
+      char f = 0;
+      if (z > 0) c_d[j] = z * lo, f = 1;
+      else if (z < 0) c_d[j] = z * up, f = 1;
+      c_flag[j] = f;
+    }
+    std::lock_guard<std::mutex> lock(mu);
+    pmax = std::max(pmax, pm), dmax = std::max(dmax, dm), cinf = std::max(cinf, ci);
+  });
+  double rp2 = 0, rd2 = 0, b2 = 0, c2 = 0, p = 0, d = 0;
+  for (int i = 0; i < m; ++i) {
+    rp2 += r_viol[i];
+    b2 += r_b[i];
+    if (r_flag[i] == 1) d += r_d[i];
+    else if (r_flag[i] == 2) rd2 += r_rd[i];
+  }
+  for (int j = 0; j < n; ++j) {
+    c2 += c_c[j];
+    p += c_p[j];
+    rd2 += c_rd[j];
+    if (c_flag[j]) d += c_d[j];
+  }
+  for (auto* v : {&ax, &r_viol, &r_b, &r_d, &r_rd, &c_c, &c_p, &c_rd, &c_d}) pool_vector(std::move(*v));
+  OriginalKkt k;
+  k.primal_residual = std::sqrt(rp2), k.dual_residual = std::sqrt(rd2);
+  k.primal_obj = p, k.dual_obj = d;
+  k.b_norm = std::sqrt(b2), k.c_norm = std::sqrt(c2);
+  k.primal_max_rel = pmax, k.dual_max_rel = dmax / (1.0 + cinf);
+  return k;
+}
+
 std::string CheckReport::summary() const {
   char buf[256];
   std::snprintf(buf, sizeof buf, "primal viol %.1e  dual viol %.1e  compl %.1e  gap %.1e  => %s", max_primal_violation,
@@ -1259,73 +1363,7 @@ Solution solve_impl(const Model& model, const Options& options) {
   post.message = post.message.empty() ? pnote : post.message + "; " + pnote;
   auto passes = [&](const Solution& s) {
     if (static_cast<int>(s.x.size()) != model.num_cols || static_cast<int>(s.y.size()) != model.num_rows) return false;
-    // original_kkt(model, s).converged(tol) (solve.cpp:77-84): KKT of (x, sense·y) on the original
-    // model with its own norms. check_solution's measures are not the same test, so the KKT
-    // statistics are recomputed here exactly as kkt_general defines them.
-    const int m = model.num_rows, n = model.num_cols;
-    std::vector<double> aty = pooled_storage(static_cast<std::size_t>(n)), ymin = pooled_storage(s.y.size());
-    parallel_ranges(m, [&](long long ib, long long ie) {
-      for (long long i = ib; i < ie; ++i) ymin[i] = s.y[i] * model.sense;
-    });
-    // A·x row-sequential in column order (kkt_general's CSR product): row_activity adds every
-    // row's terms in increasing column order, exactly that order.
-    std::vector<double> ax = model.row_activity(s.x);
-    struct GiveBack {  // the three buffers go back to the pool on every return below
-      std::vector<double>&a, &b, &c;
-      ~GiveBack() { pool_vector(std::move(a)), pool_vector(std::move(b)), pool_vector(std::move(c)); }
-    } give_back{ax, aty, ymin};
-    parallel_ranges(n, [&](long long jb, long long je) {
-      for (long long j = jb; j < je; ++j) {
-        double acc = 0;
-        for (int k = model.col_start[j]; k < model.col_start[j + 1]; ++k) acc += model.value[k] * ymin[model.row_index[k]];
-        aty[j] = acc;
-      }
-    });
-    double rp2 = 0, rd2 = 0, b2 = 0, c2 = 0, p = 0, d = 0, cinf = 0, pmax = 0, dmax = 0;
-    auto ev = [](double v, double lo, double up) {
-      if (v < lo) return (lo - v) / (1.0 + std::fabs(lo));
-      if (v > up) return (v - up) / (1.0 + std::fabs(up));
-      return 0.0;
-    };
-    for (int i = 0; i < m; ++i) {
-      const double lo = model.row_lower[i], up = model.row_upper[i];
-      const double viol = ax[i] < lo ? lo - ax[i] : (ax[i] > up ? ax[i] - up : 0.0);
-      rp2 += viol * viol;
-      pmax = std::max(pmax, ev(ax[i], lo, up));
-      const double bl = std::isfinite(lo) ? std::fabs(lo) : 0.0, bu = std::isfinite(up) ? std::fabs(up) : 0.0;
-      b2 += std::max(bl, bu) * std::max(bl, bu);
-      const double y = ymin[i];
-      if (y > 0) {
-        if (std::isfinite(lo)) d += y * lo;
-        else rd2 += y * y, dmax = std::max(dmax, y);
-      } else if (y < 0) {
-        if (std::isfinite(up)) d += y * up;
-        else rd2 += y * y, dmax = std::max(dmax, -y);
-      }
-    }
-    for (int j = 0; j < n; ++j) {
-      const double cj = model.sense * model.obj[j];
-      c2 += cj * cj;
-      cinf = std::max(cinf, std::fabs(cj));
-      p += cj * s.x[j];
-      pmax = std::max(pmax, ev(s.x[j], model.col_lower[j], model.col_upper[j]));
-      const double lam = cj - aty[j], lo = model.col_lower[j], up = model.col_upper[j];
-      double z;
-      if (std::isfinite(lo) && std::isfinite(up)) z = lam;
-      else if (std::isfinite(lo)) z = std::max(lam, 0.0);
-      else if (std::isfinite(up)) z = std::min(lam, 0.0);
-      else z = 0.0;
-      rd2 += (lam - z) * (lam - z);
-      dmax = std::max(dmax, std::fabs(lam - z));
-      if (z > 0) d += z * lo;
-      else if (z < 0) d += z * up;
-    }
-    const double rprim = std::sqrt(rp2) / (1.0 + std::sqrt(b2)), rdual = std::sqrt(rd2) / (1.0 + std::sqrt(c2));
-    const double gap = std::fabs(p - d) / (1.0 + std::fabs(p) + std::fabs(d));
-    const double rk = std::max({rprim, rdual, gap});
-    if (rk > options.tolerance) return false;
-    if (options.tolerance >= 1e-6) return true;
-    return pmax <= 1e-6 && dmax / (1.0 + cinf) <= 1e-6 && gap <= 1e-6;
+    return original_kkt(model, s.x, s.y).converged(options.tolerance);  // solve.cpp:77-84, 414
   };
   bool passed = true;
   if (post.status == Status::Optimal) {

@@ -88,6 +88,17 @@ struct CheckReport {
 };
 CheckReport check_solution(const Model& lp, const std::vector<double>& x, const std::vector<double>& row_dual);
 
+// fp64 KKT statistics of (x, y) on the original model with multipliers sense·y, as the
+// reference's kkt_general defines them (src/pdhg/cpu_backend.cpp:225-284, KktStats in
+// src/pdhg/termination.h:35-60); the presolve wrapper's test of a postsolved point
+// (original_kkt in src/core/solve.cpp:77-84).
+struct OriginalKkt {
+  double primal_residual = 0, dual_residual = 0, primal_obj = 0, dual_obj = 0, b_norm = 0, c_norm = 0;
+  double primal_max_rel = 0, dual_max_rel = 0;
+  bool converged(double eps) const;
+};
+OriginalKkt original_kkt(const Model& model, const std::vector<double>& x, const std::vector<double>& y);
+
 // Presolve R1-R4 with postsolve (presolve.h:22-65).
 struct PresolveResult {
   enum class Outcome { Reduced, Infeasible, Unchanged } outcome = Outcome::Unchanged;

@@ -11,6 +11,9 @@
 //   host_probe digest <out.txt> <model>...
 //     presolve of each model into one reused result: its digest (as `ps26119 info` prints it),
 //     one line per model.
+//   host_probe kkt <out.bin> (<model> <x.bin> <y.bin>)...
+//     original_kkt of the point: per job 11 float64 — the 8 statistics, then converged() at
+//     1e-4, 1e-8 and 1e-9.
 //   host_probe check <out.bin> (<model> <x.bin> <y.bin>)...
 //     check_solution and certified_dual_bound (with implied bounds) of the point on the
 //     model: per job 7 float64 — passed, max primal violation, max dual violation, relative
@@ -102,6 +105,26 @@ static int check_jobs(std::FILE* out, int argc, char** argv) {
   return 0;
 }
 
+static int kkt_jobs(std::FILE* out, int argc, char** argv) {
+  for (int a = 0; a + 2 < argc; a += 3) {
+    Model M;
+    ModelInfo info;
+    std::string err;
+    if (!read_model(argv[a], M, info, err)) {
+      std::fprintf(stderr, "%s: %s\n", argv[a], err.c_str());
+      return 3;
+    }
+    const std::vector<double> x = read_doubles(argv[a + 1]), y = read_doubles(argv[a + 2]);
+    const OriginalKkt k = original_kkt(M, x, y);
+    const double rec[11] = {k.primal_residual, k.dual_residual, k.primal_obj,    k.dual_obj,
+                            k.b_norm,          k.c_norm,        k.primal_max_rel, k.dual_max_rel,
+                            k.converged(1e-4) ? 1.0 : 0.0, k.converged(1e-8) ? 1.0 : 0.0,
+                            k.converged(1e-9) ? 1.0 : 0.0};
+    std::fwrite(rec, sizeof(double), 11, out);
+  }
+  return 0;
+}
+
 static int digest_jobs(std::FILE* out, int argc, char** argv) {
   PresolveResult pr;
   for (int a = 0; a < argc; ++a) {
@@ -128,13 +151,14 @@ int main(int argc, char** argv) {
     return rc;
   }
   if (argc < 6 || (argc - 3) % 3 != 0) {
-    std::fprintf(stderr, "usage: host_probe digest <out.txt> <model>... | postsolve|check <out.bin> (<model> <a.bin> <b.bin>)...\n");
+    std::fprintf(stderr, "usage: host_probe digest <out.txt> <model>... | postsolve|check|kkt <out.bin> (<model> <a.bin> <b.bin>)...\n");
     return 2;
   }
   std::FILE* out = std::fopen(argv[2], "wb");
   if (!out) return 3;
   const int rc = cmd == "postsolve" ? postsolve_jobs(out, argc - 3, argv + 3)
                  : cmd == "check"   ? check_jobs(out, argc - 3, argv + 3)
+                 : cmd == "kkt"     ? kkt_jobs(out, argc - 3, argv + 3)
                                     : 2;
   std::fclose(out);
   return rc;

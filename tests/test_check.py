@@ -59,3 +59,39 @@ def _compare(ref, tmp_path, host_probe):
         for f, label in enumerate(labels):
             assert np.array([o[f]]).view(np.uint64)[0] == np.array([w[f]]).view(np.uint64)[0] or \
                 (np.isnan(o[f]) and np.isnan(w[f])), (name, q, label, o[f], w[f])
+
+
+def test_original_kkt_matches_reference(ref, tmp_path, host_probe):
+    """original_kkt (csrc/solver.cpp), the presolve wrapper's test of a postsolved point, against
+    the reference's (src/core/solve.cpp:77-84 over pdhg::kkt_general): the 8 statistics bit for
+    bit and converged() at three tolerances, on the same model files and points; the large
+    models run the threaded form."""
+    rng = np.random.default_rng(33)
+    models = {name: GENERATED[name]() for name in ("planted_1", "columns_only_0", "staircase_T3")}
+    models["random_m50000"] = g.random_lp(50_000, seed=10)
+    models["planted_sparse"] = GENERATED["planted_sparse"]()
+    args, want, names = [], [], []
+    for k, (name, lp) in enumerate(models.items()):
+        path = str(tmp_path / f"{name}.mps")
+        write_mps(lp, path)
+        points = list(_points(lp, rng))
+        if name in ("staircase_T3", "columns_only_0"):  # the reference's own 1e-8 solution: converged
+            s = ref.solve(lp, tol=1e-8, iteration_limit=200_000)  # at 1e-4 and 1e-8, not at 1e-9
+            assert s.status == "Optimal", (name, s.status)
+            points.append((s.x, s.y))
+        for q, (x, y) in enumerate(points):
+            fx, fy = tmp_path / f"{k}_{q}_x.bin", tmp_path / f"{k}_{q}_y.bin"
+            x.tofile(fx), y.tofile(fy)
+            args += [path, str(fx), str(fy)]
+            stats = [ref.kkt_file(path, x, y, eps) for eps in (1e-4, 1e-8, 1e-9)]
+            assert stats[0] is not None, name
+            want.append(np.concatenate([stats[0][:8], [s[8] for s in stats]]))
+            names.append((name, q))
+    out = tmp_path / "kkt.bin"
+    r = subprocess.run([host_probe, "kkt", str(out), *args], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    got = np.fromfile(out, dtype=np.float64).reshape(-1, 11)
+    assert len(got) == len(want)
+    for (name, q), w, o in zip(names, want, got):
+        assert np.array_equal(o.view(np.uint64), w.view(np.uint64)), (name, q, o, w)
+    assert {tuple(w[8:]) for w in want} >= {(0.0, 0.0, 0.0), (1.0, 1.0, 0.0)}  # both outcomes seen
