@@ -10,6 +10,7 @@
 #include <atomic>
 #include <condition_variable>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 #include <functional>
 #include <mutex>
@@ -18,6 +19,22 @@
 #include <vector>
 
 namespace b200 {
+
+// The host threads one parallel section may use: every hardware thread, at most 32, or fewer
+// when the environment variable PS26119_HOST_THREADS gives a smaller positive number (read once).
+// Results do not depend on it.
+inline int host_thread_limit() {
+  static const int limit = [] {
+    const int hw = static_cast<int>(std::max(1u, std::thread::hardware_concurrency()));
+    int t = std::min(hw, 32);
+    if (const char* env = std::getenv("PS26119_HOST_THREADS")) {
+      const int want = std::atoi(env);
+      if (want > 0) t = std::min(t, want);
+    }
+    return t;
+  }();
+  return limit;
+}
 
 // Worker threads kept for the life of the process, so that a parallel section costs a wake-up
 // instead of creating and joining its threads (about 270 µs per section for 8 threads on an
@@ -104,12 +121,11 @@ class HostPool {
   std::vector<std::thread> workers_;
 };
 
-// Runs f(begin, end) over [0, n) on up to 32 host threads (inline below `min_parallel`). The
-// ranges are the same whichever threads run them.
+// Runs f(begin, end) over [0, n) on host_thread_limit() threads (inline below `min_parallel`).
+// The ranges are the same whichever threads run them.
 template <class F>
 void parallel_ranges(long long n, F&& f, long long min_parallel = 65536) {
-  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-  const long long T = n < min_parallel ? 1 : std::min<long long>(hw, 32);
+  const long long T = n < min_parallel ? 1 : std::min<long long>(n, host_thread_limit());
   if (T <= 1) {
     f(0LL, n);
     return;

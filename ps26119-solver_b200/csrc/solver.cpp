@@ -130,8 +130,8 @@ double Model::objective_value(const std::vector<double>& x) const {  // model.cp
 }
 
 namespace {
-// The host threads a pass may use (as parallel_ranges: at most 32).
-int host_threads() { return static_cast<int>(std::min(32u, std::max(1u, std::thread::hardware_concurrency()))); }
+// The host threads a pass may use (as parallel_ranges).
+int host_threads() { return host_thread_limit(); }
 // Host threads for an O(nnz) pass over a model with `nnz` entries (one below 2^18 entries).
 int pass_threads(long long nnz) { return nnz < (1LL << 18) ? 1 : host_threads(); }
 

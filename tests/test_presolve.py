@@ -290,3 +290,20 @@ def test_presolve_without_row_buckets(ref, tmp_path, host_probe_no_buckets):
     assert r.returncode == 0, r.stderr
     got = open(out).read().split()
     assert got == [ref.presolve_file(p)[0] for p in paths]
+
+
+def test_presolve_same_on_one_host_thread(ref, tmp_path):
+    # PS26119_HOST_THREADS=1 runs every host pass on the calling thread: the decisions are the
+    # same as with the threaded passes
+    from test_io import CLI
+    paths = []
+    for name in ("planted_sparse", "random_m70000"):
+        path = tmp_path / f"{name}.mps"
+        write_mps(GENERATED[name](), path)
+        paths.append(str(path))
+    for threads in ("1", "3"):
+        env = dict(os.environ, PS26119_HOST_THREADS=threads)
+        r = subprocess.run([CLI, "info", *paths], capture_output=True, text=True, env=env, timeout=300)
+        assert r.returncode == 0, r.stderr
+        got = [ln.split()[-1] for ln in r.stdout.splitlines() if "presolve digest" in ln]
+        assert got == [ref.presolve_file(p)[0] for p in paths], threads
