@@ -209,11 +209,6 @@ def test_presolve_reuses_its_result_across_models(ref, tmp_path):
     assert got == want, list(zip(order, got, want))
 
 
-@pytest.fixture(scope="module")
-def postsolve_probe(host_probe):
-    return host_probe
-
-
 def _read_probe(path, count):
     raw = open(path, "rb").read()
     out, at = [], 0
@@ -238,7 +233,7 @@ def _same_bits(a, b):
     return a.shape == b.shape and np.array_equal(np.asarray(a).view(np.uint64), np.asarray(b).view(np.uint64))
 
 
-def test_postsolve_matches_reference(ref, tmp_path, postsolve_probe):
+def test_postsolve_matches_reference(ref, tmp_path, host_probe):
     """postsolve (csrc/solver.cpp) against the reference's (src/core/presolve.cpp:158-193) on the
     same presolved models and seeded reduced points: x, y, z and the objective bit for bit. The
     points include ones without x or without y (postsolve then clears what depends on them).
@@ -265,7 +260,7 @@ def test_postsolve_matches_reference(ref, tmp_path, postsolve_probe):
             want.append(ref.postsolve_file(path, lp.num_rows, lp.num_cols, rx, ry))
             names.append((name, variant))
     out = tmp_path / "out.bin"
-    r = subprocess.run([postsolve_probe, "postsolve", str(out), *args], capture_output=True, text=True, timeout=600)
+    r = subprocess.run([host_probe, "postsolve", str(out), *args], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr
     got = _read_probe(out, len(want))
     for (name, variant), w, o in zip(names, want, got):
