@@ -458,7 +458,7 @@ def run_ours(args, rank, world, local):
     z = torch.empty(n, dtype=torch.float64, device=dev)
     stream = torch.cuda.Stream(device=dev)
     limit = 0 if args.full else args.iterations
-    engine = {"presolve": False, "exact": False}
+    engine = {"presolve": False, "exact": args.reductions == "exact"}
 
     def step():
         r = ps26119.solve_lp_device(m, n, lp.sense, lp.offset, ptrs, precision=args.precision,
@@ -666,6 +666,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="random1m")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--reductions", choices=["exact", "fast"], default="fast",
+                    help="exact: every sum in the reference's order; fast: fixed-order trees")
     ap.add_argument("--iterations", type=int, default=6400, help="iteration cap of one step")
     ap.add_argument("--full", action="store_true", help="solve to 1e-8 in every step")
     ap.add_argument("--e2e-steps", type=int, default=2)

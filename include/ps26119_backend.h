@@ -108,6 +108,20 @@ PS26119_API int ps26119_backend_norm2_estimate(ps26119_backend* b, double* out);
 PS26119_API int ps26119_dot_noalloc(long long n, const double* a, const double* b, int exact, double* out,
                                     void* stream);
 
+/* Σ of the DEVICE vector t[0, n) in fp64, written to the host double *out (synchronises
+ * `stream`, a cudaStream_t; NULL = the legacy default stream).
+ *   order 0: one sequential chain, init + t[0] + t[1] + … — the order of the reference's host
+ *            loops (e.g. pdhg::kkt_general, src/pdhg/cpu_backend.cpp:226-284);
+ *   order 1: la::parallel_sum (src/la/parallel.h:169-188): 64 contiguous chunks, each summed in
+ *            order from 0, then init + part[0] + part[1] + … in order.
+ * exact = 1 returns exactly what that sequential evaluation returns, bit for bit (ties, signed
+ * zeros, infinities and NaN included); exact = 0 uses the engine's fixed-order tree (same result
+ * run to run, different rounding). No reference counterpart: it exposes the engine's reduction
+ * kernels to tests and to callers that need reference-order sums of device data.
+ * Returns 0, or a PS26119_* status with the reason in ps26119_backend_last_error(). */
+PS26119_API int ps26119_ordered_sum(long long n, const double* t, double init, int order, int exact, double* out,
+                                    void* stream);
+
 #ifdef __cplusplus
 }
 #endif

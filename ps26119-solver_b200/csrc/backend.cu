@@ -5,8 +5,11 @@
 // exact arithmetic the engine uses, fused forms included.
 #include <cmath>
 #include <memory>
+#include <string>
 #include <vector>
 
+#include "../../include/ps26119.h"
+#include "../../include/ps26119_backend.h"
 #include "checks.cuh"
 #include "engine.hpp"
 #include "problem.cuh"
@@ -281,3 +284,35 @@ std::unique_ptr<GpuBackend> GpuBackend::create(const HostModelView& M, const Sca
 }
 
 }  // namespace b200
+
+namespace b200 {
+void set_backend_error(const std::string& text);  // c_api.cpp: the thread's last-error text
+}
+
+// Σ of a device vector in one of the reference's two summation orders (see the header).
+extern "C" int ps26119_ordered_sum(long long n, const double* t, double init, int order, int exact, double* out,
+                                   void* stream) {
+  using namespace b200;
+  if (n < 0 || !out || (n > 0 && !t) || (order != 0 && order != 1)) {
+    set_backend_error("invalid arguments: n >= 0, t and out non-NULL, order 0 or 1");
+    return PS26119_INVALID_ARGUMENT;
+  }
+  try {
+    require_device();
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    DevBuf<double> d(1);
+    SumPlan p;
+    p.add(t, 0, n, init, order == 1 ? SumOrder::kChunk64 : SumOrder::kSeq, d.get());
+    p.build(exact != 0, nullptr, st);
+    p.launch(st);
+    B200_CHECK(cudaMemcpyAsync(out, d.get(), sizeof(double), cudaMemcpyDeviceToHost, st));
+    B200_CHECK(cudaStreamSynchronize(st));
+    return 0;
+  } catch (const std::bad_alloc&) {
+    set_backend_error("out of memory");
+    return PS26119_NOT_SOLVED;
+  } catch (const std::exception& e) {
+    set_backend_error(e.what());
+    return PS26119_NUMERICAL_ERROR;
+  }
+}

@@ -12,6 +12,7 @@
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
+#include <exception>
 #include <functional>
 #include <mutex>
 #include <system_error>
@@ -39,8 +40,9 @@ inline int host_thread_limit() {
 // Worker threads kept for the life of the process, so that a parallel section costs a wake-up
 // instead of creating and joining its threads (about 270 µs per section for 8 threads on an
 // 8-core host; a solve runs some 40 sections). One section uses the pool at a time: a section
-// started while the pool is busy (another thread's), or from inside a pool worker, returns
-// false from run() and its caller uses threads of its own. The pool is never destroyed (its
+// started while the pool is busy (another thread's), from inside a pool worker, or from inside
+// a section of the same calling thread returns false from run() and its caller uses threads of
+// its own. The pool is never destroyed (its
 // workers wait for work until the process ends), and a child process made by fork() starts a
 // new pool on first use, as the parent's workers do not exist there.
 class HostPool {
@@ -59,10 +61,17 @@ class HostPool {
 
   // Runs task(t) for every t in [0, T): t = 0 and any task no worker could be started for on the
   // calling thread, the others on workers. Returns when all have finished; false, having run
-  // nothing, when the pool is busy or the caller is one of its workers.
+  // nothing, when the pool is busy, the caller is one of its workers, or the caller is already
+  // inside a section of its own (a nested section). An exception thrown by a task is caught
+  // where it is thrown; run() still waits for every task, then rethrows the first one on the
+  // calling thread.
   bool run(int T, const std::function<void(int)>& task) {
-    if (in_worker() || !use_.try_lock()) return false;
+    if (in_worker() || in_section() || !use_.try_lock()) return false;
     std::lock_guard<std::mutex> own(use_, std::adopt_lock);
+    struct SectionFlag {
+      SectionFlag() { in_section() = true; }
+      ~SectionFlag() { in_section() = false; }
+    } flag;
     while (static_cast<int>(workers_.size()) < T - 1) {
       try {
         workers_.emplace_back(&HostPool::worker, this, static_cast<int>(workers_.size()) + 1);
@@ -76,14 +85,33 @@ class HostPool {
       task_ = &task;
       want_ = on_workers;
       pending_ = on_workers;
+      error_ = nullptr;
       ++gen_;
     }
     wake_.notify_all();
-    task(0);
-    for (int t = on_workers + 1; t < T; ++t) task(t);
-    std::unique_lock<std::mutex> lk(mu_);
-    idle_.wait(lk, [&] { return pending_ == 0; });
-    task_ = nullptr;
+    std::exception_ptr mine;
+    try {
+      task(0);
+    } catch (...) {
+      mine = std::current_exception();
+    }
+    for (int t = on_workers + 1; t < T; ++t) {
+      try {
+        task(t);
+      } catch (...) {
+        if (!mine) mine = std::current_exception();
+      }
+    }
+    std::exception_ptr theirs;
+    {
+      std::unique_lock<std::mutex> lk(mu_);
+      idle_.wait(lk, [&] { return pending_ == 0; });
+      task_ = nullptr;
+      theirs = error_;
+      error_ = nullptr;
+    }
+    if (mine) std::rethrow_exception(mine);
+    if (theirs) std::rethrow_exception(theirs);
     return true;
   }
 
@@ -97,6 +125,10 @@ class HostPool {
     static thread_local bool w = false;
     return w;
   }
+  static bool& in_section() {  // the calling thread owns the pool for a section
+    static thread_local bool s = false;
+    return s;
+  }
   void worker(int id) {  // id in 1 .. workers_.size()
     in_worker() = true;
     std::uint64_t seen = 0;
@@ -107,8 +139,14 @@ class HostPool {
       if (id > want_) continue;  // not part of this section
       const std::function<void(int)>* task = task_;
       lk.unlock();
-      (*task)(id);
+      std::exception_ptr err;
+      try {
+        (*task)(id);
+      } catch (...) {  // an exception must not leave the worker: it would end the process
+        err = std::current_exception();
+      }
       lk.lock();
+      if (err && !error_) error_ = err;
       if (--pending_ == 0) idle_.notify_one();
     }
   }
@@ -117,6 +155,7 @@ class HostPool {
   std::condition_variable wake_, idle_;
   std::uint64_t gen_ = 0;
   const std::function<void(int)>* task_ = nullptr;
+  std::exception_ptr error_;  // the first exception a worker caught in the current section
   int want_ = 0, pending_ = 0;
   std::vector<std::thread> workers_;
 };
@@ -132,11 +171,32 @@ void parallel_ranges(long long n, F&& f, long long min_parallel = 65536) {
   }
   const std::function<void(int)> task = [&](int t) { f(n * t / T, n * (t + 1) / T); };
   if (HostPool::instance().run(static_cast<int>(T), task)) return;
-  std::vector<std::thread> th;  // the pool is in use: threads of this section's own
+  // the pool is in use: threads of this section's own. Exceptions are caught where they are
+  // thrown; every thread is joined before the first one is rethrown on the calling thread.
+  std::mutex err_mu;
+  std::exception_ptr err;
+  auto guarded = [&](long long t) {
+    try {
+      f(n * t / T, n * (t + 1) / T);
+    } catch (...) {
+      std::lock_guard<std::mutex> lk(err_mu);
+      if (!err) err = std::current_exception();
+    }
+  };
+  std::vector<std::thread> th;
   th.reserve(static_cast<std::size_t>(T - 1));
-  for (long long t = 1; t < T; ++t) th.emplace_back([&, t] { f(n * t / T, n * (t + 1) / T); });
-  f(0LL, n / T);
+  long long started = 1;
+  for (; started < T; ++started) {
+    try {
+      th.emplace_back(guarded, started);
+    } catch (const std::system_error&) {
+      break;  // no more threads: the calling thread runs the remaining ranges
+    }
+  }
+  guarded(0);
+  for (long long t = started; t < T; ++t) guarded(t);
   for (auto& x : th) x.join();
+  if (err) std::rethrow_exception(err);
 }
 
 // One host-to-host copy of `bytes` bytes (non-overlapping buffers).

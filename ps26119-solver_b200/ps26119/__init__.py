@@ -112,6 +112,7 @@ EXPORTS = ["ps26119_version", "ps26119_default_options", "ps26119_solve_lp", "ps
            "ps26119_backend_fused_primal", "ps26119_backend_fused_dual", "ps26119_backend_kkt",
            "ps26119_backend_sync", "ps26119_backend_scaled_get", "ps26119_backend_scaled_structure",
            "ps26119_backend_scalars", "ps26119_backend_norm2_estimate", "ps26119_dot_noalloc",
+           "ps26119_ordered_sum",
            "ps26119_server_create", "ps26119_server_submit", "ps26119_server_poll", "ps26119_server_destroy"]
 
 _lib = None
@@ -172,6 +173,8 @@ def load(path: str | None = None):
     L.ps26119_backend_norm2_estimate.argtypes = [B, _D]
     L.ps26119_dot_noalloc.argtypes = [ctypes.c_longlong, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                       ctypes.c_void_p, ctypes.c_void_p]
+    L.ps26119_ordered_sum.argtypes = [ctypes.c_longlong, ctypes.c_void_p, ctypes.c_double, ctypes.c_int,
+                                      ctypes.c_int, _D, ctypes.c_void_p]
     L.ps26119_server_create.restype = ctypes.c_void_p
     L.ps26119_server_create.argtypes = [P(_ServerOptions)]
     L.ps26119_server_submit.restype = ctypes.c_longlong
@@ -186,6 +189,20 @@ def load(path: str | None = None):
 
 def version() -> str:
     return load().ps26119_version().decode()
+
+
+def ordered_sum(t_ptr: int, n: int, init: float = 0.0, order: str = "seq", exact: bool = True,
+                stream: int | None = None) -> float:
+    """Σ of a device vector of n doubles at address t_ptr, in the reference's order: "seq" (one
+    chain init + t[0] + t[1] + …) or "chunk64" (la::parallel_sum); exact=False takes the
+    engine's fast tree instead (ps26119_ordered_sum)."""
+    L = load()
+    out = ctypes.c_double(float("nan"))
+    rc = L.ps26119_ordered_sum(int(n), ctypes.c_void_p(t_ptr), float(init), 1 if order == "chunk64" else 0,
+                               int(bool(exact)), ctypes.byref(out), ctypes.c_void_p(stream) if stream else None)
+    if rc != 0:
+        raise RuntimeError(f"ps26119_ordered_sum: {L.ps26119_backend_last_error().decode()}")
+    return out.value
 
 
 @dataclass

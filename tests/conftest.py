@@ -10,7 +10,10 @@ for p in (os.path.join(ROOT, "ps26119-solver_b200"), os.path.join(ROOT, "oracle"
     if p not in sys.path:
         sys.path.insert(0, p)
 
-REFERENCE_DATA = "/root/reference/data"  # present only where the reference sources are mounted
+# The reference sources ($PS26119_REFERENCE_DIR, else a "reference" directory beside this repository);
+# their data files are present only where the sources are mounted.
+REFERENCE_DIR = os.environ.get("PS26119_REFERENCE_DIR") or os.path.join(os.path.dirname(ROOT), "reference")
+REFERENCE_DATA = os.path.join(REFERENCE_DIR, "data")
 
 
 def pytest_configure(config):

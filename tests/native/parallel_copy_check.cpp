@@ -3,7 +3,8 @@
 // guard bytes on both sides of every destination; size_for_copy keeps or replaces a buffer as
 // documented; parallel_ranges covers every index exactly once when sections run from several
 // threads at once (all but one fall back to threads of their own), when a section is started
-// inside another, and in a child process made by fork() after the pool has started. Prints "ok"
+// inside another, in a child process made by fork() after the pool has started, and when a range
+// throws (the exception reaches the caller after every range has run). Prints "ok"
 // and exits 0, or names the first failure and exits 1.
 #include <sys/wait.h>
 #include <unistd.h>
@@ -12,6 +13,7 @@
 #include <cstdio>
 #include <cstring>
 #include <random>
+#include <stdexcept>
 #include <thread>
 #include <vector>
 
@@ -89,6 +91,29 @@ int main() {
   if (inner.load() != 70000 * T) {
     std::printf("nested sections: %lld\n", inner.load());
     return 1;
+  }
+  // an exception thrown in one range reaches the caller (pool path and own-threads path), every
+  // range still runs, and the next section covers every index
+  for (int nested = 0; nested < 2; ++nested) {
+    std::atomic<long long> visited{0};
+    bool caught = false;
+    auto throwing = [&] {
+      parallel_ranges(200000, [&](long long b, long long e) {
+        visited += e - b;
+        if (b <= 150000 && 150000 < e) throw std::runtime_error("planted");
+      });
+    };
+    try {
+      if (nested) parallel_ranges(70000, [&](long long b, long long) { if (b == 0) throwing(); });
+      else throwing();
+    } catch (const std::runtime_error& e) {
+      caught = std::strcmp(e.what(), "planted") == 0;
+    }
+    if (!caught || visited.load() != 200000 || !covers(90001) || !covers(70000)) {
+      std::printf("exception from a range (nested %d): caught %d, visited %lld\n", nested, caught ? 1 : 0,
+                  visited.load());
+      return 1;
+    }
   }
   const pid_t pid = fork();
   if (pid == 0) _exit(covers(123457) && covers(70001) ? 0 : 1);  // the child's own pool
