@@ -126,8 +126,10 @@ int ref_solve(int m, int n, int sense, double offset, const double* c, const dou
   if (time_limit > 0) o.time_limit = time_limit;
   if (check_every > 0) o.termination_check_every = check_every;
   for (int k = 0; k < n_params; ++k) {
-    // "algorithm" is this shim's own switch (2 = PDLP), not an engine parameter
+    // "algorithm" (2 = PDLP) and "use_gpu" (the reference's CUDA backend, in the library built
+    // with it) are this shim's own switches, not engine parameters
     if (std::string(names[k]) == "algorithm") o.algorithm = values[k] == 2 ? Algorithm::Pdlp : Algorithm::R2hpdhg;
+    else if (std::string(names[k]) == "use_gpu") o.use_gpu = values[k] != 0;
     else o.engine_params.emplace_back(names[k], values[k]);
   }
   if (warm_x) o.warm_x.assign(warm_x, warm_x + n);

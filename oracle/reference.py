@@ -21,6 +21,8 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_ref", "libps26119_ref.so")
+# the same reference built with its own CUDA backend (src/gpu/cuda_backend.cu, sm_100a)
+LIB_GPU_PATH = os.path.join(HERE, "_ref", "libps26119_refgpu.so")
 
 STATUS = ["Optimal", "Infeasible", "Unbounded", "IterationLimit", "TimeLimit", "NumericalError", "NotSolved"]
 INFO = ["status", "objective", "dual_objective", "primal_residual", "dual_residual", "gap", "iterations", "seconds",
@@ -28,19 +30,24 @@ INFO = ["status", "objective", "dual_objective", "primal_residual", "dual_residu
 
 _D = ctypes.POINTER(ctypes.c_double)
 _I = ctypes.POINTER(ctypes.c_int)
-_lib = None
+_libs = {}
 
 
 def available() -> bool:
     return os.path.exists(LIB_PATH)
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        if not available():
-            raise FileNotFoundError(f"{LIB_PATH} not built (make -C oracle ref)")
-        L = ctypes.CDLL(LIB_PATH)
+def available_gpu() -> bool:
+    return os.path.exists(LIB_GPU_PATH)
+
+
+def lib(gpu: bool = False):
+    key = bool(gpu)
+    if key not in _libs:
+        path = LIB_GPU_PATH if gpu else LIB_PATH
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} not built (make -C oracle {'ref_gpu' if gpu else 'ref'})")
+        L = ctypes.CDLL(path)
         model = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, _D, _D, _D, _D, _D, _I, _I, _D]
         L.ref_solve.argtypes = model + [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                         ctypes.c_longlong, ctypes.c_double, ctypes.c_int, ctypes.c_int,
@@ -98,8 +105,8 @@ def lib():
                                          _D, ctypes.POINTER(ctypes.c_longlong)]
         L.ref_certificate.argtypes = [ctypes.c_int] + model + [_D, _D, _D]
         L.ps26119_solve_lp.argtypes = None  # the reference's own C API, used by bench.py
-        _lib = L
-    return _lib
+        _libs[key] = L
+    return _libs[key]
 
 
 def _d(a):
@@ -144,14 +151,18 @@ class RefSolution:
 
 
 def solve(lp, presolve=False, precision="fp64", threads=1, tol=0.0, iteration_limit=0, time_limit=0.0,
-          check_every=0, params=None, warm_x=None, warm_y=None, algorithm="r2hpdhg") -> RefSolution:
-    """ps26119::solve with algorithm r2hpdhg (or pdlp) on the CPU (reference src/core/solve.cpp:194)."""
-    L = lib()
+          check_every=0, params=None, warm_x=None, warm_y=None, algorithm="r2hpdhg", gpu=False) -> RefSolution:
+    """ps26119::solve with algorithm r2hpdhg (or pdlp) on the CPU (reference src/core/solve.cpp:194);
+    gpu=True: the reference's own CUDA backend (Options::use_gpu, its library built with
+    src/gpu/cuda_backend.cu)."""
+    L = lib(gpu)
     args, keep = _model_args(lp)
     m, n = lp.num_rows, lp.num_cols
     params = list((params or {}).items())
     if algorithm == "pdlp":
         params.append(("algorithm", 2.0))
+    if gpu:
+        params.append(("use_gpu", 1.0))
     names = (ctypes.c_char_p * max(1, len(params)))(*[k.encode() for k, _ in params])
     vals = np.array([v for _, v in params] or [0.0], dtype=np.float64)
     wx = None if warm_x is None else np.ascontiguousarray(warm_x, dtype=np.float64)

@@ -129,9 +129,19 @@ class Engine {
 
   EngineResult run(const DeviceOutputs& out);
   EngineResult run_pdlp(const DeviceOutputs& out);
+  // Bulk-copy waits of this solve's kernels that ran out (synchronises the stream).
+  unsigned stage_errors() {
+    unsigned v = 0;
+    if (stage_err_.get()) {
+      B200_CHECK(cudaMemcpyAsync(&v, stage_err_.get(), sizeof v, cudaMemcpyDeviceToHost, st_));
+      B200_CHECK(cudaStreamSynchronize(st_));
+    }
+    return v;
+  }
 
  private:
   using clock = std::chrono::steady_clock;
+  unsigned* err() { return stage_err_.get(); }
   double elapsed() const { return std::chrono::duration<double>(clock::now() - t0_).count(); }
 
   template <class T> IterVecs<T>& vecs();
@@ -171,6 +181,7 @@ class Engine {
   DeviceModel M_;
   const EngineOptions& o_;
   cudaStream_t st_;
+  DevBuf<unsigned> stage_err_;  // this solve's bulk-copy timeouts (see count_stage_timeout)
   clock::time_point t0_;
   ScaledDevice sp_;
   IterVecs<double> vd_;
@@ -213,9 +224,11 @@ template <> IterVecs<float>& Engine::vecs<float>() { return vf_; }
 #define B200_COUNT(k) (capturing_ ? capture_count_ += (k) : kernels_ += (k))
 
 void Engine::setup() {
+  stage_err_.alloc(1);
+  B200_CHECK(cudaMemsetAsync(stage_err_.get(), 0, sizeof(unsigned), st_));
   sp_.build(M_, o_.scaling, o_.exact, st_);
   if (o_.mixed) sp_.make_f32(st_);
-  const double norm = sp_.lanczos(st_);
+  const double norm = sp_.lanczos(st_, err());
   eta_ = norm > 0 ? 0.998 / norm : 1.0;  // engine.cpp:203-204
   kernels_ += sp_.kernels;
   const int m = M_.m, n = M_.n;
@@ -306,7 +319,7 @@ void Engine::launch_residual(bool with_restart_terms, const int* skip, SumPlan& 
   B200_LAUNCH_CHECK();
   EpiResY<T> e{v.yb.get(), v.yh.get(), v.y0.get(), v.dy.get(), v.adx.get(), py, cross,
                with_restart_terms ? dyn : nullptr, skip};
-  launch_slab_tma<T>(m, sp_.a_rp.get(), sp_.a_col.get(), sp_.A_val<T>(), v.dx.get(), e, st_);
+  launch_slab_tma<T>(m, sp_.a_rp.get(), sp_.a_col.get(), sp_.A_val<T>(), v.dx.get(), e, st_, nullptr, err());
   plan.launch(st_);
   B200_COUNT(2 + plan.kernel_count());
 }
@@ -316,10 +329,10 @@ void Engine::launch_kkt_original() {
   const long long L = static_cast<long long>(m) + n;
   double* K0 = kt_.get();
   EpiKktRows er{{}, yo_.get(), M_.row_lower, M_.row_upper, K0, K0 + L, K0 + 2 * L, res_.get()};
-  launch_slab_tma<double>(m, sp_.a_rp.get(), sp_.a_col.get(), sp_.a_v0.get(), xo_.get(), er, st_);
+  launch_slab_tma<double>(m, sp_.a_rp.get(), sp_.a_col.get(), sp_.a_v0.get(), xo_.get(), er, st_, nullptr, err());
   EpiKktCols ec{{}, xo_.get(), M_.c, M_.col_lower, M_.col_upper, static_cast<double>(M_.sense), m,
                 K0 + 3 * L, K0 + L, K0 + 2 * L, res_.get()};
-  launch_slab<double>(n, M_.col_start, M_.row_index, M_.value, yo_.get(), ec, st_);
+  launch_slab<double>(n, M_.col_start, M_.row_index, M_.value, yo_.get(), ec, st_, nullptr, err());
   plan_kkt_.launch(st_);
   B200_COUNT(2 + plan_kkt_.kernel_count());
 }
@@ -351,7 +364,7 @@ void Engine::launch_ray(const T* dx, const T* dy, double* r, double* d, int drif
                                               T0 + L, T0 + 2 * L, T0 + 2 * L + n, res_.get(), s_dviol);
   B200_LAUNCH_CHECK();
   EpiRayRows er{{}, r, M_.row_lower, M_.row_upper, T0, T0 + L, res_.get(), s_pviol};
-  launch_slab_tma<double>(m, sp_.a_rp.get(), sp_.a_col.get(), sp_.a_v0.get(), d, er, st_);
+  launch_slab_tma<double>(m, sp_.a_rp.get(), sp_.a_col.get(), sp_.a_v0.get(), d, er, st_, nullptr, err());
   SumPlan& p = drift ? plan_ray2_ : plan_ray1_;
   p.launch(st_);
   B200_COUNT(4 + p.kernel_count());
@@ -373,11 +386,15 @@ void Engine::capture_epoch() {
   capture_count_ = 0;
   auto capture_scope = std::make_unique<CaptureScope>();  // no device-wide syncs elsewhere meanwhile
   B200_CHECK(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
+  // Programmatic dependent launch for every iteration kernel whose predecessor in the stream is
+  // another iteration kernel (not the first kernel of the epoch, nor the one after the residual).
   auto step = [&](int s) {
     EpiPrimal<T> ep{v.x.get(), v.xh.get(), v.xb.get(), v.x0.get(), sp_.c<T>(), sp_.l<T>(), sp_.u<T>(), P, s, 0, 0, 0};
-    launch_slab_fed<T>(n, sp_.t_rp.get(), sp_.t_ri.get(), sp_.At_val<T>(), v.y.get(), ep, st_, slab_t_.get(), cap_t_);
+    launch_slab_fed<T>(n, sp_.t_rp.get(), sp_.t_ri.get(), sp_.At_val<T>(), v.y.get(), ep, st_, slab_t_.get(), cap_t_,
+                       err(), s >= 2);
     EpiDual<T> ed{v.y.get(), v.yh.get(), v.yb.get(), v.y0.get(), sp_.rl<T>(), sp_.ru<T>(), P, s, 0, 0, 0, 0};
-    launch_slab_fed<T>(m, sp_.a_rp.get(), sp_.a_col.get(), sp_.A_val<T>(), v.xb.get(), ed, st_, slab_a_.get(), cap_a_);
+    launch_slab_fed<T>(m, sp_.a_rp.get(), sp_.a_col.get(), sp_.A_val<T>(), v.xb.get(), ed, st_, slab_a_.get(), cap_a_,
+                       err(), true);
     capture_count_ += 2;
   };
   B200_CHECK(cudaEventRecordWithFlags(ev_[0], st_, cudaEventRecordExternal));
@@ -592,11 +609,11 @@ void Engine::finish_p(EngineResult& R, Status status, const T* xs, const T* ys, 
   // in-process check (solution_checker.cpp:61-133) on xo and y_min = yo
   double c_scale = std_max(1.0, sp_.c_inf);
   EpiCheckRows cr{{}, yo_.get(), M_.row_lower, M_.row_upper, c_scale, objt_.get() + n, res_.get()};
-  launch_slab_tma<double>(m, sp_.a_rp.get(), sp_.a_col.get(), sp_.a_v0.get(), xo_.get(), cr, st_);
+  launch_slab_tma<double>(m, sp_.a_rp.get(), sp_.a_col.get(), sp_.a_v0.get(), xo_.get(), cr, st_, nullptr, err());
   // t_primal lands in objt_[0, n): the objective terms were consumed by plan_obj_ above
   EpiCheckCols cc{{}, xo_.get(), M_.c, M_.col_lower, M_.col_upper, static_cast<double>(M_.sense), c_scale, m,
                   objt_.get() + n, objt_.get(), res_.get()};
-  launch_slab<double>(n, M_.col_start, M_.row_index, M_.value, yo_.get(), cc, st_);
+  launch_slab<double>(n, M_.col_start, M_.row_index, M_.value, yo_.get(), cc, st_, nullptr, err());
   plan_chk_.launch(st_);
   kernels_ += 3 + plan_obj_.kernel_count() + plan_chk_.kernel_count();
   // outputs
@@ -883,9 +900,11 @@ void Engine::capture_pdlp_epoch(int phase) {
     T* yc = odd ? v.yh.get() : v.y.get();
     T* yn = odd ? v.y.get() : v.yh.get();
     EpiPdlpPrimal<T> ep{xc, sp_.c<T>(), sp_.l<T>(), sp_.u<T>(), xn, v.xb.get(), v.dx.get(), P, s};
-    launch_slab_fed<T>(n, sp_.t_rp.get(), sp_.t_ri.get(), sp_.At_val<T>(), yc, ep, st_, slab_t_.get(), cap_t_);
+    launch_slab_fed<T>(n, sp_.t_rp.get(), sp_.t_ri.get(), sp_.At_val<T>(), yc, ep, st_, slab_t_.get(), cap_t_, err(),
+                       s >= 1);
     EpiPdlpDual<T> ed{yc, sp_.rl<T>(), sp_.ru<T>(), yn, v.dy.get(), P, s};
-    launch_slab_fed<T>(m, sp_.a_rp.get(), sp_.a_col.get(), sp_.A_val<T>(), v.xb.get(), ed, st_, slab_a_.get(), cap_a_);
+    launch_slab_fed<T>(m, sp_.a_rp.get(), sp_.a_col.get(), sp_.A_val<T>(), v.xb.get(), ed, st_, slab_a_.get(), cap_a_,
+                       err(), true);
     capture_count_ += 2;
   }
   B200_CHECK(cudaEventRecordWithFlags(ev_[1], st_, cudaEventRecordExternal));
@@ -1170,16 +1189,17 @@ EngineResult run_engine(const DeviceModel& M, const EngineOptions& opt, const De
       if (own) cudaStreamDestroy(s);
     }
   } guard{st, own};
-  const unsigned timeouts = stage_timeouts();
   EngineResult R;
+  unsigned timeouts = 0;
   {
     auto e = std::make_unique<Engine>(M, opt, st);
     R = opt.pdlp ? e->run_pdlp(out) : e->run(out);
+    timeouts = e->stage_errors();
     const auto t = std::chrono::steady_clock::now();
     e.reset();
     R.teardown_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t).count();
   }
-  if (stage_timeouts() != timeouts) throw CudaError("a shared-memory staging wait timed out on the device");
+  if (timeouts) throw CudaError("a shared-memory staging wait timed out on the device");
   return R;
 }
 

@@ -220,7 +220,7 @@ struct ScaledDevice {
   // stream, generated and normalised on the host in the reference's order; the products run
   // on the device; α and β are reduced in the selected order and brought back each step for
   // the Sturm-bisection on the host.
-  double lanczos(cudaStream_t st) {
+  double lanczos(cudaStream_t st, unsigned* err = nullptr) {
     if (n == 0 || nnz == 0) return 0.0;
     const int K = 400;
     const double rel_tol = 1e-12;
@@ -247,8 +247,10 @@ struct ScaledDevice {
     double theta = 0, theta_old = -1;
     int stagnant = 0;
     for (int k = 0; k < K; ++k) {
-      launch_slab_tma<double>(m, a_rp.get(), a_col.get(), sa.get(), v.get(), EpiStore<double>{{}, t.get()}, st);
-      launch_slab_tma<double>(n, M.col_start, t_ri.get(), sat.get(), t.get(), EpiStore<double>{{}, w.get()}, st);
+      launch_slab_tma<double>(m, a_rp.get(), a_col.get(), sa.get(), v.get(), EpiStore<double>{{}, t.get()}, st, nullptr,
+                              err);
+      launch_slab_tma<double>(n, M.col_start, t_ri.get(), sat.get(), t.get(), EpiStore<double>{{}, w.get()}, st, nullptr,
+                              err);
       k_prod_terms<<<grid_for(n), kBlock, 0, st>>>(n, w.get(), v.get(), terms.get());
       B200_LAUNCH_CHECK();
       pal.launch(st);

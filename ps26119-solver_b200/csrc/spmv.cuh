@@ -76,8 +76,20 @@ struct SlabSmem {
   alignas(8) unsigned long long bar;
 };
 
-// Bulk-copy waits that ran out (a counter the host reads after a solve; never expected to move).
+// Bulk-copy waits that ran out (never expected to move). Each launch counts into the counter it is
+// given (a solve passes its own, so a timeout is reported by the solve it happened in); launches
+// given none count into this process-wide one.
 static __device__ unsigned int g_stage_timeouts;
+__device__ __forceinline__ void count_stage_timeout(unsigned* err) { atomicAdd(err ? err : &g_stage_timeouts, 1u); }
+
+// Programmatic dependent launch (sm_90+): a kernel launched with the programmatic-serialisation
+// attribute may start while the kernel before it in the stream is still running; it must not
+// touch that kernel's outputs (or anything a kernel still running may read or write) before
+// pdl_wait(), which returns once every earlier kernel has completed and its writes are visible.
+// pdl_allow_next() lets the next such kernel be scheduled once every block of this one has issued
+// it. In a kernel launched without the attribute both are no-ops.
+__device__ __forceinline__ void pdl_allow_next() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
   return static_cast<unsigned>(__cvta_generic_to_shared(p));
@@ -236,7 +248,7 @@ __global__ void __launch_bounds__(kSlabRows, B200_SLAB_MIN_BLOCKS) k_slab(int ro
                                                         const int* __restrict__ col,
                                                         const T* __restrict__ val,
                                                         const T* __restrict__ x, Epi epi,
-                                                        const int2* __restrict__ slab) {
+                                                        const int2* __restrict__ slab, unsigned* err) {
   __shared__ SlabSmem<T> sm;
   if (!epi.active()) return;
   const int r0 = blockIdx.x * kSlabRows;
@@ -282,7 +294,7 @@ __global__ void __launch_bounds__(kSlabRows, B200_SLAB_MIN_BLOCKS) k_slab(int ro
       phase ^= 1u;
       if (!__syncthreads_and(ok)) {  // never expected: record, drain, give up on the tile
         if (threadIdx.x == 0) {
-          atomicAdd(&g_stage_timeouts, 1u);
+          count_stage_timeout(err);
           mbar_wait_bounded(&sm.bar, phase ^ 1u);
         }
         staged = false;
@@ -326,11 +338,18 @@ __global__ void __launch_bounds__(kSlabRows, B200_SLAB_MIN_BLOCKS) k_slab(int ro
 // ---------------------------------------------------------------------- fully staged form
 // k_slab_fed: the row products and epilogue of k_slab, with every streamed operand of the slab
 // brought in by TMA bulk copies issued at block entry: the slab's row pointers and the
-// epilogue's per-row operand vectors (Epi::vec(k), rows r0 … r0+nr) on one barrier, the col/val
-// tile on another. Threads hold no operand registers while the gathers are in flight (lower
-// register use), and the start of a slab waits on one DRAM round trip (the copies, all issued
-// together) instead of a chain of them. The slab's nonzero range comes from the L2-resident slab
-// table. Sums are k_slab's sequential CSR-order sums.
+// epilogue's per-row operand vectors (Epi::vec(k), rows r0 … r0+nr), and the col/val tile.
+// Threads hold no operand registers while the gathers are in flight (lower register use), and
+// the start of a slab waits on one DRAM round trip (the copies, all issued together) instead of
+// a chain of them. The slab's nonzero range comes from the L2-resident slab table. Sums are
+// k_slab's sequential CSR-order sums.
+//
+// Launched back to back with programmatic dependent launch (the iteration kernels of an epoch),
+// a block may start while the previous kernel's last blocks still run. Everything that no kernel
+// of the epoch writes — the matrix, the row pointers, the slab table and the epilogue vectors
+// outside Epi::kLiveVecs (bit k: vec(k) is written by the iteration kernels) — is requested
+// before pdl_wait(); the live vectors and the gathered x are touched only after it, and so is
+// every store. Without the launch attribute pdl_wait() returns at once.
 //
 // The tile capacity `cap` is chosen per matrix (the largest slab, rounded up; see
 // fed_tile_capacity) and the shared memory is sized to it: the gathers' outstanding L1 misses
@@ -342,7 +361,7 @@ __global__ void __launch_bounds__(kSlabRows, B200_SLAB_MIN_BLOCKS) k_slab(int ro
 struct FedLayout {
   unsigned rp, vec, col, val, bytes;  // byte offsets into the dynamic shared memory, and its size
 };
-// bar[2] (16 bytes) and the slab's nonzero range (8 bytes) come first.
+// bar[3] (24 bytes) and the slab's nonzero range (8 bytes) come first.
 __host__ __device__ constexpr FedLayout fed_layout(int vecs, int elem, int cap) {
   const unsigned rp = 32u;
   const unsigned vec = rp + static_cast<unsigned>(kSlabRows + kTilePad) * 4u;
@@ -367,14 +386,18 @@ __global__ void __launch_bounds__(kSlabRows, B200_FED_MIN_BLOCKS) k_slab_fed(int
                                                            const int* __restrict__ col,
                                                            const T* __restrict__ val,
                                                            const T* __restrict__ x, Epi epi,
-                                                           const int2* __restrict__ slab, int cap) {
+                                                           const int2* __restrict__ slab, int cap, unsigned* err) {
   constexpr int V = Epi::kVecs;
+  constexpr unsigned kLive = Epi::kLiveVecs;
+  constexpr int kNumLive = __builtin_popcount(kLive);
   constexpr int kValAlign = 16 / static_cast<int>(sizeof(T));
   extern __shared__ __align__(16) unsigned char fed_smem[];
+  pdl_allow_next();
   if (!epi.active()) return;
   const FedLayout L = fed_layout(V, static_cast<int>(sizeof(T)), cap);
-  unsigned long long* bar = reinterpret_cast<unsigned long long*>(fed_smem);  // [0] rp + vectors, [1] tile
-  int2* krange = reinterpret_cast<int2*>(fed_smem + 16);
+  // [0] row pointers + constant vectors, [1] tile, [2] live vectors (after pdl_wait)
+  unsigned long long* bar = reinterpret_cast<unsigned long long*>(fed_smem);
+  int2* krange = reinterpret_cast<int2*>(fed_smem + 24);
   int* s_rp = reinterpret_cast<int*>(fed_smem + L.rp);
   T* s_vec = reinterpret_cast<T*>(fed_smem + L.vec);
   int* s_col = reinterpret_cast<int*>(fed_smem + L.col);
@@ -382,24 +405,26 @@ __global__ void __launch_bounds__(kSlabRows, B200_FED_MIN_BLOCKS) k_slab_fed(int
   const int tid = static_cast<int>(threadIdx.x);
   const int r0 = blockIdx.x * kSlabRows;
   const int nr = min(kSlabRows, rows - r0);
+  const unsigned vb = (static_cast<unsigned>(nr) * sizeof(T) + 15u) & ~15u;
   auto issue_tile = [&](int t0, int t1) {  // thread 0
     const int c0 = t0 & ~3, v0 = t0 & ~(kValAlign - 1);
     const int c1 = (t1 + 3) & ~3, v1 = (t1 + kValAlign - 1) & ~(kValAlign - 1);
-    const unsigned cb = static_cast<unsigned>(c1 - c0) * 4u, vb = static_cast<unsigned>(v1 - v0) * sizeof(T);
-    mbar_expect_tx(&bar[1], cb + vb);
+    const unsigned cb = static_cast<unsigned>(c1 - c0) * 4u, tb = static_cast<unsigned>(v1 - v0) * sizeof(T);
+    mbar_expect_tx(&bar[1], cb + tb);
     tma_load_1d(s_col, col + c0, cb, &bar[1]);
-    tma_load_1d(s_val, val + v0, vb, &bar[1]);
+    tma_load_1d(s_val, val + v0, tb, &bar[1]);
   };
   bool tile_pending = false;  // thread 0: a tile copy not yet waited for
   if (tid == 0) {
     mbar_init(&bar[0]);
     mbar_init(&bar[1]);
+    mbar_init(&bar[2]);
     const unsigned rb = (static_cast<unsigned>(nr + 1) * 4u + 15u) & ~15u;
-    const unsigned vb = (static_cast<unsigned>(nr) * sizeof(T) + 15u) & ~15u;
-    mbar_expect_tx(&bar[0], rb + V * vb);
+    mbar_expect_tx(&bar[0], rb + static_cast<unsigned>(V - kNumLive) * vb);
     tma_load_1d(s_rp, rp + r0, rb, &bar[0]);
 #pragma unroll
-    for (int k = 0; k < V; ++k) tma_load_1d(s_vec + k * kSlabRows, epi.vec(k) + r0, vb, &bar[0]);
+    for (int k = 0; k < V; ++k)
+      if (!((kLive >> k) & 1u)) tma_load_1d(s_vec + k * kSlabRows, epi.vec(k) + r0, vb, &bar[0]);
     const int2 kr = slab ? ld_keep(slab + blockIdx.x) : make_int2(__ldg(rp + r0), __ldg(rp + r0 + nr));
     *krange = kr;
     if (kr.x < kr.y) {
@@ -407,8 +432,18 @@ __global__ void __launch_bounds__(kSlabRows, B200_FED_MIN_BLOCKS) k_slab_fed(int
       tile_pending = true;
     }
   }
+  pdl_wait();  // from here on the previous kernels' outputs are complete and visible
   int ok = 1;
-  if (tid == 0) ok = mbar_wait_bounded(&bar[0], 0) ? 1 : 0;
+  if (tid == 0) {
+    if (kNumLive > 0) {
+      mbar_expect_tx(&bar[2], static_cast<unsigned>(kNumLive) * vb);
+#pragma unroll
+      for (int k = 0; k < V; ++k)
+        if ((kLive >> k) & 1u) tma_load_1d(s_vec + k * kSlabRows, epi.vec(k) + r0, vb, &bar[2]);
+    }
+    ok = mbar_wait_bounded(&bar[0], 0) ? 1 : 0;
+    if (kNumLive > 0) ok = (mbar_wait_bounded(&bar[2], 0) && ok) ? 1 : 0;
+  }
   bool staged = __syncthreads_and(ok) != 0;
   const int2 kr = *krange;
   const bool mine = tid < nr;
@@ -449,8 +484,9 @@ __global__ void __launch_bounds__(kSlabRows, B200_FED_MIN_BLOCKS) k_slab_fed(int
   }
   if (!staged) {  // never expected: record, wait (bounded) for copies still in flight, report NaN
     if (tid == 0) {
-      atomicAdd(&g_stage_timeouts, 1u);
+      count_stage_timeout(err);
       mbar_wait_bounded(&bar[0], 0);
+      if (kNumLive > 0) mbar_wait_bounded(&bar[2], 0);
       if (tile_pending) mbar_wait_bounded(&bar[1], phase);
     }
     s = __longlong_as_double(0x7ff8000000000000LL);
@@ -478,37 +514,58 @@ inline void slab_prepare() {
 
 template <class T, class Epi, bool kTma = false>
 inline void launch_slab(int rows, const int* rp, const int* col, const T* val, const T* x, const Epi& epi,
-                        cudaStream_t st, const int2* slab = nullptr) {
+                        cudaStream_t st, const int2* slab = nullptr, unsigned* err = nullptr) {
   if (rows <= 0) return;
   slab_prepare<T, Epi, kTma>();
   const int grid = (rows + kSlabRows - 1) / kSlabRows;
-  k_slab<T, Epi, kTma><<<grid, kSlabRows, 0, st>>>(rows, rp, col, val, x, epi, slab);
+  k_slab<T, Epi, kTma><<<grid, kSlabRows, 0, st>>>(rows, rp, col, val, x, epi, slab, err);
   B200_LAUNCH_CHECK();
 }
 
 // The TMA-staged form, for CSR arrays allocated by this library (tail-padded DevBufs). `slab`:
-// an optional table of each slab's nonzero range (see slab_table).
+// an optional table of each slab's nonzero range (see slab_table). `err`: the bulk-copy timeout
+// counter (nullptr: the process-wide one).
 template <class T, class Epi>
 inline void launch_slab_tma(int rows, const int* rp, const int* col, const T* val, const T* x, const Epi& epi,
-                            cudaStream_t st, const int2* slab = nullptr) {
-  launch_slab<T, Epi, B200_STAGE_TMA != 0>(rows, rp, col, val, x, epi, st, B200_SLAB_TABLE ? slab : nullptr);
+                            cudaStream_t st, const int2* slab = nullptr, unsigned* err = nullptr) {
+  launch_slab<T, Epi, B200_STAGE_TMA != 0>(rows, rp, col, val, x, epi, st, B200_SLAB_TABLE ? slab : nullptr, err);
 }
 
 // The fully staged form (k_slab_fed) for the iteration epilogues, whose operand vectors are
 // library allocations; `rp` must be one too, `slab` the slab table of rp and `cap` the tile
 // capacity from fed_tile_capacity. Falls back to launch_slab_tma when an operand is not 16-byte
-// aligned or the shared memory would exceed the 48 KB that needs no opt-in.
+// aligned or the shared memory would exceed the 48 KB that needs no opt-in. `pdl`: launch with
+// programmatic dependent launch (B200_PDL builds), so the kernel's blocks may start while the
+// previous kernel of the stream finishes: only where Epi::kLiveVecs names every operand vector a
+// kernel still in flight may write. The fallback never uses it.
+#ifndef B200_PDL
+#define B200_PDL 1
+#endif
 template <class T, class Epi>
 inline void launch_slab_fed(int rows, const int* rp, const int* col, const T* val, const T* x, const Epi& epi,
-                            cudaStream_t st, const int2* slab, int cap) {
+                            cudaStream_t st, const int2* slab, int cap, unsigned* err = nullptr, bool pdl = false) {
   if (rows <= 0) return;
   const FedLayout L = fed_layout(Epi::kVecs, static_cast<int>(sizeof(T)), cap);
   bool ok = B200_SLAB_FED && B200_STAGE_TMA && cap >= 16 && cap % 16 == 0 && L.bytes <= 48u * 1024u &&
             (reinterpret_cast<std::uintptr_t>(rp) & 15u) == 0;
   for (int k = 0; k < Epi::kVecs; ++k) ok = ok && (reinterpret_cast<std::uintptr_t>(epi.vec(k)) & 15u) == 0;
-  if (!ok) return launch_slab_tma<T>(rows, rp, col, val, x, epi, st, slab);
+  if (!ok) return launch_slab_tma<T>(rows, rp, col, val, x, epi, st, slab, err);
   const int grid = (rows + kSlabRows - 1) / kSlabRows;
-  k_slab_fed<T, Epi><<<grid, kSlabRows, L.bytes, st>>>(rows, rp, col, val, x, epi, slab, cap);
+  if (B200_PDL && pdl) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(static_cast<unsigned>(grid));
+    cfg.blockDim = dim3(kSlabRows);
+    cfg.dynamicSmemBytes = L.bytes;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    B200_CHECK(cudaLaunchKernelEx(&cfg, k_slab_fed<T, Epi>, rows, rp, col, val, x, epi, slab, cap, err));
+    return;
+  }
+  k_slab_fed<T, Epi><<<grid, kSlabRows, L.bytes, st>>>(rows, rp, col, val, x, epi, slab, cap, err);
   B200_LAUNCH_CHECK();
 }
 
@@ -600,8 +657,10 @@ struct EpiPrimal {
   __device__ Pre load(int j) const {
     return Pre{ld_stream(x + j), ld_stream(x0 + j), ld_stream(c + j), ld_stream(l + j), ld_stream(u + j)};
   }
-  // The streamed operands as arrays (k_slab_fed stages their slab ranges in shared memory).
+  // The streamed operands as arrays (k_slab_fed stages their slab ranges in shared memory);
+  // x is written by the primal kernel of the previous step (live), the others only between epochs.
   static constexpr int kVecs = 5;
+  static constexpr unsigned kLiveVecs = 0x1u;
   __host__ __device__ const T* vec(int k) const { return k == 0 ? x : k == 1 ? x0 : k == 2 ? c : k == 3 ? l : u; }
   __device__ Pre pre_at(const T* sv, int t) const {
     return Pre{sv[t], sv[kSlabRows + t], sv[2 * kSlabRows + t], sv[3 * kSlabRows + t], sv[4 * kSlabRows + t]};
@@ -641,6 +700,7 @@ struct EpiDual {
   __device__ bool active() const { return P == nullptr || !P->done; }
   __device__ Pre load(int i) const { return Pre{ld_stream(y + i), ld_stream(y0 + i), ld_stream(rl + i), ld_stream(ru + i)}; }
   static constexpr int kVecs = 4;
+  static constexpr unsigned kLiveVecs = 0x1u;  // y (the dual kernel of the previous step writes it)
   __host__ __device__ const T* vec(int k) const { return k == 0 ? y : k == 1 ? y0 : k == 2 ? rl : ru; }
   __device__ Pre pre_at(const T* sv, int t) const {
     return Pre{sv[t], sv[kSlabRows + t], sv[2 * kSlabRows + t], sv[3 * kSlabRows + t]};
@@ -687,6 +747,7 @@ struct EpiPdlpPrimal {
   __device__ bool active() const { return !P->done; }
   __device__ Pre load(int j) const { return Pre{x[j], c[j], l[j], u[j], xa[j]}; }
   static constexpr int kVecs = 5;
+  static constexpr unsigned kLiveVecs = 0x11u;  // x and the running average xa
   __host__ __device__ const T* vec(int k) const { return k == 0 ? x : k == 1 ? c : k == 2 ? l : k == 3 ? u : xa; }
   __device__ Pre pre_at(const T* sv, int t) const {
     return Pre{sv[t], sv[kSlabRows + t], sv[2 * kSlabRows + t], sv[3 * kSlabRows + t], sv[4 * kSlabRows + t]};
@@ -714,6 +775,7 @@ struct EpiPdlpDual {
   __device__ bool active() const { return !P->done; }
   __device__ Pre load(int i) const { return Pre{y[i], rl[i], ru[i], ya[i]}; }
   static constexpr int kVecs = 4;
+  static constexpr unsigned kLiveVecs = 0x9u;  // y and the running average ya
   __host__ __device__ const T* vec(int k) const { return k == 0 ? y : k == 1 ? rl : k == 2 ? ru : ya; }
   __device__ Pre pre_at(const T* sv, int t) const {
     return Pre{sv[t], sv[kSlabRows + t], sv[2 * kSlabRows + t], sv[3 * kSlabRows + t]};
