@@ -2,29 +2,32 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload random1m|random10k|staircase8760|batch720x64|serve48]
-                    [--precision fp64|mixed]
+                    [--precision fp64|mixed] [--reductions exact|fast]
                     [--iterations L | --full]
 
-One STEP is one cold solve of the seeded LP on the device: setup (structure, scaling, ‖Ã‖₂),
-L r²HPDHG iterations with their checks every 64 iterations, and the finish (unscaling, KKT,
-z = c − Aᵀy, in-process check). The full solve of this LP to 1e-8 takes 3,724,096 iterations
-(about six minutes), so the default step caps the iterations at L = 6,400 and the metric is
-r²HPDHG iterations per second, whole job (time to 1e-8 = setup + iterations ÷ this rate).
-`--full` drops the cap: the step is a complete solve to 1e-8 KKT and the metric is solves/s
-(use it with --workload random10k: 249,088 iterations).
+One STEP is one cold solve of the seeded LP: setup (structure, scaling, ‖Ã‖₂), at most L = 640
+r²HPDHG iterations (10 checks) and the finish (unscaling, KKT, z = c − Aᵀy, in-process check).
+The metric is r²HPDHG iterations per second, whole job, over the K steps. Both arms run exactly
+this step on the same LP (engine level, no presolve) and print the same `config`; the
+reference's CPU engine takes about 12 s per step on the 1M LP, so L is what both can time.
+`--full` drops the cap: a step is a complete solve to 1e-8 KKT and the metric is solves/s.
 
 value: model resident in HBM before the timed region (ps26119_solve_lp_device), timed with CUDA
 events on the solve's stream, max over ranks. e2e: the same steps through the reference-facing
 C API (ps26119_solve_lp_ex, presolve and in-process check on) from pinned host buffers, the
 model's host-to-device copy and the x, y, z device-to-host copy inside the timed region.
+After the timed steps a single-GPU run adds (outside the timed region): `cpu_baseline`, one
+step of the reference CPU engine; `reference_gpu`, the same step through the reference's own
+CUDA backend built for sm_100a on this GPU; `time_to_tol`, measured wall-clock solves to 1e-8
+through the C API (the 10k random LP in fp64 and mixed, the T = 8760 staircase LP in mixed),
+the first also through the reference's CUDA backend.
 
 torchrun (N > 1): every rank solves its own replica (a single LP does not shard; no collective
 on the data path): weak scaling.
 
 --impl reference: the reference's own CPU engine (built from its sources into oracle/_ref) on
-the host cores, all threads, through ps26119::solve with presolve (as its C API), on the same LP.
-A step is a bounded sample — setup plus a few hundred iterations — whose per-iteration time is
-applied to the same L iterations as the GPU arm (or the full iteration count with --full).
+all host threads through ps26119::solve, each step the same capped cold solve, timed on the
+host clock; a single-GPU run adds its measured time to 1e-8 on the 10k random LP.
 """
 from __future__ import annotations
 
@@ -43,22 +46,24 @@ sys.path[:0] = [os.path.join(ROOT, "ps26119-solver_b200"), os.path.join(ROOT, "o
 
 WORKLOADS = {
     "random1m": {"desc": "random equality LP m=1,000,000 n=1,500,000 nnz=6,000,000 (6/row, N(0,1)), seed 1",
-                 "kind": "random", "m": 1_000_000, "full_iterations": 3_724_096},
+                 "kind": "random", "m": 1_000_000},
     "random10k": {"desc": "random equality LP m=10,000 n=15,000 nnz=60,000 (6/row, N(0,1)), seed 1",
-                  "kind": "random", "m": 10_000, "full_iterations": 249_088},
+                  "kind": "random", "m": 10_000},
     "staircase8760": {"desc": "staircase planning LP T=8760 (429,240 x 525,600), seed 1", "kind": "staircase",
-                      "T": 8760, "full_iterations": None},
+                      "T": 8760},
     "batch720x64": {"desc": "64 scenarios (b, c x lognormal(0, 0.1)) of the staircase LP T=720 "
-                            "(35,280 x 43,200, 126,024 nnz), seed 1", "kind": "batch", "T": 720, "K": 64,
-                    "full_iterations": None},
+                            "(35,280 x 43,200, 126,024 nnz), seed 1", "kind": "batch", "T": 720, "K": 64},
     "serve48": {"desc": "48 LP requests from the random-LP generator, m log-uniform in [1e3, 2e4] (n = 1.5m, "
                         "6 nnz/row), Poisson arrivals, each solved to 1e-8 (a bounded sample of the "
                         "2,000-request stream with m up to 2e5), seed 1", "kind": "serve", "N": 48,
-                "m_lo": 1_000, "m_hi": 20_000, "slots": 16, "full_iterations": None},
+                "m_lo": 1_000, "m_hi": 20_000, "slots": 16},
 }
 # DRAM bytes per iteration (both fused kernels: dram__bytes_read.sum + dram__bytes_write.sum of
-# one launch each) from the ncu capture summarised in profiles/k_slab_fed_random1m.md.
+# one launch each) from the ncu capture summarised in the named profile.
 NCU_TRAFFIC = {("random1m", "fp64"): 152.4e6 + 123.5e6}
+NCU_TRAFFIC_SOURCE = {("random1m", "fp64"): "profiles/k_slab_fed_random1m.md"}
+# Measured to-tolerance solves a default single-LP run adds after its timed steps.
+TIME_TO_TOL = [("random10k", "fp64"), ("random10k", "mixed"), ("staircase8760", "mixed")]
 
 
 def make_lp(name):
@@ -438,7 +443,17 @@ def metric_name(args):
     w = args.workload
     if args.full:
         return f"time-to-1e-8 KKT on {w} ({args.precision}) as solves/s"
-    return f"r2HPDHG iterations/s on {w} ({args.precision}); time-to-1e-8 = setup + iterations / rate"
+    return f"r2HPDHG iterations/s on {w} ({args.precision}), cold solves capped at {args.iterations} iterations"
+
+
+def shared_config(args, lp, world):
+    """The `config` both arms print: the workload and what one step does, nothing arm-specific."""
+    m, n, nnz = lp.num_rows, lp.num_cols, lp.nnz
+    s = 4 if args.precision == "mixed" else 8
+    return {"workload": WORKLOADS[args.workload]["desc"], "m": m, "n": n, "nnz": nnz, "tolerance": 1e-8,
+            "precision": args.precision, "iteration_cap": None if args.full else args.iterations,
+            "presolve": False, "parallelism": f"replicas x{world}",
+            "l2": f"inputs larger than L2: {bytes_per_iteration(m, n, nnz, s, s) / 1e6:.0f} MB streamed per iteration"}
 
 
 def run_ours(args, rank, world, local):
@@ -486,33 +501,31 @@ def run_ours(args, rank, world, local):
     step_ms = [evs[k].elapsed_time(evs[k + 1]) for k in range(args.steps)]
     barrier(world)
     r, st = results[-1]
-    iters_per_step = int(np.mean([rr.iterations for rr, _ in results]))
-    units = args.steps if args.full else args.steps * iters_per_step
+    iters = int(sum(rr.iterations for rr, _ in results))
+    units = args.steps if args.full else iters
     value = world * units / (ms / 1e3)
     s_v = s_w = 4 if args.precision == "mixed" else 8
     bpi = bytes_per_iteration(m, n, nnz, s_v, s_w)
-    iter_ms = st["spmv_kernel_ms"] / max(1, st["spmv_kernel_launches"] // 2)
+    kern_ms = sum(s["spmv_kernel_ms"] for _, s in results)
+    kern_pairs = max(1, sum(s["spmv_kernel_launches"] for _, s in results) // 2)
+    iter_ms = kern_ms / kern_pairs
     peak, peak_src = hbm_peak()
     achieved = bpi / (iter_ms * 1e-3) / 1e9
-    full = WORKLOADS[args.workload]["full_iterations"]
-    rate = value / world
     line = {
         "metric": metric_name(args), "value": value, "unit": "solves/s" if args.full else "iterations/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if args.precision == "fp64" else "f32+f64", "data": "synthetic (seeded generator)",
-        "config": {"workload": WORKLOADS[args.workload]["desc"], "m": m, "n": n, "nnz": nnz, "tolerance": 1e-8,
-                   "precision": args.precision, "entry": "ps26119_solve_lp_device (engine level, no presolve)",
-                   "iterations_per_step": iters_per_step, "iteration_cap": limit or None,
-                   "iterations_to_1e-8": full, "parallelism": f"replicas x{world}",
-                   "l2": f"inputs larger than L2: {bpi / 1e6:.0f} MB streamed per iteration",
-                   "time_to_1e-8_s": (None if args.full or not full else
-                                      st["setup_seconds"] + full / rate)},
+        "config": shared_config(args, lp, world),
+        "entry": "ps26119_solve_lp_device (model resident in HBM, engine level, no presolve)",
+        "reductions": args.reductions,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": NCU_TRAFFIC.get((args.workload, args.precision)),
+                     "traffic_source": NCU_TRAFFIC_SOURCE.get((args.workload, args.precision)),
                      "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)",
                      "unit_of_work": "one r2HPDHG iteration: the two fused SpMV+update kernels",
-                     "algorithmic_bytes": bpi, "kernel_us_per_iteration": iter_ms * 1e3},
+                     "algorithmic_bytes": bpi, "kernel_us_per_iteration": iter_ms * 1e3,
+                     "timing": "CUDA events recorded inside the epoch graphs on the solve's stream, all timed steps"},
         "step_ms": step_ms,
         "step_engine_ms": [1e3 * rr.seconds for rr, _ in results],
         "gpu_launches": int(sum(s["kernel_launches"] for _, s in results)),
@@ -532,8 +545,71 @@ def run_ours(args, rank, world, local):
     if not args.no_e2e:
         line["e2e"] = run_e2e(args, lp, world, limit)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = reference_sample(args, lp, iters_per_step, full)
+        line["cpu_baseline"] = reference_sample(args, lp)
+    if rank == 0 and world == 1 and not args.no_reference_gpu and not args.full:
+        line["reference_gpu"] = reference_gpu_sample(args, lp, value)
+    if rank == 0 and world == 1 and not args.no_time_to_tol and not args.full:
+        del arrs, x, y, z
+        line["time_to_tol"] = time_to_tol_records(args)
     return line
+
+
+def reference_gpu_sample(args, lp, ours):
+    """The reference's own CUDA backend (src/gpu/cuda_backend.cu built for sm_100a, Options::use_gpu)
+    on the same LP and cap, same GPU, one untimed warm-up then two timed cold solves (wall clock,
+    setup included, as our step)."""
+    import reference
+    if not reference.available_gpu():
+        return {"value": None, "note": "reference CUDA library not built (make -C oracle ref_gpu)"}
+    runs = []
+    for k in range(3):
+        t0 = time.perf_counter()
+        s = reference.solve(lp, presolve=False, precision=args.precision, threads=0,
+                            iteration_limit=args.iterations, gpu=True)
+        sec = time.perf_counter() - t0
+        if s.status not in ("IterationLimit", "Optimal"):
+            return {"value": None, "note": f"reference GPU solve ended {s.status}: {s.message}"}
+        if k:
+            runs.append((sec, s))
+    wall = sum(r[0] for r in runs)
+    its = sum(r[1].iterations for r in runs)
+    loop = sum(r[1].seconds - r[1].setup_seconds for r in runs)
+    value = its / wall
+    return {"value": value, "unit": "iterations/s", "ms_per_step": 1e3 * wall / len(runs),
+            "loop_iterations_per_s": its / loop, "setup_s": runs[-1][1].setup_seconds,
+            "ms_per_iteration_loop": 1e3 * loop / its, "ours_over_reference_gpu": ours / value,
+            "kind": "the reference's CUDA backend (src/gpu/cuda_backend.cu, its k_spmv_subwarp SpMV and "
+                    "update kernels) built for sm_100a, driven by its own r2HPDHG loop (host setup and checks)"}
+
+
+def time_to_tol_records(args):
+    """Measured time to 1e-8 KKT, one cold call of ps26119_solve_lp_ex each (presolve, the engine,
+    the in-process check and the certified bound), wall clock, on the named LPs; the 10k LP also
+    through the reference's own CUDA backend on the same GPU. Outside the timed steps."""
+    import ps26119
+    out = []
+    for name, precision in TIME_TO_TOL:
+        lp = make_lp(name)
+        t0 = time.perf_counter()
+        r = ps26119.solve_lp(lp.c, (lp.col_start, lp.row_index, lp.value), lp.row_lower, lp.row_upper,
+                             lp.col_lower, lp.col_upper, sense=lp.sense, offset=lp.offset, algorithm="r2hpdhg",
+                             precision=precision, time_limit=900)
+        sec = time.perf_counter() - t0
+        rec = {"workload": name, "precision": precision, "seconds": sec, "status": r.status_name,
+               "iterations": r.iterations, "objective": r.objective, "certified_bound": r.certified_bound,
+               "error_to_certified_bound": abs(r.objective - r.certified_bound) / (1.0 + abs(r.objective)),
+               "rel_kkt": max(r.primal_residual, r.dual_residual, r.gap), "check": r.check,
+               "entry": "ps26119_solve_lp_ex (presolve, engine, in-process check, certified bound)"}
+        if name == "random10k" and precision == "fp64" and not args.no_reference_gpu:
+            import reference
+            if reference.available_gpu():
+                t0 = time.perf_counter()
+                s = reference.solve(lp, presolve=True, precision=precision, threads=0, gpu=True, time_limit=900)
+                rec["reference_gpu"] = {"seconds": time.perf_counter() - t0, "status": s.status,
+                                        "iterations": s.iterations, "objective": s.objective,
+                                        "entry": "reference ps26119::solve, use_gpu (its CUDA backend), presolve"}
+        out.append(rec)
+    return out
 
 
 def gather_ceiling(m, lp):
@@ -577,24 +653,22 @@ def run_e2e(args, lp, world, limit):
             "iterations_per_step": iters // max(1, args.e2e_steps), "check": r.check}
 
 
-def reference_sample(args, lp, iterations, full):
-    """The reference CPU engine on this workload: one bounded, iteration-limited run with all
-    host threads, its per-iteration time applied to the iterations of one GPU step."""
+def reference_sample(args, lp):
+    """The reference CPU engine on this workload: one cold solve with the same iteration cap
+    (engine level, no presolve) on all host threads, wall clock (a bounded sample, 10-15 s)."""
     import reference
     cores = os.cpu_count() or 1
     if not reference.available():
         return {"value": None, "unit": "iterations/s", "cores": cores, "cpu_model": cpu_model(), "kind": "reference",
                 "sample": "reference library not built"}
-    s = reference.solve(lp, presolve=True, precision=args.precision, threads=0,
-                        iteration_limit=args.cpu_sample_iterations)
-    per_iter = (s.seconds - s.setup_seconds) / max(1, s.iterations)
-    its = full if args.full else iterations
-    total = s.setup_seconds + per_iter * its
-    return {"value": (1.0 if args.full else its) / total, "unit": "solves/s" if args.full else "iterations/s",
+    t0 = time.perf_counter()
+    s = reference.solve(lp, presolve=False, precision=args.precision, threads=0,
+                        iteration_limit=0 if args.full else args.iterations)
+    sec = time.perf_counter() - t0
+    return {"value": (1.0 if args.full else s.iterations) / sec, "unit": "solves/s" if args.full else "iterations/s",
             "cores": cores, "cpu_model": cpu_model(), "kind": "reference",
-            "sample": f"reference ps26119::solve (r2hpdhg, presolve, {cores} threads): {s.iterations} iterations "
-                      f"+ setup in {s.seconds:.1f} s ({per_iter * 1e3:.2f} ms/iteration, setup "
-                      f"{s.setup_seconds:.2f} s), applied to {its} iterations"}
+            "sample": f"reference ps26119::solve (r2hpdhg, no presolve, {cores} threads): one cold solve of "
+                      f"{s.iterations} iterations in {sec:.1f} s (setup {s.setup_seconds:.2f} s)"}
 
 
 def run_reference(args, rank, world):
@@ -613,49 +687,57 @@ def run_reference(args, rank, world):
             return {"impl": "reference", "unavailable": "--full batch: the reference CPU batch to 1e-8 takes hours"}
         scen = make_scenarios(args.workload, lp)
         K = len(scen)
-        rates = []
+        times, its = [], 0
         for i in range(args.warmup + args.steps):
             t0 = time.perf_counter()
             w = reference.batch(lp, scen, threads=0, iteration_limit=args.cpu_sample_iterations)
             sec = time.perf_counter() - t0
             if i >= args.warmup:
-                rates.append(K * max(x["iterations"] for x in w) / sec)
-        value = float(np.mean(rates))
+                times.append(sec)
+                its += K * max(x["iterations"] for x in w)
+        value = its / sum(times)
         unit = "scenario-iterations/s"
         sample = (f"reference solve_batch ({cores} threads): {args.cpu_sample_iterations} lockstep iterations of "
                   f"{K} scenarios incl. setup per step")
         return {"metric": f"batched r2HPDHG on {args.workload} ({unit})", "value": value, "unit": unit,
-                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": None,
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(times)),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic (seeded generator)",
                 "config": {"workload": WORKLOADS[args.workload]["desc"], "scenarios": K, "tolerance": 1e-8},
                 "impl": "reference",
                 "cpu_baseline": {"value": value, "unit": unit, "cores": cores, "cpu_model": cpu_model(), "kind": "reference", "sample": sample},
                 "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    full = WORKLOADS[args.workload]["full_iterations"]
-    its = full if args.full else args.iterations
-    times, sample = [], None
+    # one step = one cold solve of the LP capped at the same iteration count as our arm (setup,
+    # iterations, finish), timed on the host clock
+    times, its = [], 0
     for i in range(args.warmup + args.steps):
-        s = reference.solve(lp, presolve=True, precision=args.precision, threads=0,
-                            iteration_limit=args.cpu_sample_iterations)
-        per_iter = (s.seconds - s.setup_seconds) / max(1, s.iterations)
+        t0 = time.perf_counter()
+        s = reference.solve(lp, presolve=False, precision=args.precision, threads=0,
+                            iteration_limit=0 if args.full else args.iterations)
+        sec = time.perf_counter() - t0
         if i >= args.warmup:
-            times.append(s.setup_seconds + per_iter * its)
-        sample = (f"reference ps26119::solve (r2hpdhg, presolve, {cores} threads): {s.iterations} iterations + "
-                  f"setup per step ({per_iter * 1e3:.2f} ms/iteration), applied to {its} iterations")
-    sec = float(np.mean(times))
-    value = (1.0 if args.full else its) / sec
+            times.append(sec)
+            its += s.iterations
+    value = (args.steps if args.full else its) / sum(times)
     unit = "solves/s" if args.full else "iterations/s"
-    return {"metric": metric_name(args), "value": value, "unit": unit, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
-            "data": "synthetic (seeded generator)",
-            "config": {"workload": WORKLOADS[args.workload]["desc"], "m": lp.num_rows, "n": lp.num_cols,
-                       "nnz": lp.nnz, "tolerance": 1e-8, "precision": args.precision,
-                       "iterations_per_step": its},
-            "impl": "reference",
-            "cpu_baseline": {"value": value, "unit": unit, "cores": cores, "cpu_model": cpu_model(), "kind": "reference", "sample": sample},
+    sample = (f"reference ps26119::solve (r2hpdhg, no presolve, {cores} threads): each step one cold solve "
+              f"capped at {args.iterations} iterations, setup {s.setup_seconds:.2f} s of {times[-1]:.1f} s")
+    line = {"metric": metric_name(args), "value": value, "unit": unit, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(times)), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+            "data": "synthetic (seeded generator)", "config": shared_config(args, lp, world),
+            "entry": "reference ps26119::solve (its CPU engine, all host threads)", "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": unit, "cores": cores, "cpu_model": cpu_model(),
+                             "kind": "reference", "sample": sample},
             "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if world == 1 and not args.no_time_to_tol and not args.full:
+        lp10 = make_lp("random10k")
+        t0 = time.perf_counter()
+        r = reference.solve(lp10, presolve=True, precision="fp64", threads=0, time_limit=900)
+        line["time_to_tol"] = [{"workload": "random10k", "precision": "fp64", "seconds": time.perf_counter() - t0,
+                                "status": r.status, "iterations": r.iterations, "objective": r.objective,
+                                "entry": f"reference ps26119::solve (CPU engine, presolve, {cores} threads)"}]
+    return line
 
 
 def main():
@@ -668,12 +750,16 @@ def main():
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--reductions", choices=["exact", "fast"], default="fast",
                     help="exact: every sum in the reference's order; fast: fixed-order trees")
-    ap.add_argument("--iterations", type=int, default=6400, help="iteration cap of one step")
+    ap.add_argument("--reductions", choices=["exact", "fast"], default="fast",
+                    help="exact: every sum in the reference's order; fast: fixed-order trees")
+    ap.add_argument("--iterations", type=int, default=640, help="iteration cap of one step (both arms)")
     ap.add_argument("--full", action="store_true", help="solve to 1e-8 in every step")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-sample-iterations", type=int, default=256)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reference-gpu", action="store_true", help="skip the reference CUDA backend's sample")
+    ap.add_argument("--no-time-to-tol", action="store_true", help="skip the measured time-to-1e-8 records")
     ap.add_argument("--serve-sample", type=int, default=8, help="requests solved sequentially for the baseline")
     ap.add_argument("--serve-slots", type=int, default=0, help="server slots (0: the workload's)")
     args = ap.parse_args()
