@@ -53,6 +53,9 @@ WORKLOADS = {
                       "T": 8760},
     "batch720x64": {"desc": "64 scenarios (b, c x lognormal(0, 0.1)) of the staircase LP T=720 "
                             "(35,280 x 43,200, 126,024 nnz), seed 1", "kind": "batch", "T": 720, "K": 64},
+    "batch720x64f": {"desc": "64 feasible scenarios of the staircase LP T=720 (35,280 x 43,200, 126,024 nnz): "
+                             "interior point, slacks and c x lognormal(0, 0.1), seed 1", "kind": "batch", "T": 720,
+                     "K": 64, "feasible": True},
     "serve48": {"desc": "48 LP requests from the random-LP generator, m log-uniform in [1e3, 2e4] (n = 1.5m, "
                         "6 nnz/row), Poisson arrivals, each solved to 1e-8 (a bounded sample of the "
                         "2,000-request stream with m up to 2e5), seed 1", "kind": "serve", "N": 48,
@@ -74,7 +77,8 @@ def make_lp(name):
 
 def make_scenarios(name, lp):
     from ps26119 import generators as g
-    return g.scenarios(lp, WORKLOADS[name]["K"], sigma=0.1, seed=1)
+    make = g.feasible_scenarios if WORKLOADS[name].get("feasible") else g.scenarios
+    return make(lp, WORKLOADS[name]["K"], sigma=0.1, seed=1)
 
 
 def make_requests(name):
@@ -227,7 +231,7 @@ def run_batch(args, rank, world, local):
 
     def step():
         res = ps26119.solve_batch(lp.c, A, lp.row_lower, lp.row_upper, lp.col_lower, lp.col_upper, scenarios=scen,
-                                  sense=lp.sense, offset=lp.offset, iteration_limit=limit)
+                                  sense=lp.sense, offset=lp.offset, iteration_limit=limit, precision=args.precision)
         bad = [r.status_name for r in res if r.status_name not in ("Optimal", "IterationLimit")]
         if bad or (args.full and any(r.status_name != "Optimal" for r in res)):
             raise RuntimeError(f"batch ended {set(r.status_name for r in res)}")
@@ -257,8 +261,10 @@ def run_batch(args, rank, world, local):
     line = {
         "metric": f"batched r2HPDHG on {args.workload} ({unit})", "value": value, "unit": unit, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3 / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+        "data": "synthetic (seeded generator)",
         "config": {"workload": WORKLOADS[args.workload]["desc"], "m": m, "n": n, "nnz": nnz, "scenarios": K,
+                   "precision": args.precision,
                    "tolerance": 1e-8, "iteration_cap": limit or None, "entry": "ps26119_solve_batch (host arrays)",
                    "iterations_per_step": its, "parallelism": f"replicas x{world}",
                    "l2": f"inputs larger than L2: {bpi / 1e6:.0f} MB streamed per lockstep iteration"},
@@ -268,6 +274,10 @@ def run_batch(args, rank, world, local):
         "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": nnz * 12 + (n + 1) * 4 + K * 8 * (3 * n + 2 * m),
                 "d2h_bytes_per_step": K * 8 * (2 * n + m), "note": "the batch entry point takes host arrays"},
     }
+    if args.full:
+        line["scenarios_optimal"] = sum(r.status_name == "Optimal" for r in res)
+        line["iterations"] = {"max": its, "median": float(np.median([r.iterations for r in res]))}
+        line["sequential_fp64"] = sequential_sample(args, lp, scen, value / world)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         import reference
         cores = os.cpu_count() or 1
@@ -282,6 +292,29 @@ def run_batch(args, rank, world, local):
                                     "sample": f"reference solve_batch ({cores} threads), {rits} lockstep iterations "
                                               f"of {K} scenarios incl. setup in {rs:.1f} s"}
     return line
+
+
+def sequential_sample(args, lp, scen, batched_rate):
+    """Scenarios solved one at a time to 1e-8 in plain fp64 through the single-LP engine on the
+    same GPU (ps26119_solve_lp_engine, no presolve): a sample of args.serve_sample scenarios,
+    evenly spaced; the batch's speed-up is its solves/s times the mean sequential solve time."""
+    import ps26119
+    S = max(1, min(len(scen), args.serve_sample))
+    pick = [scen[(2 * j + 1) * len(scen) // (2 * S)] for j in range(S)]
+    times, its = [], []
+    for sc in pick:
+        t0 = time.perf_counter()
+        r = ps26119.solve_lp(sc["obj"], (lp.col_start, lp.row_index, lp.value), sc["row_lower"], sc["row_upper"],
+                             lp.col_lower, lp.col_upper, sense=lp.sense, offset=lp.offset, algorithm="r2hpdhg",
+                             precision="fp64", engine={"presolve": False}, time_limit=1800)
+        times.append(time.perf_counter() - t0)
+        its.append(r.iterations)
+        if r.status != ps26119.OPTIMAL:
+            return {"note": f"sequential solve ended {r.status_name}: {r.message}"}
+    t_seq = float(np.mean(times))
+    return {"solves_per_s": 1.0 / t_seq, "speedup": batched_rate * t_seq, "iterations": its,
+            "sample": f"{S} of the {len(scen)} scenarios (evenly spaced), each solved alone to 1e-8 in plain fp64, "
+                      "ps26119_solve_lp_engine without presolve, same GPU"}
 
 
 def bytes_per_iteration(m, n, nnz, s_v, s_w):
@@ -748,8 +781,6 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="random1m")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
-    ap.add_argument("--reductions", choices=["exact", "fast"], default="fast",
-                    help="exact: every sum in the reference's order; fast: fixed-order trees")
     ap.add_argument("--reductions", choices=["exact", "fast"], default="fast",
                     help="exact: every sum in the reference's order; fast: fixed-order trees")
     ap.add_argument("--iterations", type=int, default=640, help="iteration cap of one step (both arms)")

@@ -9,7 +9,9 @@
 //
 // Per iteration: k_bspmm with the primal epilogue (Ãᵀy, projection, reflection, Halpern) and
 // with the dual epilogue (Ãx̄, dual update): two launches. The per-slot step sizes and Halpern
-// counters live in device arrays written at each check.
+// counters live in device arrays written at each check. An epoch of K iterations is one CUDA
+// graph (two variants: with and without the r⁰ section after the first step), captured for the
+// current slot count and blocks and captured again after a compaction moves them.
 // Per check (every K iterations): fixed-point residuals (one SpMM), restart distances, the
 // KKT statistics of every slot on the ORIGINAL matrix (two SpMMs), all per-slot sums in one
 // launch, one download of W×32 doubles; the host then takes the reference's per-scenario
@@ -473,12 +475,22 @@ class BatchEngine {
     for (auto& e : ev_) B200_CHECK(cudaEventCreate(&e));
   }
   ~BatchEngine() {
+    drop_graphs();
     for (auto& e : ev_) cudaEventDestroy(e);
   }
   BatchEngine(const BatchEngine&) = delete;
   BatchEngine& operator=(const BatchEngine&) = delete;
 
   void run(std::vector<BatchOutcome>& out);
+  // Bulk-copy waits of this batch's setup kernels that ran out (synchronises the stream).
+  unsigned stage_errors() {
+    unsigned v = 0;
+    if (stage_err_.get()) {
+      B200_CHECK(cudaMemcpyAsync(&v, stage_err_.get(), sizeof v, cudaMemcpyDeviceToHost, st_));
+      B200_CHECK(cudaStreamSynchronize(st_));
+    }
+    return v;
+  }
 
  private:
   double elapsed() const { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0_).count(); }
@@ -490,6 +502,12 @@ class BatchEngine {
   template <class Epi>
   void spmm(int rows, const int* rp, const int* col, const double* val, const double* X, const Epi& epi, bool capped);
   void step(int s);
+  void epoch_body(bool r0_section);
+  void launch_epoch(bool r0_section);
+  void drop_graphs() {
+    for (auto& g : graph_)
+      if (g) cudaGraphExecDestroy(g), g = nullptr;
+  }
   void compact(const std::vector<int>& keep);
   void finish_slot(int t, BatchOutcome& o, Status st, const BKkt& kk, long long it, const std::string& msg);
 
@@ -499,6 +517,8 @@ class BatchEngine {
   const EngineOptions& o_;
   cudaStream_t st_;
   cudaEvent_t ev_[4] = {};  // SpMM time of an epoch: [0,1] step 0, [2,3] steps 1..K-1
+  cudaGraphExec_t graph_[2] = {nullptr, nullptr};  // epoch without / with the r⁰ section
+  long long graph_kernels_[2] = {0, 0};
   double spmm_ms_ = 0.0;
   long long spmm_launches_ = 0;
   std::chrono::steady_clock::time_point t0_;
@@ -508,6 +528,7 @@ class BatchEngine {
 
   DevBuf<double> c_, cl_, cu_, rl_, ru_, v_;
   DevBuf<int> cs_, ri_;
+  DevBuf<unsigned> stage_err_;  // this batch's bulk-copy timeouts (see count_stage_timeout)
   ScaledDevice sp_;
   // interleaved blocks: original data, scaled data, iterates, work and term arrays
   enum NVec { OC, OCL, OCU, C, L, U, X, X0, XH, XB, DX, XO, TPX, TDXN, TP, TDC, TRDC, TC2, TSC2, kNVec };
@@ -587,7 +608,9 @@ void BatchEngine::setup() {
   ScalingOptions so = o_.scaling;
   so.bound_objective_rescaling = false;
   sp_.build(dm, so, o_.exact, st_);
-  const double norm = sp_.lanczos(st_);
+  stage_err_.alloc(1);
+  B200_CHECK(cudaMemsetAsync(stage_err_.get(), 0, sizeof(unsigned), st_));
+  const double norm = sp_.lanczos(st_, stage_err_.get());
   eta_ = norm > 0 ? 0.998 / norm : 1.0;
   setup_s_ = elapsed();
 
@@ -679,6 +702,57 @@ void BatchEngine::step(int s) {
   spmm(m_, sp_.a_rp.get(), sp_.a_col.get(), sp_.sa.get(), nv_[XB].get(), ed, false);
 }
 
+// The K iterations of an epoch (the body of the epoch graph), with the r⁰ residual right after
+// the first step when a slot starts a Halpern cycle (batch.cpp:359-366).
+void BatchEngine::epoch_body(bool r0_section) {
+  const int Kc = o_.check_every;
+  B200_CHECK(cudaEventRecordWithFlags(ev_[0], st_, cudaEventRecordExternal));
+  for (int s = 0; s < Kc; ++s) {
+    step(s);
+    if (s == 0) B200_CHECK(cudaEventRecordWithFlags(ev_[1], st_, cudaEventRecordExternal));
+    if (s == 0 && r0_section) {
+      launch_residual(false);
+      ISegs g{};
+      g.s[0] = {nv_[TPX].get(), n_, nullptr, 0, 0.0, kBPx0};
+      g.s[1] = {mv_[TPY].get(), m_, nullptr, 0, 0.0, kBPy0};
+      g.s[2] = {mv_[TCR].get(), m_, nullptr, 0, 0.0, kBCr0};
+      g.n = 3;
+      launch_sums(g);
+    }
+    if (s == 0) B200_CHECK(cudaEventRecordWithFlags(ev_[2], st_, cudaEventRecordExternal));
+  }
+  B200_CHECK(cudaEventRecordWithFlags(ev_[3], st_, cudaEventRecordExternal));
+}
+
+// Replays the epoch graph of this variant, capturing it first for the current slots.
+void BatchEngine::launch_epoch(bool r0_section) {
+  const int v = r0_section ? 1 : 0;
+  if (!graph_[v]) {
+    const long long before = launches_;
+    cudaGraph_t g;
+    {
+      CaptureScope scope;  // no device-wide synchronisation elsewhere meanwhile
+      B200_CHECK(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
+      try {
+        epoch_body(r0_section);
+      } catch (...) {
+        cudaGraph_t dead = nullptr;
+        cudaStreamEndCapture(st_, &dead);
+        if (dead) cudaGraphDestroy(dead);
+        throw;
+      }
+      B200_CHECK(cudaStreamEndCapture(st_, &g));
+    }
+    const cudaError_t e = cudaGraphInstantiate(&graph_[v], g, 0);
+    cudaGraphDestroy(g);
+    B200_CHECK(e);
+    graph_kernels_[v] = launches_ - before;
+    launches_ = before;
+  }
+  B200_CHECK(cudaGraphLaunch(graph_[v], st_));
+  launches_ += graph_kernels_[v];
+}
+
 void BatchEngine::launch_residual(bool distances) {
   const long long nw = static_cast<long long>(n_) * W_;
   k_bres_x<<<grid_for(nw), kBlock, 0, st_>>>(nw, nv_[XB].get(), nv_[XH].get(), nv_[X0].get(), nv_[DX].get(),
@@ -719,6 +793,7 @@ void BatchEngine::compact(const std::vector<int>& keep) {
   };
   for (auto& v : nv_) gather(v, n_, spare_n_);
   for (auto& v : mv_) gather(v, m_, spare_m_);
+  drop_graphs();  // the blocks moved and the slot count changed: capture again
   std::vector<double> nbs(W2), nos(W2);
   for (int t = 0; t < W2; ++t) nbs[t] = hbs_[keep[t]], nos[t] = hos_[keep[t]];
   hbs_.swap(nbs), hos_.swap(nos);
@@ -796,25 +871,7 @@ void BatchEngine::run(std::vector<BatchOutcome>& out) {
     B200_CHECK(cudaMemcpyAsync(tau_.get(), h_par_.get(), W_ * sizeof(double), cudaMemcpyHostToDevice, st_));
     B200_CHECK(cudaMemcpyAsync(sigma_.get(), h_par_.get() + W_, W_ * sizeof(double), cudaMemcpyHostToDevice, st_));
     B200_CHECK(cudaMemcpyAsync(inner0_.get(), h_inner_.get(), W_ * sizeof(long long), cudaMemcpyHostToDevice, st_));
-    B200_CHECK(cudaEventRecord(ev_[0], st_));
-    for (int s = 0; s < Kc; ++s) {
-      step(s);
-      if (s == 0) {
-        B200_CHECK(cudaEventRecord(ev_[1], st_));
-        B200_CHECK(cudaEventRecord(ev_[2], st_));  // moved past the r⁰ section below when there is one
-      }
-      if (s == 0 && any_new) {  // r⁰ right after the epoch's first step (batch.cpp:359-366)
-        launch_residual(false);
-        ISegs g{};
-        g.s[0] = {nv_[TPX].get(), n_, nullptr, 0, 0.0, kBPx0};
-        g.s[1] = {mv_[TPY].get(), m_, nullptr, 0, 0.0, kBPy0};
-        g.s[2] = {mv_[TCR].get(), m_, nullptr, 0, 0.0, kBCr0};
-        g.n = 3;
-        launch_sums(g);
-        B200_CHECK(cudaEventRecord(ev_[2], st_));
-      }
-    }
-    B200_CHECK(cudaEventRecord(ev_[3], st_));
+    launch_epoch(any_new);
     for (int t = 0; t < W_; ++t) inner[sid_[t]] += Kc;
     it += Kc;
     // ---- check: residual + restart distances, KKT of every slot, one download
@@ -958,6 +1015,7 @@ std::vector<BatchOutcome> run_batch_host(const HostModelView& base, const std::v
     BatchEngine eng(base, scenarios, group, opt, st, t0);
     std::vector<BatchOutcome> part(scenarios.size());
     eng.run(part);
+    if (eng.stage_errors()) throw CudaError("a shared-memory staging wait timed out on the device");
     for (int k : group) out[k] = std::move(part[k]);
   }
   return out;

@@ -47,6 +47,26 @@ static __global__ void k_lanczos_next(int n, const double* w, double* v, double*
     v[j] = w[j] / bn;
   }
 }
+// The same two steps with α and β read from the device, where the sums left them: α = *al,
+// β_prev = sqrt(*bsq_prev) (0 without one), β = sqrt(*bsq) — sqrt correctly rounded, as the
+// host's std::sqrt. `hist` receives (α, β²) of step k for the host's later replay.
+static __global__ void k_lanczos_update_dev(int n, double* w, const double* v, const double* vprev, const double* al,
+                                            const double* bsq_prev, double* t) {
+  const double a = *al, bp = bsq_prev ? sqrt(*bsq_prev) : 0.0;
+  B200_FOR(j, n) {
+    w[j] -= a * v[j] + bp * vprev[j];
+    t[j] = w[j] * w[j];
+  }
+}
+static __global__ void k_lanczos_next_dev(int n, const double* w, double* v, double* vprev, const double* ab,
+                                          double* hist) {
+  const double bn = sqrt(ab[1]);
+  if (blockIdx.x == 0 && threadIdx.x == 0) hist[0] = ab[0], hist[1] = ab[1];
+  B200_FOR(j, n) {
+    vprev[j] = v[j];
+    v[j] = w[j] / bn;
+  }
+}
 
 
 struct ScaledDevice {
@@ -218,8 +238,11 @@ struct ScaledDevice {
 
   // ‖Ã‖₂ by Lanczos on ÃᵀÃ (csr.cpp:86-132). The start vector is the reference's xorshift64*
   // stream, generated and normalised on the host in the reference's order; the products run
-  // on the device; α and β are reduced in the selected order and brought back each step for
-  // the Sturm-bisection on the host.
+  // on the device; α and β are reduced in the selected order and stay on the device, where the
+  // next step's update reads them. The host reads them back once per batch of steps (21, then
+  // 8 at a time) and replays the reference's per-step decisions on them (Sturm bisection,
+  // breakdown and stagnation tests) in step order: the result and the number of steps that
+  // count are the sequential loop's; steps run past the stopping one are discarded.
   double lanczos(cudaStream_t st, unsigned* err = nullptr) {
     if (n == 0 || nnz == 0) return 0.0;
     const int K = 400;
@@ -237,50 +260,55 @@ struct ScaledDevice {
     DevBuf<double> v(n), vprev(n), w(n), t(m), terms(n);
     B200_CHECK(cudaMemcpyAsync(v.get(), hv.data(), hv.size() * sizeof(double), cudaMemcpyHostToDevice, st));
     B200_CHECK(cudaMemsetAsync(vprev.get(), 0, static_cast<std::size_t>(n) * sizeof(double), st));
-    DevBuf<double> out(2);
+    DevBuf<double> out(2), hist(2 * static_cast<std::size_t>(K));
     SumPlan pal, pbn;
     pal.add(terms.get(), 0, n, 0.0, SumOrder::kSeq, out.get());
     pbn.add(terms.get(), 0, n, 0.0, SumOrder::kSeq, out.get() + 1);
     pal.build(exact, nullptr, st);
     pbn.build(exact, nullptr, st);
-    std::vector<double> alpha, beta;
+    std::vector<double> alpha, beta, h(2 * static_cast<std::size_t>(K));
     double theta = 0, theta_old = -1;
     int stagnant = 0;
-    for (int k = 0; k < K; ++k) {
-      launch_slab_tma<double>(m, a_rp.get(), a_col.get(), sa.get(), v.get(), EpiStore<double>{{}, t.get()}, st, nullptr,
-                              err);
-      launch_slab_tma<double>(n, M.col_start, t_ri.get(), sat.get(), t.get(), EpiStore<double>{{}, w.get()}, st, nullptr,
-                              err);
-      k_prod_terms<<<grid_for(n), kBlock, 0, st>>>(n, w.get(), v.get(), terms.get());
-      B200_LAUNCH_CHECK();
-      pal.launch(st);
-      double al = 0;
-      B200_CHECK(cudaMemcpyAsync(&al, out.get(), sizeof al, cudaMemcpyDeviceToHost, st));
-      B200_CHECK(cudaStreamSynchronize(st));
-      const double bprev = beta.empty() ? 0.0 : beta.back();
-      k_lanczos_update<<<grid_for(n), kBlock, 0, st>>>(n, w.get(), v.get(), vprev.get(), al, bprev, terms.get());
-      B200_LAUNCH_CHECK();
-      pbn.launch(st);
-      double bn = 0;
-      B200_CHECK(cudaMemcpyAsync(&bn, out.get() + 1, sizeof bn, cudaMemcpyDeviceToHost, st));
-      B200_CHECK(cudaStreamSynchronize(st));
-      kernels += 4 + pal.kernel_count() + pbn.kernel_count();
-      bn = std::sqrt(bn);
-      alpha.push_back(al);
-      theta = tridiag_max_eig(alpha, beta, static_cast<int>(alpha.size()));
-      if (bn <= 1e-14 * std_max(1.0, theta)) break;
-      beta.push_back(bn);
-      if (theta - theta_old <= rel_tol * theta) {
-        if (++stagnant >= 5 && k >= 20) break;
-      } else {
-        stagnant = 0;
+    int done = 0;  // steps launched
+    for (;;) {
+      const int batch = std::min(K - done, done == 0 ? 21 : 8);
+      for (int k = done; k < done + batch; ++k) {
+        launch_slab_tma<double>(m, a_rp.get(), a_col.get(), sa.get(), v.get(), EpiStore<double>{{}, t.get()}, st,
+                                nullptr, err);
+        launch_slab_tma<double>(n, M.col_start, t_ri.get(), sat.get(), t.get(), EpiStore<double>{{}, w.get()}, st,
+                                nullptr, err);
+        k_prod_terms<<<grid_for(n), kBlock, 0, st>>>(n, w.get(), v.get(), terms.get());
+        B200_LAUNCH_CHECK();
+        pal.launch(st);
+        // β of the previous step is still in out[1]: this step's β² overwrites it only below
+        k_lanczos_update_dev<<<grid_for(n), kBlock, 0, st>>>(n, w.get(), v.get(), vprev.get(), out.get(),
+                                                              k > 0 ? out.get() + 1 : nullptr, terms.get());
+        B200_LAUNCH_CHECK();
+        pbn.launch(st);
+        k_lanczos_next_dev<<<grid_for(n), kBlock, 0, st>>>(n, w.get(), v.get(), vprev.get(), out.get(),
+                                                            hist.get() + 2 * k);
+        B200_LAUNCH_CHECK();
+        kernels += 5 + pal.kernel_count() + pbn.kernel_count();
       }
-      theta_old = theta;
-      k_lanczos_next<<<grid_for(n), kBlock, 0, st>>>(n, w.get(), v.get(), vprev.get(), bn);
-      B200_LAUNCH_CHECK();
-      ++kernels;
+      B200_CHECK(cudaMemcpyAsync(h.data() + 2 * done, hist.get() + 2 * done, 2 * batch * sizeof(double),
+                                 cudaMemcpyDeviceToHost, st));
+      B200_CHECK(cudaStreamSynchronize(st));
+      for (int k = done; k < done + batch; ++k) {  // the reference's loop body, step by step
+        const double al = h[2 * k], bn = std::sqrt(h[2 * k + 1]);
+        alpha.push_back(al);
+        theta = tridiag_max_eig(alpha, beta, static_cast<int>(alpha.size()));
+        if (bn <= 1e-14 * std_max(1.0, theta)) return std::sqrt(std_max(theta, 0.0)) * (1.0 + 1e-4);
+        beta.push_back(bn);
+        if (theta - theta_old <= rel_tol * theta) {
+          if (++stagnant >= 5 && k >= 20) return std::sqrt(std_max(theta, 0.0)) * (1.0 + 1e-4);
+        } else {
+          stagnant = 0;
+        }
+        theta_old = theta;
+      }
+      done += batch;
+      if (done >= K) return std::sqrt(std_max(theta, 0.0)) * (1.0 + 1e-4);
     }
-    return std::sqrt(std_max(theta, 0.0)) * (1.0 + 1e-4);
   }
 
   // Largest eigenvalue of the Lanczos tridiagonal by Sturm bisection (csr.cpp:54-84).

@@ -49,23 +49,26 @@ __device__ __forceinline__ double block_sum_fixed(double v, double* sh) {
 // ------------------------------------------------------------------ exact chains, in parallel
 // A chain s = init; s = fl(s + t[i]) for i = lo, lo+1, … is inherently sequential, and walking
 // 2.5 million terms with one warp costs milliseconds. It is evaluated here in parallel, with the
-// sequential chain's result bit for bit, from one property of round-to-nearest: while every
-// partial sum stays inside one binade [2^e, 2^(e+1)) (ulp u = 2^(e−52)), each partial sum is a
-// multiple of u, so fl(s + t) = s + u·rint(t/u) exactly — unless t/u is a tie (x.5), or the exact
-// sum leaves the binade. Inside such a run the chain is an INTEGER sum of k = rint(t/u), which is
-// associative. So:
+// sequential chain's result bit for bit, from one property of round-to-nearest-even: while every
+// partial sum stays inside one binade [2^e, 2^(e+1)) (ulp u = 2^(e−52)), each partial sum is an
+// integer multiple S·u, and fl(S·u + t) = (S + k)·u with k = rint(t/u) — or, when t/u = f + ½ is a
+// tie, k = f or f + 1, whichever makes S + k even. So inside such a run the chain is an integer
+// walk whose only dependence on the past is the parity of S: a run of terms is summarised by its
+// effect for each of the two parities (XRun), and effects compose associatively. So:
 //   k_xstat   per tile of kXTile terms: an approximate fp64 sum and the approximate range of the
 //             tile's running sums (any order; only used to guess each tile's binade);
 //   k_xagg    per tile: the guessed binade's u from the approximate start (the approximate sums
-//             of the chain's earlier tiles), then K = Σ k and the minimum / maximum of the
-//             integer running sums, in int64 (exact); ties and |t/u| ≥ 2^51 mark the tile;
+//             of the chain's earlier tiles), then the tile's XRun (exact int64: change of S, its
+//             lowest and highest running value, parity after, per parity before); a term with
+//             |t/u| ≥ 2^51 (or non-finite) marks the tile;
 //   k_xchain  one warp per chain walks its tiles in order with the EXACT s: a tile is committed
-//             as s ← (s/u + K)·u when s lies in the guessed binade and s/u plus every running
-//             integer sum stays within [2^52 + 1, 2^53 − 1] (so each exact partial sum lies inside
-//             the binade, at least u/2 from its ends); any other tile is walked in windows of
-//             256 terms with the same test per term, committing the valid prefix and adding the
-//             first failing term with one plain fp64 addition (so ties, binade changes, zeros,
-//             subnormals, infinities and NaN get exactly the sequential chain's arithmetic).
+//             as s ← (S0 + K[S0 mod 2])·u when s = S0·u lies in the guessed binade and every
+//             running S stays within [2^52 + 1, 2^53 − 1] (then each exact partial sum lies inside
+//             the binade, at least u/2 from its ends, and rounds to that grid); any other tile is
+//             walked in windows of 256 terms with the same exact test per term (a warp scan of
+//             the lanes' XRuns), committing the valid prefix and adding the first failing term
+//             with one plain fp64 addition (so binade changes, zeros, subnormals, infinities and
+//             NaN get exactly the sequential chain's arithmetic).
 // The approximations only choose between two exact paths; the result never depends on them.
 constexpr int kXTile = 2048;    // terms per tile (8 per thread of a 256-thread block)
 constexpr int kXPer = 8;        // terms per thread (tiles) and per lane (windows)
@@ -83,14 +86,70 @@ struct XTileStat {
   int bad;                 // a non-finite term
   int pad;
 };
+// The effect of a run of terms on S (the partial sum in units of u), for S even (index 0) and
+// odd (1) at the run's start: K the change of S, mn / mx the lowest / highest running change
+// over positions 1…len (LLONG_MAX / LLONG_MIN for an empty run), out the parity after; bad: a
+// term the integer form cannot take (|t/u| ≥ 2^51 or non-finite).
+struct XRun {
+  long long K[2], mn[2], mx[2];
+  int out[2];
+  int bad;
+};
 struct XTileAgg {
-  double u;               // the binade's ulp the integers are counted in (0: no guess)
-  long long K, pmin, pmax;  // Σ k and the min / max of the running integer sums (positions 1…len)
-  int ok;                 // no tie, every |t/u| < 2^51
-  int pad;
+  double u;  // the binade's ulp the run is counted in (0: no guess)
+  XRun r;
 };
 
 constexpr long long kX52 = 1LL << 52, kX53 = 1LL << 53;
+
+__device__ __forceinline__ XRun x_identity() {
+  XRun r;
+  r.K[0] = r.K[1] = 0;
+  r.mn[0] = r.mn[1] = LLONG_MAX;
+  r.mx[0] = r.mx[1] = LLONG_MIN;
+  r.out[0] = 0, r.out[1] = 1;
+  r.bad = 0;
+  return r;
+}
+// a then b (selects instead of indexing with a.out[p], so everything stays in registers)
+__device__ __forceinline__ XRun x_compose(const XRun& a, const XRun& b) {
+  XRun r;
+  r.bad = a.bad | b.bad;
+#pragma unroll
+  for (int p = 0; p < 2; ++p) {
+    const bool q = a.out[p] != 0;
+    const long long bK = q ? b.K[1] : b.K[0], bmn = q ? b.mn[1] : b.mn[0], bmx = q ? b.mx[1] : b.mx[0];
+    r.K[p] = a.K[p] + bK;
+    r.mn[p] = bmn == LLONG_MAX ? a.mn[p] : min(a.mn[p], a.K[p] + bmn);
+    r.mx[p] = bmx == LLONG_MIN ? a.mx[p] : max(a.mx[p], a.K[p] + bmx);
+    r.out[p] = q ? b.out[1] : b.out[0];
+  }
+  return r;
+}
+__device__ __forceinline__ XRun x_shfl_down(const XRun& v, int off) {
+  XRun r;
+#pragma unroll
+  for (int p = 0; p < 2; ++p) {
+    r.K[p] = __shfl_down_sync(kFull, v.K[p], off);
+    r.mn[p] = __shfl_down_sync(kFull, v.mn[p], off);
+    r.mx[p] = __shfl_down_sync(kFull, v.mx[p], off);
+  }
+  const int packed = __shfl_down_sync(kFull, v.out[0] | (v.out[1] << 1) | (v.bad << 2), off);
+  r.out[0] = packed & 1, r.out[1] = (packed >> 1) & 1, r.bad = packed >> 2;
+  return r;
+}
+__device__ __forceinline__ XRun x_shfl_up(const XRun& v, int off) {
+  XRun r;
+#pragma unroll
+  for (int p = 0; p < 2; ++p) {
+    r.K[p] = __shfl_up_sync(kFull, v.K[p], off);
+    r.mn[p] = __shfl_up_sync(kFull, v.mn[p], off);
+    r.mx[p] = __shfl_up_sync(kFull, v.mx[p], off);
+  }
+  const int packed = __shfl_up_sync(kFull, v.out[0] | (v.out[1] << 1) | (v.bad << 2), off);
+  r.out[0] = packed & 1, r.out[1] = (packed >> 1) & 1, r.bad = packed >> 2;
+  return r;
+}
 
 // e = floor(log2 |v|) for a normal v whose ulp 2^(e−52) and 2^(52−e) are both normal doubles;
 // otherwise returns false.
@@ -104,15 +163,50 @@ __device__ __forceinline__ bool x_binade(double v, int& e) {
 __device__ __forceinline__ double x_pow2(int p) {  // 2^p, p in [−1022, 1023]
   return __longlong_as_double(static_cast<long long>(p + 1023) << 52);
 }
-// k = rint(t/u) with inv_u = 1/u (powers of two: t·inv_u is exact unless it under/overflows);
-// returns false for a tie, |t/u| ≥ 2^51, or a non-finite t.
-__device__ __forceinline__ bool x_count(double t, double inv_u, long long& k) {
+// A term in units of u (inv_u = 1/u, powers of two: t·inv_u is exact unless it under/overflows):
+// false for |t/u| ≥ 2^51 or a non-finite t; else kf = rint(t/u), or floor(t/u) for a tie.
+__device__ __forceinline__ bool x_term(double t, double inv_u, long long& kf, bool& tie) {
   const double q = t * inv_u;
   if (!(fabs(q) < 2251799813685248.0)) return false;  // 2^51; also NaN / inf
   const double f = floor(q);
-  if (q - f == 0.5) return false;  // a tie: rounding depends on the partial sum's last bit
-  k = static_cast<long long>(rint(q));
+  tie = q - f == 0.5;
+  kf = static_cast<long long>(tie ? f : rint(q));
   return true;
+}
+// The step of S with parity `par` for a term (kf, tie): returns k; par becomes S + k's parity.
+__device__ __forceinline__ long long x_step(long long kf, bool tie, int& par) {
+  long long k = kf;
+  if (tie) {
+    k += (par + kf) & 1;  // to the even neighbour
+    par = 0;
+  } else {
+    par = static_cast<int>((par + k) & 1);
+  }
+  return k;
+}
+// The XRun of up to kXPer terms v[0, cnt).
+__device__ __forceinline__ XRun x_run_of(const double* v, int cnt, double inv_u) {
+  XRun r = x_identity();
+  long long kf[kXPer];
+  bool tie[kXPer];
+#pragma unroll
+  for (int q = 0; q < kXPer; ++q)
+    if (q < cnt && !x_term(v[q], inv_u, kf[q], tie[q])) r.bad = 1, kf[q] = 0, tie[q] = false;
+#pragma unroll
+  for (int p = 0; p < 2; ++p) {
+    int par = p;
+    long long K = 0;
+#pragma unroll
+    for (int q = 0; q < kXPer; ++q)
+      if (q < cnt) {
+        K += x_step(kf[q], tie[q], par);
+        r.mn[p] = min(r.mn[p], K);
+        r.mx[p] = max(r.mx[p], K);
+      }
+    r.K[p] = K;
+    r.out[p] = par;
+  }
+  return r;
 }
 // |S| inside [2^52 + 1, 2^53 − 1] with the sign of S0.
 __device__ __forceinline__ bool x_inside(long long S0, long long S) {
@@ -188,8 +282,7 @@ static __global__ void __launch_bounds__(kXThreads) k_xstat(const XChain* ch, co
 static __global__ void __launch_bounds__(kXThreads) k_xagg(const XChain* ch, const int* tile_chain,
                                                            const XTileStat* st, XTileAgg* ag, const int* skip) {
   __shared__ double shd[32];
-  __shared__ long long shl[32];
-  __shared__ int shi[32];
+  __shared__ XRun shr[kXThreads / 32];
   if (skip && *skip) return;
   const int tile = blockIdx.x;
   const XChain c = ch[tile_chain[tile]];
@@ -204,29 +297,41 @@ static __global__ void __launch_bounds__(kXThreads) k_xagg(const XChain* ch, con
   const bool guess = x_binade(s0, e0) && x_binade(lo_v, e1) && x_binade(hi_v, e2) && e0 == e1 && e0 == e2 &&
                      (s0 > 0) == (lo_v > 0) && (s0 > 0) == (hi_v > 0);
   if (!guess) {
-    if (threadIdx.x == 0) ag[tile] = XTileAgg{0.0, 0, 0, 0, 0, 0};
+    if (threadIdx.x == 0) {
+      XTileAgg g;
+      g.u = 0.0;
+      g.r = x_identity();
+      g.r.bad = 1;
+      ag[tile] = g;
+    }
     return;
   }
   const double inv_u = x_pow2(52 - e0);
   const long long i0 = a + static_cast<long long>(threadIdx.x) * kXPer;
-  long long run = 0, mn = LLONG_MAX, mx = LLONG_MIN;
-  int ok = 1;
+  double v[kXPer];
+  int cnt = 0;
 #pragma unroll
-  for (int q = 0; q < kXPer; ++q)
-    if (i0 + q < b) {
-      long long k = 0;
-      ok &= x_count(c.t[i0 + q], inv_u, k) ? 1 : 0;
-      run += k;
-      mn = run < mn ? run : mn;
-      mx = run > mx ? run : mx;
-    }
-  long long total;
-  const long long before = x_block_excl(run, total, shl);
-  if (mn != LLONG_MAX) mn += before, mx += before;
-  mn = x_block_reduce(mn, [](long long x, long long y) { return x < y ? x : y; }, shl);
-  mx = x_block_reduce(mx, [](long long x, long long y) { return x > y ? x : y; }, shl);
-  ok = x_block_reduce(ok, [](int x, int y) { return x & y; }, shi);
-  if (threadIdx.x == 0) ag[tile] = XTileAgg{x_pow2(e0 - 52), total, mn, mx, ok, 0};
+  for (int q = 0; q < kXPer; ++q) {
+    v[q] = i0 + q < b ? c.t[i0 + q] : 0.0;
+    cnt += i0 + q < b ? 1 : 0;
+  }
+  XRun r = x_run_of(v, cnt, inv_u);
+  // ordered reduction: lanes, then the block's warps in order
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int off = 1; off < 32; off <<= 1) {
+    const XRun o = x_shfl_down(r, off);
+    if ((lane & (2 * off - 1)) == 0 && lane + off < 32) r = x_compose(r, o);
+  }
+  if (lane == 0) shr[wid] = r;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    XRun t = shr[0];
+    for (int w = 1; w < kXThreads / 32; ++w) t = x_compose(t, shr[w]);
+    XTileAgg g;
+    g.u = x_pow2(e0 - 52);
+    g.r = t;
+    ag[tile] = g;
+  }
 }
 
 // The chain over t[a, b) from the exact partial sum s, by windows of 32·kXPer terms (all 32 lanes
@@ -246,48 +351,51 @@ __device__ __forceinline__ double x_window_walk(const double* __restrict__ t, lo
     }
     const double u = x_pow2(e - 52), inv_u = x_pow2(52 - e);
     const long long S0 = static_cast<long long>(s * inv_u);
+    const int p0 = static_cast<int>(S0 & 1);
     const long long i0 = pos + static_cast<long long>(lane) * kXPer;
     double v[kXPer];
-    long long pk[kXPer];  // this lane's inclusive running integer sums
-    int first = kXPer;    // this lane's first invalid position (kXPer: none)
-    long long run = 0;
+    int cnt = 0;
 #pragma unroll
     for (int q = 0; q < kXPer; ++q) {
       v[q] = i0 + q < b ? t[i0 + q] : 0.0;
-      long long k = 0;
-      const bool ok = i0 + q < b && x_count(v[q], inv_u, k);
-      run += k;
-      pk[q] = run;
-      if (!ok && first == kXPer && i0 + q < b) first = q;
+      cnt += i0 + q < b ? 1 : 0;
     }
-    long long inc = run;  // warp inclusive scan of the lane totals
+    XRun inc = x_run_of(v, cnt, inv_u);  // warp inclusive scan in lane order
     for (int off = 1; off < 32; off <<= 1) {
-      const long long o = __shfl_up_sync(kFull, inc, off);
-      if (lane >= off) inc += o;
+      const XRun o = x_shfl_up(inc, off);
+      if (lane >= off) inc = x_compose(o, inc);
     }
-    const long long before = inc - run;
+    XRun ex = x_shfl_up(inc, 1);
+    if (lane == 0) ex = x_identity();
+    // this lane's terms with its exact incoming state: the first invalid position
+    long long run = p0 ? ex.K[1] : ex.K[0], committed = run;
+    int par = p0 ? ex.out[1] : ex.out[0], first = kXPer;
+    double vf = 0.0;
 #pragma unroll
-    for (int q = 0; q < kXPer; ++q)
-      if (q < first && i0 + q < b && !x_inside(S0, S0 + before + pk[q])) first = q;
-    const bool has_end = i0 < b;  // this lane holds at least one term
-    const unsigned fail = __ballot_sync(kFull, has_end && first < kXPer && i0 + first < b);
+    for (int q = 0; q < kXPer; ++q) {
+      if (q < cnt && first == kXPer) {
+        long long kf;
+        bool tie;
+        bool ok = x_term(v[q], inv_u, kf, tie);
+        if (ok) {
+          int p2 = par;
+          const long long k = x_step(kf, tie, p2);
+          ok = x_inside(S0, S0 + run + k);
+          if (ok) run += k, par = p2;
+        }
+        if (!ok) first = q, committed = run, vf = v[q];
+      }
+    }
+    const unsigned fail = __ballot_sync(kFull, first < kXPer);
     if (fail == 0) {
-      const long long total = __shfl_sync(kFull, inc, 31);
+      const long long total = __shfl_sync(kFull, p0 ? inc.K[1] : inc.K[0], 31);
       s = static_cast<double>(S0 + total) * u;
       pos = pos + 32LL * kXPer < b ? pos + 32LL * kXPer : b;
       continue;
     }
     const int fl = __ffs(fail) - 1;
     const int fq = __shfl_sync(kFull, first, fl);
-    long long committed = before;  // the running sum just before this lane's first invalid term
-#pragma unroll
-    for (int q = 0; q < kXPer; ++q)
-      if (q + 1 == first) committed = before + pk[q];
     committed = __shfl_sync(kFull, committed, fl);
-    double vf = 0.0;
-#pragma unroll
-    for (int q = 0; q < kXPer; ++q)
-      if (q == fq) vf = v[q];
     vf = __shfl_sync(kFull, vf, fl);
     s = static_cast<double>(S0 + committed) * u;  // the valid prefix (nothing when it is empty)
     s += vf;                                      // the failing term, as the sequential chain adds it
@@ -295,46 +403,57 @@ __device__ __forceinline__ double x_window_walk(const double* __restrict__ t, lo
     pos += f + 1;
     if (f < kXPer) {  // little progress: a plain run of up to 32 terms before the next window
       const long long rem = b - pos;
-      const int cnt = rem <= 0 ? 0 : (rem < 32 ? static_cast<int>(rem) : 32);
-      const double w = lane < cnt ? t[pos + lane] : 0.0;
-      for (int j = 0; j < cnt; ++j) s += __shfl_sync(kFull, w, j);
-      pos += cnt;
+      const int n2 = rem <= 0 ? 0 : (rem < 32 ? static_cast<int>(rem) : 32);
+      const double w = lane < n2 ? t[pos + lane] : 0.0;
+      for (int j = 0; j < n2; ++j) s += __shfl_sync(kFull, w, j);
+      pos += n2;
     }
   }
   return s;
 }
 
-// One warp per chain: tiles in order (committed whole when valid for the exact s), the rest
-// walked in windows.
-static __global__ void k_xchain(const XChain* ch, int nch, const XTileAgg* ag, const int* skip) {
+// One warp per chain (4 warps per block): tiles in order (committed whole when valid for the
+// exact s), the rest walked in windows. The tile summaries are brought into shared memory 32 at a
+// time, so the walk over them waits on no global load.
+constexpr int kXChainWarps = 4;
+static __global__ void __launch_bounds__(32 * kXChainWarps) k_xchain(const XChain* ch, int nch, const XTileAgg* ag,
+                                                                      const int* skip) {
+  __shared__ XTileAgg sg[kXChainWarps][32];
   if (skip && *skip) return;
   const int warp = static_cast<int>((blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x) >> 5);
-  const int lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
   if (warp >= nch) return;
   const XChain c = ch[warp];
   double s = c.init;
   if (c.ntiles == 0) {
     s = x_window_walk(c.t, c.lo, c.hi, s);
   } else {
-    for (int g = 0; g < c.ntiles; g += 32) {
-      XTileAgg mine{0.0, 0, 0, 0, 0, 0};
-      if (g + lane < c.ntiles) mine = ag[c.tile0 + g + lane];
-      const int cnt = c.ntiles - g < 32 ? c.ntiles - g : 32;
+    for (int g0 = 0; g0 < c.ntiles; g0 += 32) {
+      const int cnt = c.ntiles - g0 < 32 ? c.ntiles - g0 : 32;
+      __syncwarp();
+      if (lane < cnt) sg[wl][lane] = ag[c.tile0 + g0 + lane];
+      __syncwarp();
       for (int j = 0; j < cnt; ++j) {
-        const double u = __shfl_sync(kFull, mine.u, j);
-        const long long K = __shfl_sync(kFull, mine.K, j), pmin = __shfl_sync(kFull, mine.pmin, j);
-        const long long pmax = __shfl_sync(kFull, mine.pmax, j);
-        const int ok = __shfl_sync(kFull, mine.ok, j);
-        bool commit = false;
-        int e;
-        if (ok && u != 0.0 && x_binade(s, e) && x_pow2(e - 52) == u) {
-          const long long S0 = static_cast<long long>(s * x_pow2(52 - e));
-          commit = x_inside(S0, S0 + pmin) && x_inside(S0, S0 + pmax);
-          if (commit) s = static_cast<double>(S0 + K) * u;
+        // lane 0 decides from the tile's summary; every lane follows its decision
+        int commit = 0;
+        if (lane == 0) {
+          const XTileAgg& G = sg[wl][j];
+          int e;
+          if (!G.r.bad && G.u != 0.0 && x_binade(s, e) && x_pow2(e - 52) == G.u) {
+            const long long S0 = static_cast<long long>(s * x_pow2(52 - e));
+            const bool odd = (S0 & 1) != 0;
+            const long long mn = odd ? G.r.mn[1] : G.r.mn[0], mx = odd ? G.r.mx[1] : G.r.mx[0];
+            if (x_inside(S0, S0 + mn) && x_inside(S0, S0 + mx)) {
+              s = static_cast<double>(S0 + (odd ? G.r.K[1] : G.r.K[0])) * G.u;
+              commit = 1;
+            }
+          }
         }
+        commit = __shfl_sync(kFull, commit, 0);
+        s = __shfl_sync(kFull, s, 0);
         if (!commit) {
           long long a, b;
-          x_tile_range(c, c.tile0 + g + j, a, b);
+          x_tile_range(c, c.tile0 + g0 + j, a, b);
           s = x_window_walk(c.t, a, b, s);
         }
       }
@@ -440,11 +559,12 @@ class SumPlan {
         B200_LAUNCH_CHECK();
       }
       if (n1_ > 0) {
-        k_xchain<<<(n1_ + 3) / 4, 128, 0, st>>>(c1, n1_, ta, skip_);
+        k_xchain<<<(n1_ + kXChainWarps - 1) / kXChainWarps, 32 * kXChainWarps, 0, st>>>(c1, n1_, ta, skip_);
         B200_LAUNCH_CHECK();
       }
       if (n2_ > 0) {
-        k_xchain<<<(n2_ + 3) / 4, 128, 0, st>>>(reinterpret_cast<const XChain*>(seg2_.get()), n2_, ta, skip_);
+        k_xchain<<<(n2_ + kXChainWarps - 1) / kXChainWarps, 32 * kXChainWarps, 0, st>>>(
+            reinterpret_cast<const XChain*>(seg2_.get()), n2_, ta, skip_);
         B200_LAUNCH_CHECK();
       }
     } else if (nt_ > 0) {

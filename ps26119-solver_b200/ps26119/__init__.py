@@ -413,7 +413,8 @@ def solve_lp_device(m, n, sense, offset, ptrs, precision="fp64", tolerance=1e-8,
 
 
 def solve_batch(c, A, row_lower, row_upper, col_lower=None, col_upper=None, scenarios=(), sense=1, offset=0.0,
-                tolerance=1e-8, time_limit=3600.0, iteration_limit=0, engine=None, verbosity=0) -> list[Result]:
+                tolerance=1e-8, time_limit=3600.0, iteration_limit=0, engine=None, verbosity=0,
+                precision="fp64") -> list[Result]:
     """ps26119::solve_batch on the GPU: the base LP (as :func:`solve_lp`) and a list of scenarios,
     each a dict with any of obj, col_lower, col_upper, row_lower, row_upper (missing = the
     base's). Returns one :class:`Result` per scenario (x, y, z set when the scenario has a point)."""
@@ -439,7 +440,7 @@ def solve_batch(c, A, row_lower, row_upper, col_lower=None, col_upper=None, scen
                 a = np.ascontiguousarray(scenarios[k][key], dtype=np.float64)
                 keep.append(a)
                 setattr(sc[t], key, _ptr(a))
-    opt = _options("r2hpdhg", "fp64", True, tolerance, time_limit, iteration_limit, verbosity, 1)
+    opt = _options("r2hpdhg", precision, True, tolerance, time_limit, iteration_limit, verbosity, 1)
     eo = engine_options(**(engine or {}))
     res = (_Result * max(1, K))()
     x, y, z = np.full((K, n), np.nan), np.full((K, m), np.nan), np.full((K, n), np.nan)

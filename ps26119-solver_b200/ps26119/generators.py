@@ -20,7 +20,12 @@ Generators (sizes are parameters; the named configurations fix them):
   construction) with inequality slack proportional to a per-period demand
   U(50, 150) x (1 + 0.3 sin(2 pi h / 24)).
 * :func:`scenarios` — K scenarios of a base LP whose objective and finite row bounds are
-  multiplied element-wise by lognormal(0, sigma) factors.
+  multiplied element-wise by lognormal(0, sigma) factors. On the staircase LP this makes most
+  scenarios infeasible (the equality rows' right-hand sides no longer agree with each other).
+* :func:`feasible_scenarios` — K scenarios that stay feasible: the base's interior point x* is
+  multiplied by lognormal(0, sigma) factors (clipped to the column bounds), the row bounds are
+  rebuilt around it with the base's slacks times lognormal factors, and the objective is
+  multiplied by lognormal factors.
 
 All randomness comes from ``numpy.random.Generator(PCG64(seed))``.
 """
@@ -30,7 +35,8 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-__all__ = ["Lp", "random_lp", "staircase_lp", "scenarios", "from_dense", "csc_from_triplets"]
+__all__ = ["Lp", "random_lp", "staircase_lp", "scenarios", "feasible_scenarios", "from_dense",
+           "csc_from_triplets"]
 
 
 @dataclass
@@ -184,5 +190,28 @@ def scenarios(base: Lp, K: int, sigma: float = 0.1, seed: int = 1) -> list[dict]
         fb = np.exp(sigma * rng.standard_normal(base.num_rows))
         rl = np.where(np.isfinite(base.row_lower), base.row_lower * fb, base.row_lower)
         ru = np.where(np.isfinite(base.row_upper), base.row_upper * fb, base.row_upper)
+        out.append({"obj": base.c * fc, "row_lower": rl, "row_upper": ru})
+    return out
+
+
+def feasible_scenarios(base: Lp, K: int, sigma: float = 0.1, seed: int = 1) -> list[dict]:
+    """K feasible scenarios of a base LP that carries an interior point ``meta["x0"]`` (the
+    generators above record it): x' = clip(x0 · lognormal(0, sigma), col bounds), row bounds
+    around A x' (equality rows: A x'; one-sided rows: A x' ∓ base slack · lognormal(0, sigma)),
+    objective c · lognormal(0, sigma). Same dict format as :func:`scenarios`."""
+    x0 = np.asarray(base.meta["x0"], dtype=np.float64)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    ax0 = base.row_activity(x0)
+    lo_slack = np.where(np.isfinite(base.row_lower), ax0 - base.row_lower, np.inf)
+    up_slack = np.where(np.isfinite(base.row_upper), base.row_upper - ax0, np.inf)
+    eq = base.row_lower == base.row_upper
+    out = []
+    for _ in range(K):
+        xs = np.clip(x0 * np.exp(sigma * rng.standard_normal(base.num_cols)), base.col_lower, base.col_upper)
+        ax = base.row_activity(xs)
+        fb = np.exp(sigma * rng.standard_normal(base.num_rows))
+        rl = np.where(eq, ax, ax - lo_slack * fb)
+        ru = np.where(eq, ax, ax + up_slack * fb)
+        fc = np.exp(sigma * rng.standard_normal(base.num_cols))
         out.append({"obj": base.c * fc, "row_lower": rl, "row_upper": ru})
     return out
