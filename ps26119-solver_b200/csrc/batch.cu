@@ -496,7 +496,7 @@ class BatchEngine {
   double elapsed() const { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0_).count(); }
   void upload_model();
   void setup();
-  void launch_sums(const ISegs& segs);
+  void launch_sums(const ISegs& segs, bool exact);
   void launch_residual(bool distances);
   void launch_kkt();
   template <class Epi>
@@ -570,10 +570,11 @@ void BatchEngine::spmm(int rows, const int* rp, const int* col, const double* va
   ++launches_;
 }
 
-void BatchEngine::launch_sums(const ISegs& segs) {
+// exact: each slot's sums in the reference's order (one lane per slot); else the fixed split.
+void BatchEngine::launch_sums(const ISegs& segs, bool exact) {
   if (segs.n == 0 || W_ == 0) return;
   const int gx = (W_ + 31) / 32;
-  if (o_.exact) {
+  if (exact) {
     k_isum_seq<<<dim3(gx, segs.n), 32, 0, st_>>>(segs, W_, res_.get());
     B200_LAUNCH_CHECK();
     ++launches_;
@@ -669,7 +670,7 @@ void BatchEngine::setup() {
   segs.s[2] = {mv_[TSB2].get(), m_, nullptr, 0, 0.0, kBSb2};
   segs.s[3] = {nv_[TSC2].get(), n_, nullptr, 0, 0.0, kBSc2};
   segs.n = 4;
-  launch_sums(segs);
+  launch_sums(segs, true);  // the rescaling sums enter the scaled data: always the reference's order
   B200_CHECK(cudaMemcpyAsync(h_res_.get(), res_.get(), static_cast<std::size_t>(W_) * kRes * sizeof(double),
                              cudaMemcpyDeviceToHost, st_));
   B200_CHECK(cudaStreamSynchronize(st_));
@@ -717,7 +718,7 @@ void BatchEngine::epoch_body(bool r0_section) {
       g.s[1] = {mv_[TPY].get(), m_, nullptr, 0, 0.0, kBPy0};
       g.s[2] = {mv_[TCR].get(), m_, nullptr, 0, 0.0, kBCr0};
       g.n = 3;
-      launch_sums(g);
+      launch_sums(g, o_.exact);
     }
     if (s == 0) B200_CHECK(cudaEventRecordWithFlags(ev_[2], st_, cudaEventRecordExternal));
   }
@@ -882,14 +883,18 @@ void BatchEngine::run(std::vector<BatchOutcome>& out) {
       g.s[0] = {nv_[TPX].get(), n_, nullptr, 0, 0.0, kBPx};
       g.s[1] = {mv_[TPY].get(), m_, nullptr, 0, 0.0, kBPy};
       g.s[2] = {mv_[TCR].get(), m_, nullptr, 0, 0.0, kBCr};
-      g.s[3] = {nv_[TDXN].get(), n_, nullptr, 0, 0.0, kBDxn};
-      g.s[4] = {mv_[TDYN].get(), m_, nullptr, 0, 0.0, kBDyn};
-      g.s[5] = {mv_[TRP2].get(), m_, nullptr, 0, 0.0, kBRp2};
-      g.s[6] = {mv_[TDR].get(), m_, nv_[TDC].get(), n_, 0.0, kBD};
-      g.s[7] = {mv_[TRDR].get(), m_, nv_[TRDC].get(), n_, 0.0, kBRd2};
-      g.s[8] = {nv_[TP].get(), n_, nullptr, 0, 0.0, kBP};
-      g.n = 9;
-      launch_sums(g);
+      g.s[3] = {mv_[TRP2].get(), m_, nullptr, 0, 0.0, kBRp2};
+      g.s[4] = {mv_[TDR].get(), m_, nv_[TDC].get(), n_, 0.0, kBD};
+      g.s[5] = {mv_[TRDR].get(), m_, nv_[TRDC].get(), n_, 0.0, kBRd2};
+      g.s[6] = {nv_[TP].get(), n_, nullptr, 0, 0.0, kBP};
+      g.n = 7;
+      launch_sums(g, o_.exact);
+      // the restart distances enter each slot's primal weight ω: always the reference's order
+      ISegs d{};
+      d.s[0] = {nv_[TDXN].get(), n_, nullptr, 0, 0.0, kBDxn};
+      d.s[1] = {mv_[TDYN].get(), m_, nullptr, 0, 0.0, kBDyn};
+      d.n = 2;
+      launch_sums(d, true);
     }
     B200_CHECK(cudaMemcpyAsync(h_res_.get(), res_.get(), static_cast<std::size_t>(W_) * kRes * sizeof(double),
                                cudaMemcpyDeviceToHost, st_));

@@ -193,7 +193,7 @@ class Engine {
   DevBuf<double> res_;
   PinnedBuf<double> hres_;
   DevBuf<double> rt_, kt_, rayt_, xo_, yo_, r1_, d1_, r2_, d2_, objt_;
-  SumPlan plan_r0_, plan_res_, plan_kkt_, plan_ray1_, plan_ray2_, plan_obj_, plan_chk_;
+  SumPlan plan_r0_, plan_res_, plan_pid_, plan_kkt_, plan_ray1_, plan_ray2_, plan_obj_, plan_chk_;
   cudaGraphExec_t g_epoch_[2] = {nullptr, nullptr};
   cudaGraphExec_t g_check_[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
   cudaGraphExec_t g_pdlp_[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};         // [precision][phase]
@@ -272,8 +272,10 @@ void Engine::build_plans() {
   plan_res_.add(px, 0, n, 0.0, SumOrder::kChunk64, R + kPx);
   plan_res_.add(py, 0, m, 0.0, SumOrder::kChunk64, R + kPy);
   plan_res_.add(cross, 0, m, 0.0, SumOrder::kChunk64, R + kCross);
-  plan_res_.add(dxn, 0, n, 0.0, SumOrder::kChunk64, R + kDxn2);
-  plan_res_.add(dyn, 0, m, 0.0, SumOrder::kChunk64, R + kDyn2);
+  // the restart distances enter the PID primal weight ω (and so every later step): always the
+  // reference's order, whatever the mode (positive terms: the exact chains are cheap on them)
+  plan_pid_.add(dxn, 0, n, 0.0, SumOrder::kChunk64, R + kDxn2);
+  plan_pid_.add(dyn, 0, m, 0.0, SumOrder::kChunk64, R + kDyn2);
   // KKT: host loops of kkt_general (rows, then columns for the continuing sums)
   double* K0 = kt_.get();
   const long long L = m + n;
@@ -297,6 +299,7 @@ void Engine::build_plans() {
   plan_chk_.add(O, 0, n, 0.0, SumOrder::kSeq, R + kChkPrimal);
   plan_r0_.build(o_.exact, skip_r0_flag(params_.get()), st_);
   plan_res_.build(o_.exact, nullptr, st_);
+  plan_pid_.build(true, nullptr, st_);
   plan_kkt_.build(o_.exact, nullptr, st_);
   plan_ray1_.build(o_.exact, nullptr, st_);
   plan_ray2_.build(o_.exact, nullptr, st_);
@@ -322,6 +325,10 @@ void Engine::launch_residual(bool with_restart_terms, const int* skip, SumPlan& 
   launch_slab_tma<T>(m, sp_.a_rp.get(), sp_.a_col.get(), sp_.A_val<T>(), v.dx.get(), e, st_, nullptr, err());
   plan.launch(st_);
   B200_COUNT(2 + plan.kernel_count());
+  if (with_restart_terms) {
+    plan_pid_.launch(st_);
+    B200_COUNT(plan_pid_.kernel_count());
+  }
 }
 
 void Engine::launch_kkt_original() {
@@ -510,7 +517,7 @@ double Engine::initial_primal_weight() {  // engine.cpp:207-218
   SumPlan p;
   p.add(tm.get(), 0, m, 0.0, SumOrder::kSeq, s.get());
   p.add(tn.get(), 0, n, 0.0, SumOrder::kSeq, s.get() + 1);
-  p.build(o_.exact, nullptr, st_);
+  p.build(true, nullptr, st_);  // ω0 enters every step: always the reference's order
   p.launch(st_);
   double h[2];
   B200_CHECK(cudaMemcpyAsync(h, s.get(), sizeof h, cudaMemcpyDeviceToHost, st_));
@@ -1024,7 +1031,7 @@ EngineResult Engine::run_pdlp(const DeviceOutputs& out) {
   hres2_.alloc(kNumSlots);
   plan_dist_.add(rt_.get(), 0, nn, 0.0, SumOrder::kChunk64, res_.get() + kPx);
   plan_dist_.add(rt_.get() + 2 * nn, 0, mm, 0.0, SumOrder::kChunk64, res_.get() + kPy);
-  plan_dist_.build(o_.exact, nullptr, st_);
+  plan_dist_.build(true, nullptr, st_);  // the distances enter ω: always the reference's order
   mixed_now_ = o_.mixed;
   double omega = initial_primal_weight();
   if (mixed_now_) init_iterates<float>();

@@ -264,8 +264,8 @@ struct ScaledDevice {
     SumPlan pal, pbn;
     pal.add(terms.get(), 0, n, 0.0, SumOrder::kSeq, out.get());
     pbn.add(terms.get(), 0, n, 0.0, SumOrder::kSeq, out.get() + 1);
-    pal.build(exact, nullptr, st);
-    pbn.build(exact, nullptr, st);
+    pal.build(true, nullptr, st);  // α and β enter η = 0.998/‖Ã‖₂: always the reference's order
+    pbn.build(true, nullptr, st);
     std::vector<double> alpha, beta, h(2 * static_cast<std::size_t>(K));
     double theta = 0, theta_old = -1;
     int stagnant = 0;
@@ -373,7 +373,7 @@ struct ScaledDevice {
     SumPlan p;
     p.add(tmp_m.get(), 0, m, 0.0, SumOrder::kSeq, sums.get());
     p.add(tmp_n.get(), 0, n, 0.0, SumOrder::kSeq, sums.get() + 1);
-    p.build(exact, nullptr, st);
+    p.build(true, nullptr, st);  // norms that enter the scaled data: always the reference's order
     p.launch(st);
     double h[2];
     B200_CHECK(cudaMemcpyAsync(h, sums.get(), sizeof h, cudaMemcpyDeviceToHost, st));

