@@ -95,9 +95,15 @@ struct XRun {
   int out[2];
   int bad;
 };
+// A tile's summary: its terms before `split` counted in the grid u (the binade of the tile's
+// approximate start), the term at `split` (where the approximate running sum leaves that binade;
+// split = −1: it never does) added as a plain fp64 addition, the terms after it counted in the
+// grid u1 of the binade the running sum moved to. u = 0: no usable guess (bad is set).
 struct XTileAgg {
-  double u;  // the binade's ulp the run is counted in (0: no guess)
-  XRun r;
+  double u, u1;
+  XRun pre, suf;
+  int split;
+  int pad;
 };
 
 constexpr long long kX52 = 1LL << 52, kX53 = 1LL << 53;
@@ -208,6 +214,32 @@ __device__ __forceinline__ XRun x_run_of(const double* v, int cnt, double inv_u)
   }
   return r;
 }
+// The XRun of the terms v[q] whose bit q is set in `mask` (the others left out).
+__device__ __forceinline__ XRun x_run_masked(const double* v, unsigned mask, double inv_u) {
+  XRun r = x_identity();
+  long long kf[kXPer];
+  bool tie[kXPer];
+#pragma unroll
+  for (int q = 0; q < kXPer; ++q) {
+    kf[q] = 0, tie[q] = false;
+    if (((mask >> q) & 1u) && !x_term(v[q], inv_u, kf[q], tie[q])) r.bad = 1, kf[q] = 0, tie[q] = false;
+  }
+#pragma unroll
+  for (int p = 0; p < 2; ++p) {
+    int par = p;
+    long long K = 0;
+#pragma unroll
+    for (int q = 0; q < kXPer; ++q)
+      if ((mask >> q) & 1u) {
+        K += x_step(kf[q], tie[q], par);
+        r.mn[p] = min(r.mn[p], K);
+        r.mx[p] = max(r.mx[p], K);
+      }
+    r.K[p] = K;
+    r.out[p] = par;
+  }
+  return r;
+}
 // |S| inside [2^52 + 1, 2^53 − 1] with the sign of S0.
 __device__ __forceinline__ bool x_inside(long long S0, long long S) {
   return S0 > 0 ? (S >= kX52 + 1 && S <= kX53 - 1) : (S <= -(kX52 + 1) && S >= -(kX53 - 1));
@@ -279,87 +311,148 @@ static __global__ void __launch_bounds__(kXThreads) k_xstat(const XChain* ch, co
   if (threadIdx.x == 0) st[tile] = XTileStat{total, mn, mx, bad, 0};
 }
 
-static __global__ void __launch_bounds__(kXThreads) k_xagg(const XChain* ch, const int* tile_chain,
-                                                           const XTileStat* st, XTileAgg* ag, const int* skip) {
-  __shared__ double shd[32];
-  __shared__ XRun shr[kXThreads / 32];
-  if (skip && *skip) return;
-  const int tile = blockIdx.x;
-  const XChain c = ch[tile_chain[tile]];
-  long long a, b;
-  x_tile_range(c, tile, a, b);
-  // the approximate running sum at the tile's start
-  double pre = 0.0;
-  for (int k = c.tile0 + static_cast<int>(threadIdx.x); k < tile; k += blockDim.x) pre += st[k].sum;
-  pre = x_block_reduce(pre, [](double x, double y) { return x + y; }, shd);
-  const double s0 = c.init + pre, lo_v = s0 + st[tile].pmin, hi_v = s0 + st[tile].pmax;
-  int e0, e1, e2;
-  const bool guess = x_binade(s0, e0) && x_binade(lo_v, e1) && x_binade(hi_v, e2) && e0 == e1 && e0 == e2 &&
-                     (s0 > 0) == (lo_v > 0) && (s0 > 0) == (hi_v > 0);
-  if (!guess) {
-    if (threadIdx.x == 0) {
-      XTileAgg g;
-      g.u = 0.0;
-      g.r = x_identity();
-      g.r.bad = 1;
-      ag[tile] = g;
-    }
-    return;
-  }
-  const double inv_u = x_pow2(52 - e0);
-  const long long i0 = a + static_cast<long long>(threadIdx.x) * kXPer;
-  double v[kXPer];
-  int cnt = 0;
-#pragma unroll
-  for (int q = 0; q < kXPer; ++q) {
-    v[q] = i0 + q < b ? c.t[i0 + q] : 0.0;
-    cnt += i0 + q < b ? 1 : 0;
-  }
-  XRun r = x_run_of(v, cnt, inv_u);
-  // ordered reduction: lanes, then the block's warps in order
+// Ordered reduction of the block's per-thread runs (thread order); the result in thread 0.
+__device__ __forceinline__ XRun x_block_ordered(XRun r, XRun* sh) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   for (int off = 1; off < 32; off <<= 1) {
     const XRun o = x_shfl_down(r, off);
     if ((lane & (2 * off - 1)) == 0 && lane + off < 32) r = x_compose(r, o);
   }
-  if (lane == 0) shr[wid] = r;
   __syncthreads();
+  if (lane == 0) sh[wid] = r;
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int w = 1; w < kXThreads / 32; ++w) r = x_compose(r, sh[w]);
+  return r;
+}
+
+static __global__ void __launch_bounds__(kXThreads) k_xagg(const XChain* ch, const int* tile_chain,
+                                                           const XTileStat* st, XTileAgg* ag, const int* skip) {
+  __shared__ double shd[32];
+  __shared__ int shi[32];
+  __shared__ XRun shr[kXThreads / 32];
+  __shared__ double sh_at_split;
+  if (skip && *skip) return;
+  const int tile = blockIdx.x;
+  const XChain c = ch[tile_chain[tile]];
+  long long a, b;
+  x_tile_range(c, tile, a, b);
+  // the approximate running sum at the tile's start (the approximate sums of the earlier tiles)
+  double pre = 0.0;
+  for (int k = c.tile0 + static_cast<int>(threadIdx.x); k < tile; k += blockDim.x) pre += st[k].sum;
+  pre = x_block_reduce(pre, [](double x, double y) { return x + y; }, shd);
+  const double s0 = c.init + pre;
+  int e0;
+  XTileAgg g;
+  g.u = g.u1 = 0.0;
+  g.split = -1;
+  g.pad = 0;
+  g.pre = g.suf = x_identity();
+  if (!x_binade(s0, e0)) {  // uniform over the block
+    if (threadIdx.x == 0) g.pre.bad = 1, ag[tile] = g;
+    return;
+  }
+  const long long i0 = a + static_cast<long long>(threadIdx.x) * kXPer;
+  double v[kXPer];
+  double run = 0.0;
+#pragma unroll
+  for (int q = 0; q < kXPer; ++q) {
+    v[q] = i0 + q < b ? c.t[i0 + q] : 0.0;
+    run += v[q];
+  }
+  // approximate running sums: the first position whose running sum leaves e0's binade
+  double total;
+  const double before = x_block_excl(run, total, shd);
+  const int base = static_cast<int>(threadIdx.x) * kXPer;
+  int first = INT_MAX;
+  double acc = s0 + before;
+#pragma unroll
+  for (int q = 0; q < kXPer; ++q)
+    if (i0 + q < b) {
+      acc += v[q];
+      int e;
+      if (first == INT_MAX && !(x_binade(acc, e) && e == e0 && (acc > 0) == (s0 > 0))) first = base + q;
+    }
+  const int split = x_block_reduce(first, [](int x, int y) { return x < y ? x : y; }, shi);
+  // the binade after the split: all later approximate running sums must share it
+  int e1 = e0, ok1 = 1;
+  if (split != INT_MAX) {
+    if (split >= base && split < base + kXPer) {
+      double acc2 = s0 + before;
+#pragma unroll
+      for (int q = 0; q < kXPer; ++q)
+        if (q <= split - base) acc2 += v[q];
+      sh_at_split = acc2;
+    }
+    __syncthreads();
+    const double after = sh_at_split;
+    ok1 = x_binade(after, e1) ? 1 : 0;
+    double acc3 = s0 + before;
+#pragma unroll
+    for (int q = 0; q < kXPer; ++q)
+      if (i0 + q < b) {
+        acc3 += v[q];
+        int e;
+        if (base + q > split && !(x_binade(acc3, e) && e == e1 && (acc3 > 0) == (after > 0))) ok1 = 0;
+      }
+    ok1 = x_block_reduce(ok1, [](int x, int y) { return x & y; }, shi);
+  }
+  unsigned mpre = 0, msuf = 0;
+#pragma unroll
+  for (int q = 0; q < kXPer; ++q)
+    if (i0 + q < b) {
+      if (base + q < split) mpre |= 1u << q;
+      else if (split != INT_MAX && base + q > split) msuf |= 1u << q;
+    }
+  const XRun rp = x_block_ordered(x_run_masked(v, mpre, x_pow2(52 - e0)), shr);
+  XRun rs = x_identity();
+  if (split != INT_MAX && ok1) rs = x_block_ordered(x_run_masked(v, msuf, x_pow2(52 - e1)), shr);
   if (threadIdx.x == 0) {
-    XRun t = shr[0];
-    for (int w = 1; w < kXThreads / 32; ++w) t = x_compose(t, shr[w]);
-    XTileAgg g;
     g.u = x_pow2(e0 - 52);
-    g.r = t;
+    g.pre = rp;
+    if (split != INT_MAX) {
+      g.split = split;
+      g.u1 = ok1 ? x_pow2(e1 - 52) : 0.0;
+      g.suf = rs;
+      if (!ok1) g.suf.bad = 1;
+    }
     ag[tile] = g;
   }
 }
 
 // The chain over t[a, b) from the exact partial sum s, by windows of 32·kXPer terms (all 32 lanes
-// call it with the same s and return the same s).
+// call it with the same s and return the same s). The next window's terms are requested before
+// the current one is evaluated, so a run of valid windows waits on memory once.
+__device__ __forceinline__ void x_load_window(const double* __restrict__ t, long long pos, long long b,
+                                              double (&v)[kXPer]) {
+  const long long i0 = pos + static_cast<long long>(threadIdx.x & 31) * kXPer;
+#pragma unroll
+  for (int q = 0; q < kXPer; ++q) v[q] = i0 + q < b ? t[i0 + q] : 0.0;
+}
 __device__ __forceinline__ double x_window_walk(const double* __restrict__ t, long long a, long long b, double s) {
   const int lane = threadIdx.x & 31;
   long long pos = a;
+  double v[kXPer], nx[kXPer];
+  x_load_window(t, pos, b, v);
   while (pos < b) {
     int e;
     if (!x_binade(s, e)) {  // zero, subnormal, inf or NaN: a plain sequential run of up to 32 terms
       const long long rem = b - pos;
       const int cnt = rem < 32 ? static_cast<int>(rem) : 32;
-      const double v = lane < cnt ? t[pos + lane] : 0.0;
-      for (int j = 0; j < cnt; ++j) s += __shfl_sync(kFull, v, j);
+      const double w = lane < cnt ? t[pos + lane] : 0.0;
+      for (int j = 0; j < cnt; ++j) s += __shfl_sync(kFull, w, j);
       pos += cnt;
+      x_load_window(t, pos, b, v);
       continue;
     }
+    x_load_window(t, pos + 32LL * kXPer, b, nx);  // the next window, if this one is valid
     const double u = x_pow2(e - 52), inv_u = x_pow2(52 - e);
     const long long S0 = static_cast<long long>(s * inv_u);
     const int p0 = static_cast<int>(S0 & 1);
     const long long i0 = pos + static_cast<long long>(lane) * kXPer;
-    double v[kXPer];
     int cnt = 0;
 #pragma unroll
-    for (int q = 0; q < kXPer; ++q) {
-      v[q] = i0 + q < b ? t[i0 + q] : 0.0;
-      cnt += i0 + q < b ? 1 : 0;
-    }
+    for (int q = 0; q < kXPer; ++q) cnt += i0 + q < b ? 1 : 0;
     XRun inc = x_run_of(v, cnt, inv_u);  // warp inclusive scan in lane order
     for (int off = 1; off < 32; off <<= 1) {
       const XRun o = x_shfl_up(inc, off);
@@ -391,6 +484,8 @@ __device__ __forceinline__ double x_window_walk(const double* __restrict__ t, lo
       const long long total = __shfl_sync(kFull, p0 ? inc.K[1] : inc.K[0], 31);
       s = static_cast<double>(S0 + total) * u;
       pos = pos + 32LL * kXPer < b ? pos + 32LL * kXPer : b;
+#pragma unroll
+      for (int q = 0; q < kXPer; ++q) v[q] = nx[q];
       continue;
     }
     const int fl = __ffs(fail) - 1;
@@ -408,13 +503,31 @@ __device__ __forceinline__ double x_window_walk(const double* __restrict__ t, lo
       for (int j = 0; j < n2; ++j) s += __shfl_sync(kFull, w, j);
       pos += n2;
     }
+    x_load_window(t, pos, b, v);
   }
   return s;
 }
 
-// One warp per chain (4 warps per block): tiles in order (committed whole when valid for the
-// exact s), the rest walked in windows. The tile summaries are brought into shared memory 32 at a
-// time, so the walk over them waits on no global load.
+// Commits the run r (counted in the grid u) onto the exact s when s lies in u's binade and every
+// running S stays inside it; returns false (s unchanged) otherwise.
+__device__ __forceinline__ bool x_commit(double& s, double u, const XRun& r) {
+  int e;
+  if (r.bad || u == 0.0 || !x_binade(s, e) || x_pow2(e - 52) != u) return false;
+  const long long S0 = static_cast<long long>(s * x_pow2(52 - e));
+  const bool odd = (S0 & 1) != 0;
+  if (r.mn[0] == LLONG_MAX) return true;  // an empty run
+  const long long mn = odd ? r.mn[1] : r.mn[0], mx = odd ? r.mx[1] : r.mx[0];
+  if (!x_inside(S0, S0 + mn) || !x_inside(S0, S0 + mx)) return false;
+  s = static_cast<double>(S0 + (odd ? r.K[1] : r.K[0])) * u;
+  return true;
+}
+
+// One warp per chain (4 warps per block): tiles in order, the rest walked in windows. The tile
+// summaries are brought into shared memory 32 at a time; the lanes take one tile each and a warp
+// scan of their XRuns gives every tile its exact incoming S, so one step commits every tile up
+// to the first one that is not valid for the exact s or whose running sum changes binade. Such a
+// tile is taken on its own: its part before the change, the changing term as a plain addition,
+// its part after; what does not commit is walked in windows.
 constexpr int kXChainWarps = 4;
 static __global__ void __launch_bounds__(32 * kXChainWarps) k_xchain(const XChain* ch, int nch, const XTileAgg* ag,
                                                                       const int* skip) {
@@ -433,29 +546,64 @@ static __global__ void __launch_bounds__(32 * kXChainWarps) k_xchain(const XChai
       __syncwarp();
       if (lane < cnt) sg[wl][lane] = ag[c.tile0 + g0 + lane];
       __syncwarp();
-      for (int j = 0; j < cnt; ++j) {
-        // lane 0 decides from the tile's summary; every lane follows its decision
-        int commit = 0;
-        if (lane == 0) {
-          const XTileAgg& G = sg[wl][j];
-          int e;
-          if (!G.r.bad && G.u != 0.0 && x_binade(s, e) && x_pow2(e - 52) == G.u) {
-            const long long S0 = static_cast<long long>(s * x_pow2(52 - e));
-            const bool odd = (S0 & 1) != 0;
-            const long long mn = odd ? G.r.mn[1] : G.r.mn[0], mx = odd ? G.r.mx[1] : G.r.mx[0];
-            if (x_inside(S0, S0 + mn) && x_inside(S0, S0 + mx)) {
-              s = static_cast<double>(S0 + (odd ? G.r.K[1] : G.r.K[0])) * G.u;
-              commit = 1;
+      int j = 0;
+      while (j < cnt) {
+        int e;
+        const bool have = x_binade(s, e);
+        const double u = have ? x_pow2(e - 52) : 0.0;
+        const long long S0 = have ? static_cast<long long>(s * x_pow2(52 - e)) : 0;
+        const int p0 = static_cast<int>(S0 & 1);
+        // lane l >= j: tile l's run if it stays in this binade; lanes below j: nothing
+        XRun r = x_identity();
+        bool mine_ok = false;
+        if (lane >= j && lane < cnt) {
+          const XTileAgg& G = sg[wl][lane];
+          mine_ok = have && !G.pre.bad && G.split < 0 && G.u == u;
+          r = G.pre;
+        }
+        XRun inc = r;
+        for (int off = 1; off < 32; off <<= 1) {
+          const XRun o = x_shfl_up(inc, off);
+          if (lane >= off) inc = x_compose(o, inc);
+        }
+        XRun ex = x_shfl_up(inc, 1);
+        if (lane == 0) ex = x_identity();
+        const long long Kb = p0 ? ex.K[1] : ex.K[0];
+        const int pb = p0 ? ex.out[1] : ex.out[0];
+        bool valid = false;
+        if (mine_ok) {
+          const long long mn = pb ? r.mn[1] : r.mn[0], mx = pb ? r.mx[1] : r.mx[0];
+          valid = x_inside(S0, S0 + Kb + mn) && x_inside(S0, S0 + Kb + mx);
+        }
+        const unsigned bad = __ballot_sync(kFull, lane >= j && lane < cnt && !valid);
+        const int f = bad ? __ffs(bad) - 1 : cnt;  // first tile not committed
+        if (f > j) {  // tiles j … f−1: S0 plus the exclusive change at tile f (or the total)
+          const long long K = f < 32 ? __shfl_sync(kFull, Kb, f & 31) : __shfl_sync(kFull, p0 ? inc.K[1] : inc.K[0], 31);
+          s = static_cast<double>(S0 + K) * u;
+        }
+        if (f < cnt) {  // tile f on its own
+          long long a, b;
+          x_tile_range(c, c.tile0 + g0 + f, a, b);
+          long long resume = a;
+          if (lane == 0) {
+            const XTileAgg& G = sg[wl][f];
+            double s2 = s;
+            if (x_commit(s2, G.u, G.pre)) {
+              if (G.split < 0) {
+                resume = b;
+              } else {
+                s2 += c.t[a + G.split];  // the term that changes the binade, as the chain adds it
+                resume = a + G.split + 1;
+                if (x_commit(s2, G.u1, G.suf)) resume = b;
+              }
+              s = s2;
             }
           }
+          s = __shfl_sync(kFull, s, 0);
+          resume = __shfl_sync(kFull, resume, 0);
+          if (resume < b) s = x_window_walk(c.t, resume, b, s);
         }
-        commit = __shfl_sync(kFull, commit, 0);
-        s = __shfl_sync(kFull, s, 0);
-        if (!commit) {
-          long long a, b;
-          x_tile_range(c, c.tile0 + g0 + j, a, b);
-          s = x_window_walk(c.t, a, b, s);
-        }
+        j = f + 1;
       }
     }
   }
