@@ -164,6 +164,10 @@ typedef struct {
   long long spmv_kernel_launches;
   double teardown_seconds;     /* releasing the engine's device state after the loop */
   double call_seconds;         /* the whole entry-point call, host wall clock */
+  int slab_variant_primal;     /* launch variants of the fused iteration kernels picked by the */
+  int slab_variant_dual;       /*   autotuner for this matrix (indices of the library's variant list) */
+  int tuned;                   /* 1: this solve timed the variants itself (first of its shape class) */
+  int reserved;
 } ps26119_stats;
 
 PS26119_API void ps26119_last_stats(ps26119_stats* out);

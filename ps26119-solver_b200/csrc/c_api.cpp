@@ -97,6 +97,9 @@ void fill_stats(const Solution& s, long long m, long long n, long long nnz) {
   g_stats.spmv_kernel_ms = R.iter_kernel_ms;
   g_stats.spmv_kernel_launches = R.iter_kernel_launches;
   g_stats.teardown_seconds = R.teardown_seconds;
+  g_stats.slab_variant_primal = R.slab_variant_primal;
+  g_stats.slab_variant_dual = R.slab_variant_dual;
+  g_stats.tuned = R.tuned;
 }
 
 void fill(const Solution& s, ps26119_result* result) {  // c_api.cpp:58-71

@@ -26,6 +26,7 @@
 #include "checks.cuh"
 #include "engine.hpp"
 #include "problem.cuh"
+#include "tune.hpp"
 
 namespace b200 {
 
@@ -155,6 +156,7 @@ class Engine {
   Status ray_verdict(const double* h, int which, const Kkt& k, std::string& why) const;
   void setup();
   void build_plans();
+  template <class T> void tune_slab();
   template <class T> void init_iterates();
   bool apply_warm_start();
   template <class T> void restart();
@@ -202,6 +204,8 @@ class Engine {
   DevBuf<double> res2_;
   DevBuf<int2> slab_a_, slab_t_;
   int cap_a_ = kSlabTile, cap_t_ = kSlabTile;  // k_slab_fed tile capacities (largest slab, rounded up)
+  int var_a_ = 0, var_t_ = 0;                  // k_slab_fed launch variants (dual, primal), tuned
+  bool tuned_now_ = false;                     // this solve measured the variants itself
   PinnedBuf<double> hres2_;
   SumPlan plan_dist_;
   long long epoch_kernels_[2] = {0, 0}, check_kernels_[2][3] = {{0, 0, 0}, {0, 0, 0}};
@@ -255,6 +259,61 @@ void Engine::setup() {
   xo_.alloc(nn), yo_.alloc(mm), r1_.alloc(mm), d1_.alloc(nn), r2_.alloc(mm), d2_.alloc(nn);
   objt_.alloc(mm + 2 * nn);
   build_plans();
+  if (o_.mixed) tune_slab<float>();
+  else tune_slab<double>();
+}
+
+// The autotuner (tune.hpp): times every k_slab_fed variant on this matrix, for both iteration
+// kernels, unless the shape class was measured before in this process. The iterates are not
+// initialised yet, so the timed launches (real operands, step parameters of an idle step)
+// disturb nothing; every variant computes the same values.
+template <class T>
+void Engine::tune_slab() {
+  const int forced = tune_forced();
+  if (forced >= 0) {
+    var_a_ = var_t_ = forced < kNumSlabVariants ? forced : 0;
+    return;
+  }
+  if (!tune_enabled()) return;
+  const int prec = std::is_same<T, float>::value ? 1 : 0;
+  const int m = M_.m, n = M_.n;
+  const TuneKey kt = tune_key(0, prec, n, M_.nnz), ka = tune_key(1, prec, m, M_.nnz);
+  TuneCache& cache = TuneCache::instance();
+  if (cache.get(kt, var_t_) && cache.get(ka, var_a_)) return;
+  IterVecs<T>& v = vecs<T>();
+  StepParams hp{};
+  hp.tau = 0.0, hp.sigma = 0.0, hp.rho = o_.reflection, hp.inner0 = 0, hp.K = o_.check_every, hp.done = 0;
+  hp.skip_r0 = 1;
+  B200_CHECK(cudaMemcpyAsync(params_.get(), &hp, sizeof hp, cudaMemcpyHostToDevice, st_));
+  const StepParams* P = params_.get();
+  auto measure = [&](auto&& launch) {
+    double ms[kNumSlabVariants];
+    for (int k = 0; k < kNumSlabVariants; ++k) {
+      launch(k);  // warm-up (first use of the instantiation, caches)
+      B200_CHECK(cudaEventRecord(ev_[0], st_));
+      for (int r = 0; r < 3; ++r) launch(k);
+      B200_CHECK(cudaEventRecord(ev_[1], st_));
+      B200_CHECK(cudaEventSynchronize(ev_[1]));
+      float t = 0;
+      B200_CHECK(cudaEventElapsedTime(&t, ev_[0], ev_[1]));
+      ms[k] = t / 3.0;
+      kernels_ += 4;
+    }
+    return pick_variant(ms, kNumSlabVariants);
+  };
+  var_t_ = measure([&](int k) {
+    EpiPrimal<T> ep{v.x.get(), v.xh.get(), v.xb.get(), v.x0.get(), sp_.c<T>(), sp_.l<T>(), sp_.u<T>(), P, 1, 0, 0, 0};
+    launch_slab_fed<T>(n, sp_.t_rp.get(), sp_.t_ri.get(), sp_.At_val<T>(), v.y.get(), ep, st_, slab_t_.get(), cap_t_,
+                       err(), false, k);
+  });
+  var_a_ = measure([&](int k) {
+    EpiDual<T> ed{v.y.get(), v.yh.get(), v.yb.get(), v.y0.get(), sp_.rl<T>(), sp_.ru<T>(), P, 1, 0, 0, 0, 0};
+    launch_slab_fed<T>(m, sp_.a_rp.get(), sp_.a_col.get(), sp_.A_val<T>(), v.xb.get(), ed, st_, slab_a_.get(), cap_a_,
+                       err(), false, k);
+  });
+  cache.put(kt, var_t_);
+  cache.put(ka, var_a_);
+  tuned_now_ = true;
 }
 
 void Engine::build_plans() {
@@ -398,10 +457,10 @@ void Engine::capture_epoch() {
   auto step = [&](int s) {
     EpiPrimal<T> ep{v.x.get(), v.xh.get(), v.xb.get(), v.x0.get(), sp_.c<T>(), sp_.l<T>(), sp_.u<T>(), P, s, 0, 0, 0};
     launch_slab_fed<T>(n, sp_.t_rp.get(), sp_.t_ri.get(), sp_.At_val<T>(), v.y.get(), ep, st_, slab_t_.get(), cap_t_,
-                       err(), s >= 2);
+                       err(), s >= 2, var_t_);
     EpiDual<T> ed{v.y.get(), v.yh.get(), v.yb.get(), v.y0.get(), sp_.rl<T>(), sp_.ru<T>(), P, s, 0, 0, 0, 0};
     launch_slab_fed<T>(m, sp_.a_rp.get(), sp_.a_col.get(), sp_.A_val<T>(), v.xb.get(), ed, st_, slab_a_.get(), cap_a_,
-                       err(), true);
+                       err(), true, var_a_);
     capture_count_ += 2;
   };
   B200_CHECK(cudaEventRecordWithFlags(ev_[0], st_, cudaEventRecordExternal));
@@ -732,6 +791,7 @@ EngineResult Engine::run(const DeviceOutputs& out) {
     R.kernel_launches = kernels_;
     R.iter_kernel_ms = iter_ms_;
     R.iter_kernel_launches = iter_launches_;
+    R.slab_variant_primal = var_t_, R.slab_variant_dual = var_a_, R.tuned = tuned_now_ ? 1 : 0;
     R.seconds = elapsed();
     return R;
   };
@@ -908,10 +968,10 @@ void Engine::capture_pdlp_epoch(int phase) {
     T* yn = odd ? v.y.get() : v.yh.get();
     EpiPdlpPrimal<T> ep{xc, sp_.c<T>(), sp_.l<T>(), sp_.u<T>(), xn, v.xb.get(), v.dx.get(), P, s};
     launch_slab_fed<T>(n, sp_.t_rp.get(), sp_.t_ri.get(), sp_.At_val<T>(), yc, ep, st_, slab_t_.get(), cap_t_, err(),
-                       s >= 1);
+                       s >= 1, var_t_);
     EpiPdlpDual<T> ed{yc, sp_.rl<T>(), sp_.ru<T>(), yn, v.dy.get(), P, s};
     launch_slab_fed<T>(m, sp_.a_rp.get(), sp_.a_col.get(), sp_.A_val<T>(), v.xb.get(), ed, st_, slab_a_.get(), cap_a_,
-                       err(), true);
+                       err(), true, var_a_);
     capture_count_ += 2;
   }
   B200_CHECK(cudaEventRecordWithFlags(ev_[1], st_, cudaEventRecordExternal));
@@ -1060,6 +1120,7 @@ EngineResult Engine::run_pdlp(const DeviceOutputs& out) {
     R.kernel_launches = kernels_;
     R.iter_kernel_ms = iter_ms_;
     R.iter_kernel_launches = iter_launches_;
+    R.slab_variant_primal = var_t_, R.slab_variant_dual = var_a_, R.tuned = tuned_now_ ? 1 : 0;
     R.seconds = elapsed();
     return R;
   };

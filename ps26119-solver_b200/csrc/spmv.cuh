@@ -381,7 +381,7 @@ inline int fed_tile_capacity(long long max_slab_nnz) {
 #define B200_FED_MIN_BLOCKS 5
 #endif
 
-template <class T, class Epi>
+template <class T, class Epi, int GB = kGatherBatch>
 __global__ void __launch_bounds__(kSlabRows, B200_FED_MIN_BLOCKS) k_slab_fed(int rows, const int* __restrict__ rp,
                                                            const int* __restrict__ col,
                                                            const T* __restrict__ val,
@@ -472,13 +472,13 @@ __global__ void __launch_bounds__(kSlabRows, B200_FED_MIN_BLOCKS) k_slab_fed(int
     }
     const int c0 = t0 & ~3, v0 = t0 & ~(kValAlign - 1);
     const int a = max(beg, t0), b = min(end, t1);
-    for (int k = a; k < b; k += kGatherBatch) {
-      double p[kGatherBatch];
+    for (int k = a; k < b; k += GB) {  // GB gathers in flight, then their products added in CSR order
+      double p[GB];
 #pragma unroll
-      for (int q = 0; q < kGatherBatch; ++q)
+      for (int q = 0; q < GB; ++q)
         p[q] = (k + q < b) ? static_cast<double>(s_val[k + q - v0]) * gather(x, s_col[k + q - c0]) : 0.0;
 #pragma unroll
-      for (int q = 0; q < kGatherBatch; ++q)
+      for (int q = 0; q < GB; ++q)
         if (k + q < b) s += p[q];  // in CSR order
     }
   }
@@ -541,32 +541,94 @@ inline void launch_slab_tma(int rows, const int* rp, const int* col, const T* va
 #ifndef B200_PDL
 #define B200_PDL 1
 #endif
-template <class T, class Epi>
-inline void launch_slab_fed(int rows, const int* rp, const int* col, const T* val, const T* x, const Epi& epi,
-                            cudaStream_t st, const int2* slab, int cap, unsigned* err = nullptr, bool pdl = false) {
-  if (rows <= 0) return;
-  const FedLayout L = fed_layout(Epi::kVecs, static_cast<int>(sizeof(T)), cap);
-  bool ok = B200_SLAB_FED && B200_STAGE_TMA && cap >= 16 && cap % 16 == 0 && L.bytes <= 48u * 1024u &&
-            (reinterpret_cast<std::uintptr_t>(rp) & 15u) == 0;
-  for (int k = 0; k < Epi::kVecs; ++k) ok = ok && (reinterpret_cast<std::uintptr_t>(epi.vec(k)) & 15u) == 0;
-  if (!ok) return launch_slab_tma<T>(rows, rp, col, val, x, epi, st, slab, err);
-  const int grid = (rows + kSlabRows - 1) / kSlabRows;
+
+// Launch variants of k_slab_fed, chosen per matrix by the autotuner (tune.cuh): `gather` = GB
+// (2, 4 or 8 gathers in flight per thread), `ctas` = resident CTAs per SM (0: as many as the
+// registers and shared memory allow; k: dynamic shared memory padded so that no more than k
+// fit). Every variant computes
+// the same sums in the same order: the results do not depend on the choice.
+struct SlabVariant {
+  int gather, ctas;
+};
+constexpr SlabVariant kSlabVariants[] = {{4, 0}, {2, 0}, {8, 0}, {4, 5}, {4, 4}};
+constexpr int kNumSlabVariants = static_cast<int>(sizeof(kSlabVariants) / sizeof(kSlabVariants[0]));
+
+// Dynamic shared memory of a k_slab_fed launch that needs `bytes` under variant `v`.
+inline unsigned fed_smem_bytes(unsigned bytes, const SlabVariant& v) {
+  if (v.ctas <= 0) return bytes;
+  static const int per_sm = [] {
+    int dev = 0, v = 0;
+    (void)cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess) v = 233472;
+    (void)cudaGetLastError();
+    return v;
+  }();
+  static const int reserved = [] {
+    int dev = 0, v = 0;
+    (void)cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrReservedSharedMemoryPerBlock, dev) != cudaSuccess) v = 1024;
+    (void)cudaGetLastError();
+    return v;
+  }();
+  // v.ctas + 1 blocks of this size (plus their reserved bytes) exceed the SM's shared memory
+  const long long pad = static_cast<long long>(per_sm) / (v.ctas + 1) - reserved + 16;
+  return static_cast<unsigned>(std::max<long long>(bytes, (pad + 15) / 16 * 16));
+}
+
+template <class T, class Epi, int GB>
+inline void launch_fed_gb(int grid, unsigned smem, cudaStream_t st, bool pdl, int rows, const int* rp, const int* col,
+                          const T* val, const T* x, const Epi& epi, const int2* slab, int cap, unsigned* err) {
+  if (smem > 48u * 1024u) {  // once per instantiation, outside any capture: allow the padded size
+    static const bool opt = [] {
+      (void)cudaFuncSetAttribute(k_slab_fed<T, Epi, GB>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+      (void)cudaGetLastError();
+      return true;
+    }();
+    (void)opt;
+  }
   if (B200_PDL && pdl) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(static_cast<unsigned>(grid));
     cfg.blockDim = dim3(kSlabRows);
-    cfg.dynamicSmemBytes = L.bytes;
+    cfg.dynamicSmemBytes = smem;
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    B200_CHECK(cudaLaunchKernelEx(&cfg, k_slab_fed<T, Epi>, rows, rp, col, val, x, epi, slab, cap, err));
+    B200_CHECK(cudaLaunchKernelEx(&cfg, k_slab_fed<T, Epi, GB>, rows, rp, col, val, x, epi, slab, cap, err));
     return;
   }
-  k_slab_fed<T, Epi><<<grid, kSlabRows, L.bytes, st>>>(rows, rp, col, val, x, epi, slab, cap, err);
+  k_slab_fed<T, Epi, GB><<<grid, kSlabRows, smem, st>>>(rows, rp, col, val, x, epi, slab, cap, err);
   B200_LAUNCH_CHECK();
+}
+
+// The fully staged form (k_slab_fed) for the iteration epilogues, whose operand vectors are
+// library allocations; `rp` must be one too, `slab` the slab table of rp and `cap` the tile
+// capacity from fed_tile_capacity. Falls back to launch_slab_tma when an operand is not 16-byte
+// aligned or the kernel's own shared memory would exceed 48 KB. `pdl`: launch with programmatic
+// dependent launch (B200_PDL builds), so the kernel's blocks may start while the previous kernel
+// of the stream finishes: only where Epi::kLiveVecs names every operand vector a kernel still in
+// flight may write. The fallback never uses it. `variant`: an index into kSlabVariants.
+template <class T, class Epi>
+inline void launch_slab_fed(int rows, const int* rp, const int* col, const T* val, const T* x, const Epi& epi,
+                            cudaStream_t st, const int2* slab, int cap, unsigned* err = nullptr, bool pdl = false,
+                            int variant = 0) {
+  if (rows <= 0) return;
+  const FedLayout L = fed_layout(Epi::kVecs, static_cast<int>(sizeof(T)), cap);
+  bool ok = B200_SLAB_FED && B200_STAGE_TMA && cap >= 16 && cap % 16 == 0 && L.bytes <= 48u * 1024u &&
+            (reinterpret_cast<std::uintptr_t>(rp) & 15u) == 0;
+  for (int k = 0; k < Epi::kVecs; ++k) ok = ok && (reinterpret_cast<std::uintptr_t>(epi.vec(k)) & 15u) == 0;
+  if (!ok) return launch_slab_tma<T>(rows, rp, col, val, x, epi, st, slab, err);
+  const SlabVariant v = kSlabVariants[(variant >= 0 && variant < kNumSlabVariants) ? variant : 0];
+  const int grid = (rows + kSlabRows - 1) / kSlabRows;
+  const unsigned smem = fed_smem_bytes(L.bytes, v);
+  switch (v.gather) {
+    case 2: return launch_fed_gb<T, Epi, 2>(grid, smem, st, pdl, rows, rp, col, val, x, epi, slab, cap, err);
+    case 8: return launch_fed_gb<T, Epi, 8>(grid, smem, st, pdl, rows, rp, col, val, x, epi, slab, cap, err);
+    default: return launch_fed_gb<T, Epi, 4>(grid, smem, st, pdl, rows, rp, col, val, x, epi, slab, cap, err);
+  }
 }
 
 // The nonzero range [rp[b·kSlabRows], rp[min((b+1)·kSlabRows, rows)]) of every slab b.

@@ -76,7 +76,9 @@ class _Stats(ctypes.Structure):  # ps26119_stats
                 ("switch_iteration", ctypes.c_longlong), ("kernel_launches", ctypes.c_longlong),
                 ("m", ctypes.c_longlong), ("n", ctypes.c_longlong), ("nnz", ctypes.c_longlong),
                 ("spmv_kernel_ms", ctypes.c_double), ("spmv_kernel_launches", ctypes.c_longlong),
-                ("teardown_seconds", ctypes.c_double), ("call_seconds", ctypes.c_double)]
+                ("teardown_seconds", ctypes.c_double), ("call_seconds", ctypes.c_double),
+                ("slab_variant_primal", ctypes.c_int), ("slab_variant_dual", ctypes.c_int), ("tuned", ctypes.c_int),
+                ("reserved", ctypes.c_int)]
 
 
 class _Scenario(ctypes.Structure):  # ps26119_scenario
