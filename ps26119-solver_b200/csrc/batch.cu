@@ -32,6 +32,7 @@
 #include <type_traits>
 #include "checks.cuh"
 #include "problem.cuh"
+#include "tune.hpp"
 
 namespace b200 {
 namespace {
@@ -500,7 +501,9 @@ class BatchEngine {
   void launch_residual(bool distances);
   void launch_kkt();
   template <class Epi>
-  void spmm(int rows, const int* rp, const int* col, const double* val, const double* X, const Epi& epi, bool capped);
+  void spmm(int rows, const int* rp, const int* col, const double* val, const double* X, const Epi& epi, bool capped,
+            int shape = 0);
+  void tune_spmm();
   void step(int s);
   void epoch_body(bool r0_section);
   void launch_epoch(bool r0_section);
@@ -525,6 +528,7 @@ class BatchEngine {
   int m_ = 0, n_ = 0, W_ = 0;
   double eta_ = 1.0, setup_s_ = 0.0;
   long long launches_ = 0;
+  int shape_[2] = {0, 0};  // SpMM shapes of the primal and dual step kernels (tune_spmm)
 
   DevBuf<double> c_, cl_, cu_, rl_, ru_, v_;
   DevBuf<int> cs_, ri_;
@@ -544,8 +548,12 @@ class BatchEngine {
 };
 
 template <class Epi>
+// `shape`: how the W slots of a row are spread over lanes. 0: G = 32 lanes per row (fewer for
+// W < 32) with S = ⌈W/G⌉ slots per lane; c > 0: G/2^c lanes with 2^c times the slots (while
+// S ≤ 8). Every shape sums each (row, slot) in the same order; the iteration kernels use the
+// shape the autotuner measured fastest on this matrix (tune_spmm).
 void BatchEngine::spmm(int rows, const int* rp, const int* col, const double* val, const double* X, const Epi& epi,
-                       bool capped) {
+                       bool capped, int shape) {
   if (rows <= 0) return;
   int lg = 0, S = 1;
   if (W_ >= 32) {
@@ -555,6 +563,7 @@ void BatchEngine::spmm(int rows, const int* rp, const int* col, const double* va
   } else {
     while ((1 << lg) < W_) ++lg;
   }
+  for (int c = 0; c < shape && lg > 0 && S < 8; ++c) --lg, S *= 2;
   const long long threads = static_cast<long long>(rows) << lg;
   long long blocks = (threads + 255) / 256;
   if (capped) blocks = std::min<long long>(blocks, 148 * 8);
@@ -682,6 +691,7 @@ void BatchEngine::setup() {
     }
   }
   bs_.upload(hbs_.data(), W_, st_), os_.upload(hos_.data(), W_, st_);
+  tune_spmm();  // before the start point is written: the timed launches overwrite the iterates
   k_bscale_cols<<<grid_for(nw), kBlock, 0, st_>>>(nw, W_, static_cast<double>(B_.sense), nv_[OC].get(),
                                                   nv_[OCL].get(), nv_[OCU].get(), sp_.col_scale.get(), bs_.get(),
                                                   os_.get(), nv_[C].get(), nv_[L].get(), nv_[U].get(), nv_[X].get(),
@@ -694,13 +704,62 @@ void BatchEngine::setup() {
   B200_CHECK(cudaStreamSynchronize(st_));
 }
 
+// The autotuner for the two step kernels (tune.hpp): every SpMM shape timed on this matrix and
+// slot count, unless the shape class was measured before in this process. The choice stays
+// for the whole batch (later compactions keep the shape index).
+void BatchEngine::tune_spmm() {
+  const int forced = tune_forced();
+  if (forced >= 0) {
+    shape_[0] = shape_[1] = forced < 3 ? forced : 0;
+    return;
+  }
+  if (!tune_enabled()) return;
+  const long long nnz = B_.col_start[n_];
+  // the batch step kernels are classes 10 and 11, with the slot count in the precision field
+  const TuneKey k0 = tune_key(10 + 0, W_, n_, nnz), k1 = tune_key(10 + 1, W_, m_, nnz);
+  TuneCache& cache = TuneCache::instance();
+  if (cache.get(k0, shape_[0]) && cache.get(k1, shape_[1])) return;
+  cudaEvent_t a, b;
+  B200_CHECK(cudaEventCreate(&a));
+  B200_CHECK(cudaEventCreate(&b));
+  auto measure = [&](auto&& launch) {
+    double ms[3];
+    for (int c = 0; c < 3; ++c) {
+      launch(c);
+      B200_CHECK(cudaEventRecord(a, st_));
+      for (int r = 0; r < 3; ++r) launch(c);
+      B200_CHECK(cudaEventRecord(b, st_));
+      B200_CHECK(cudaEventSynchronize(b));
+      float t = 0;
+      B200_CHECK(cudaEventElapsedTime(&t, a, b));
+      ms[c] = t / 3.0;
+    }
+    return pick_variant(ms, 3);
+  };
+  const int Kc = o_.check_every;
+  shape_[0] = measure([&](int c) {
+    EpiBPrimal ep{nv_[C].get(), nv_[L].get(), nv_[U].get(), nv_[X0].get(), tau_.get(), nv_[X].get(), nv_[XH].get(),
+                  nv_[XB].get(), inner0_.get(), 1, Kc - 1, 2 * o_.reflection, 1 - 2 * o_.reflection};
+    spmm(n_, cs_.get(), sp_.t_ri.get(), sp_.sat.get(), mv_[Y].get(), ep, false, c);
+  });
+  shape_[1] = measure([&](int c) {
+    EpiBDual ed{mv_[RL].get(), mv_[RU].get(), mv_[Y0].get(), sigma_.get(), mv_[Y].get(), mv_[YH].get(), mv_[YB].get(),
+                inner0_.get(), 1, Kc - 1, 2 * o_.reflection, 1 - 2 * o_.reflection};
+    spmm(m_, sp_.a_rp.get(), sp_.a_col.get(), sp_.sa.get(), nv_[XB].get(), ed, false, c);
+  });
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cache.put(k0, shape_[0]);
+  cache.put(k1, shape_[1]);
+}
+
 void BatchEngine::step(int s) {
   EpiBPrimal ep{nv_[C].get(), nv_[L].get(), nv_[U].get(), nv_[X0].get(), tau_.get(), nv_[X].get(), nv_[XH].get(),
                 nv_[XB].get(), inner0_.get(), s, o_.check_every - 1, 2 * o_.reflection, 1 - 2 * o_.reflection};
-  spmm(n_, cs_.get(), sp_.t_ri.get(), sp_.sat.get(), mv_[Y].get(), ep, false);
+  spmm(n_, cs_.get(), sp_.t_ri.get(), sp_.sat.get(), mv_[Y].get(), ep, false, shape_[0]);
   EpiBDual ed{mv_[RL].get(), mv_[RU].get(), mv_[Y0].get(), sigma_.get(), mv_[Y].get(), mv_[YH].get(), mv_[YB].get(),
               inner0_.get(), s, o_.check_every - 1, 2 * o_.reflection, 1 - 2 * o_.reflection};
-  spmm(m_, sp_.a_rp.get(), sp_.a_col.get(), sp_.sa.get(), nv_[XB].get(), ed, false);
+  spmm(m_, sp_.a_rp.get(), sp_.a_col.get(), sp_.sa.get(), nv_[XB].get(), ed, false, shape_[1]);
 }
 
 // The K iterations of an epoch (the body of the epoch graph), with the r⁰ residual right after
