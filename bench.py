@@ -63,7 +63,7 @@ WORKLOADS = {
 }
 # DRAM bytes per iteration (both fused kernels: dram__bytes_read.sum + dram__bytes_write.sum of
 # one launch each) from the ncu capture summarised in the named profile.
-NCU_TRAFFIC = {("random1m", "fp64"): 152.4e6 + 123.5e6}
+NCU_TRAFFIC = {("random1m", "fp64"): (146.1e6 + 5.7e6) + (120.1e6 + 3.6e6)}
 NCU_TRAFFIC_SOURCE = {("random1m", "fp64"): "profiles/k_slab_fed_random1m.md"}
 # Measured to-tolerance solves a default single-LP run adds after its timed steps.
 TIME_TO_TOL = [("random10k", "fp64"), ("random10k", "mixed"), ("staircase8760", "mixed")]
