@@ -68,14 +68,16 @@ constexpr int kBatchNz = B200_BATCH_NZ;
 #ifndef B200_BATCH_HINTS
 #define B200_BATCH_HINTS 1
 #endif
-__device__ __forceinline__ double bstream(const double* p) {
+template <class T>
+__device__ __forceinline__ T bstream(const T* p) {
 #if B200_BATCH_HINTS
   return ld_stream(p);
 #else
   return *p;
 #endif
 }
-__device__ __forceinline__ void bkeep(double* p, double v) {
+template <class T>
+__device__ __forceinline__ void bkeep(T* p, T v) {
 #if B200_BATCH_HINTS
   st_keep(p, v);
 #else
@@ -97,10 +99,12 @@ __device__ __forceinline__ void bapply(const E& e, long long r, int t, long long
   else e(r, t, q, acc, mx, p);
 }
 
-template <int S, class Epi>
+// TV / TX: the matrix values and the gathered block in the working precision (double, or float
+// in the mixed form's first phase); products and sums in fp64 either way.
+template <int S, class Epi, class TV, class TX>
 __global__ void __launch_bounds__(256) k_bspmm(int rows, int W, int lg, const int* __restrict__ rp,
-                                               const int* __restrict__ col, const double* __restrict__ val,
-                                               const double* __restrict__ X, Epi epi) {
+                                               const int* __restrict__ col, const TV* __restrict__ val,
+                                               const TX* __restrict__ X, Epi epi) {
   const int G = 1 << lg, g = threadIdx.x & (G - 1);
   const long long gid = (blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x) >> lg;
   const long long ng = (static_cast<long long>(gridDim.x) * blockDim.x) >> lg;
@@ -128,7 +132,7 @@ __global__ void __launch_bounds__(256) k_bspmm(int rows, int W, int lg, const in
 #pragma unroll
       for (int u = 0; u < kBatchNz; ++u) {
         cc[u] = p + u < e ? col[p + u] : 0;
-        aa[u] = p + u < e ? val[p + u] : 0.0;
+        aa[u] = p + u < e ? static_cast<double>(val[p + u]) : 0.0;
       }
       double xv[kBatchNz][S];
 #pragma unroll
@@ -136,7 +140,7 @@ __global__ void __launch_bounds__(256) k_bspmm(int rows, int W, int lg, const in
 #pragma unroll
         for (int s = 0; s < S; ++s) {
           const int t = g + s * G;
-          xv[u][s] = (p + u < e && t < W) ? X[static_cast<long long>(cc[u]) * W + t] : 0.0;
+          xv[u][s] = (p + u < e && t < W) ? static_cast<double>(X[static_cast<long long>(cc[u]) * W + t]) : 0.0;
         }
 #pragma unroll
       for (int u = 0; u < kBatchNz; ++u)
@@ -167,69 +171,79 @@ __global__ void __launch_bounds__(256) k_bspmm(int rows, int W, int lg, const in
   }
 }
 
-// Primal step of every slot (batch.cpp:331-343), acc = (Ãᵀy)_j.
+// Primal step of every slot (batch.cpp:331-343), acc = (Ãᵀy)_j, in the working precision T
+// (double: the reference's arithmetic; float: the mixed form's first phase, as the single-LP
+// engine's fp32 kernels).
+template <class T>
 struct EpiBPrimal {
   static constexpr int kMax = 0;
-  const double *C, *L, *U, *X0, *tau;
-  double *X, *XH, *XB;
+  const T *C, *L, *U, *X0;
+  const double* tau;
+  T *X, *XH, *XB;
   const long long* inner0;
   int step, last;  // last: the epoch's last step
   double a2, b2;
   struct Pre {
-    double x, c, l, u, x0;
+    T x, c, l, u, x0;
   };
   __device__ Pre load(long long q, int) const {
     return Pre{bstream(X + q), bstream(C + q), bstream(L + q), bstream(U + q), bstream(X0 + q)};
   }
   __device__ void operator()(long long, int t, long long q, double aty, double*, const Pre& p) const {
     const long long in = inner0[t] + step;
-    const double w = static_cast<double>(in + 1) / static_cast<double>(in + 2);
-    const double x = p.x;
-    const double h = ref_clamp(x - tau[t] * (p.c - aty), p.l, p.u);
+    const T w = static_cast<T>(static_cast<double>(in + 1) / static_cast<double>(in + 2));
+    const T x = p.x;
+    const T h = ref_clamp<T>(x - static_cast<T>(tau[t]) * (p.c - static_cast<T>(aty)), p.l, p.u);
     // x̂ is read only by the residual, check and restart that follow the epoch's last step and
     // the first step of a slot's Halpern cycle; on the other steps it is not stored
     if (step == last || in == 0) XH[q] = h;
-    bkeep(XB + q, 2 * h - x);  // gathered by the dual kernel next
-    X[q] = w * (a2 * h + b2 * x) + (1 - w) * p.x0;
+    bkeep(XB + q, static_cast<T>(static_cast<T>(2) * h - x));  // gathered by the dual kernel next
+    X[q] = w * (static_cast<T>(a2) * h + static_cast<T>(b2) * x) + (static_cast<T>(1) - w) * p.x0;
   }
 };
 // Dual step of every slot (batch.cpp:345-358), acc = (Ãx̄)_i.
+template <class T>
 struct EpiBDual {
   static constexpr int kMax = 0;
-  const double *RL, *RU, *Y0, *sigma;
-  double *Y, *YH, *YB;
+  const T *RL, *RU, *Y0;
+  const double* sigma;
+  T *Y, *YH, *YB;
   const long long* inner0;
   int step, last;
   double a2, b2;
   struct Pre {
-    double y, rl, ru, y0;
+    T y, rl, ru, y0;
   };
   __device__ Pre load(long long q, int) const { return Pre{bstream(Y + q), bstream(RL + q), bstream(RU + q), bstream(Y0 + q)}; }
-  __device__ void operator()(long long, int t, long long q, double ax, double*, const Pre& p) const {
+  __device__ void operator()(long long, int t, long long q, double axd, double*, const Pre& p) const {
     const long long in = inner0[t] + step;
-    const double w = static_cast<double>(in + 1) / static_cast<double>(in + 2);
-    const double sg = sigma[t];
-    const double y = p.y;
-    const double v = ax - y / sg;
-    const double h = y - sg * ax + sg * ref_clamp(v, p.rl, p.ru);
+    const T w = static_cast<T>(static_cast<double>(in + 1) / static_cast<double>(in + 2));
+    const T sg = static_cast<T>(sigma[t]), ax = static_cast<T>(axd);
+    const T y = p.y;
+    const T v = ax - y / sg;
+    const T h = y - sg * ax + sg * ref_clamp<T>(v, p.rl, p.ru);
     if (step == last || in == 0) {  // ŷ, ȳ: read only after those steps (as x̂ above)
       YH[q] = h;
-      YB[q] = 2 * h - y;
+      YB[q] = static_cast<T>(2) * h - y;
     }
-    bkeep(Y + q, w * (a2 * h + b2 * y) + (1 - w) * p.y0);  // gathered by the primal kernel next
+    bkeep(Y + q, static_cast<T>(w * (static_cast<T>(a2) * h + static_cast<T>(b2) * y) + (static_cast<T>(1) - w) * p.y0));
   }
 };
 // Residual rows after adx = Ã·Δx (compute_residuals, batch.cpp:305-318): terms Δy², Δy·(AΔx)
-// and, at a check, the restart distance (ŷ − y0)² (batch.cpp:399-403).
+// and, at a check, the restart distance (ŷ − y0)² (batch.cpp:399-403); fp64 terms.
+template <class T>
 struct EpiBRes {
   static constexpr int kMax = 0;
-  const double *YB, *YH, *Y0;
+  const T *YB, *YH, *Y0;
   double *t_py, *t_cr, *t_dyn;
   __device__ void operator()(long long, int, long long q, double adx, double*) const {
-    const double dy = YB[q] - YH[q];
+    const double dy = static_cast<double>(static_cast<T>(YB[q] - YH[q]));
     t_py[q] = dy * dy;
-    t_cr[q] = dy * adx;
-    if (t_dyn) t_dyn[q] = (YH[q] - Y0[q]) * (YH[q] - Y0[q]);
+    t_cr[q] = dy * static_cast<double>(static_cast<T>(adx));
+    if (t_dyn) {
+      const double e = static_cast<double>(YH[q]) - static_cast<double>(Y0[q]);
+      t_dyn[q] = e * e;
+    }
   }
 };
 // kkt_general rows (cpu_backend.cpp:238-252) per slot, acc = (A x)_i on the original matrix.
@@ -398,35 +412,41 @@ __global__ void k_bscale_rows(long long mw, int W, const double* RLo, const doub
   }
 }
 // Δx = x̄ − x̂ and its terms; at a check also (x̂ − x0)² (batch.cpp:306, 395-398).
-__global__ void k_bres_x(long long nw, const double* XB, const double* XH, const double* X0, double* DX, double* t_px,
-                         double* t_dxn) {
+template <class T>
+__global__ void k_bres_x(long long nw, const T* XB, const T* XH, const T* X0, T* DX, double* t_px, double* t_dxn) {
   B200_FOR(q, nw) {
-    const double d = XB[q] - XH[q];
+    const T d = XB[q] - XH[q];
     DX[q] = d;
-    t_px[q] = d * d;
-    if (t_dxn) t_dxn[q] = (XH[q] - X0[q]) * (XH[q] - X0[q]);
+    t_px[q] = static_cast<double>(d) * static_cast<double>(d);
+    if (t_dxn) {
+      const double e = static_cast<double>(XH[q]) - static_cast<double>(X0[q]);
+      t_dxn[q] = e * e;
+    }
   }
 }
 // unscale (batch.cpp:267-275): x = clamp(C x̂ / bs, l, u), y_min = R ŷ / os
-__global__ void k_bunscale_x(long long nw, int W, const double* XH, const double* col_scale, const double* bs,
+template <class T>
+__global__ void k_bunscale_x(long long nw, int W, const T* XH, const double* col_scale, const double* bs,
                              const double* CLo, const double* CUo, double* XO) {
   B200_FOR(q, nw) {
     const long long j = q / W;
     const int t = static_cast<int>(q % W);
-    XO[q] = ref_clamp(col_scale[j] * XH[q] / bs[t], CLo[q], CUo[q]);
+    XO[q] = ref_clamp(col_scale[j] * static_cast<double>(XH[q]) / bs[t], CLo[q], CUo[q]);
   }
 }
-__global__ void k_bunscale_y(long long mw, int W, const double* YH, const double* row_scale, const double* os,
+template <class T>
+__global__ void k_bunscale_y(long long mw, int W, const T* YH, const double* row_scale, const double* os,
                              double* YO) {
   B200_FOR(q, mw) {
     const long long i = q / W;
     const int t = static_cast<int>(q % W);
-    YO[q] = row_scale[i] * YH[q] / os[t];
+    YO[q] = row_scale[i] * static_cast<double>(YH[q]) / os[t];
   }
 }
 // restart of the flagged slots: x = x0 = x̂, y = y0 = ŷ (batch.cpp:413-420)
-__global__ void k_brestart(long long nw, long long mw, int W, const int* flag, const double* XH, double* X, double* X0,
-                           const double* YH, double* Y, double* Y0) {
+template <class T>
+__global__ void k_brestart(long long nw, long long mw, int W, const int* flag, const T* XH, T* X, T* X0, const T* YH,
+                           T* Y, T* Y0) {
   B200_FOR(q, (nw > mw ? nw : mw)) {
     const int t = static_cast<int>(q % W);
     if (!flag[t]) continue;
@@ -434,12 +454,18 @@ __global__ void k_brestart(long long nw, long long mw, int W, const int* flag, c
     if (q < mw) Y[q] = YH[q], Y0[q] = YH[q];
   }
 }
-__global__ void k_bgather(long long rows, int W, int W2, const int* keep, const double* src, double* dst) {
+template <class T>
+__global__ void k_bgather(long long rows, int W, int W2, const int* keep, const T* src, T* dst) {
   B200_FOR(q, rows * W2) {
     const long long r = q / W2;
     const int t2 = static_cast<int>(q % W2);
     dst[q] = src[r * W + keep[t2]];
   }
+}
+// element-wise precision change of a whole block (the mixed form's start and promotion)
+template <class D, class S>
+__global__ void k_bconvert(long long len, const S* src, D* dst) {
+  B200_FOR(q, len) dst[q] = static_cast<D>(src[q]);
 }
 __global__ void k_bcolumn(long long rows, int W, int t, const double* src, double* dst) {
   B200_FOR(r, rows) dst[r] = src[r * W + t];
@@ -500,8 +526,8 @@ class BatchEngine {
   void launch_sums(const ISegs& segs, bool exact);
   void launch_residual(bool distances);
   void launch_kkt();
-  template <class Epi>
-  void spmm(int rows, const int* rp, const int* col, const double* val, const double* X, const Epi& epi, bool capped,
+  template <class Epi, class TV, class TX>
+  void spmm(int rows, const int* rp, const int* col, const TV* val, const TX* X, const Epi& epi, bool capped,
             int shape = 0);
   void tune_spmm();
   void step(int s);
@@ -512,6 +538,8 @@ class BatchEngine {
       if (g) cudaGraphExecDestroy(g), g = nullptr;
   }
   void compact(const std::vector<int>& keep);
+  void start_mixed();
+  void promote();
   void finish_slot(int t, BatchOutcome& o, Status st, const BKkt& kk, long long it, const std::string& msg);
 
   const HostModelView& B_;
@@ -538,6 +566,12 @@ class BatchEngine {
   enum NVec { OC, OCL, OCU, C, L, U, X, X0, XH, XB, DX, XO, TPX, TDXN, TP, TDC, TRDC, TC2, TSC2, kNVec };
   enum MVec { ORL, ORU, RL, RU, Y, Y0, YH, YB, YO, TPY, TCR, TDYN, TRP2, TDR, TRDR, TB2, TSB2, kMVec };
   DevBuf<double> nv_[kNVec], mv_[kMVec], spare_n_, spare_m_;
+  // the mixed form's first phase: fp32 copies of the scaled data and of the iterate blocks
+  enum FN { FC, FL, FU, FX, FX0, FXH, FXB, FDX, kFN };
+  enum FM { FRL, FRU, FY, FY0, FYH, FYB, kFM };
+  DevBuf<float> fn_[kFN], fm_[kFM], fspare_n_, fspare_m_;
+  bool mixed_now_ = false;
+  long long switch_it_ = -1;
   DevBuf<double> res_, part_, tau_, sigma_, bs_, os_, col_buf_n_, col_buf_m_, col_buf_c_, obj_t_, obj_out_;
   DevBuf<long long> inner0_;
   DevBuf<int> flag_, keep_;
@@ -547,12 +581,12 @@ class BatchEngine {
   std::vector<double> hbs_, hos_;
 };
 
-template <class Epi>
 // `shape`: how the W slots of a row are spread over lanes. 0: G = 32 lanes per row (fewer for
 // W < 32) with S = ⌈W/G⌉ slots per lane; c > 0: G/2^c lanes with 2^c times the slots (while
 // S ≤ 8). Every shape sums each (row, slot) in the same order; the iteration kernels use the
 // shape the autotuner measured fastest on this matrix (tune_spmm).
-void BatchEngine::spmm(int rows, const int* rp, const int* col, const double* val, const double* X, const Epi& epi,
+template <class Epi, class TV, class TX>
+void BatchEngine::spmm(int rows, const int* rp, const int* col, const TV* val, const TX* X, const Epi& epi,
                        bool capped, int shape) {
   if (rows <= 0) return;
   int lg = 0, S = 1;
@@ -570,10 +604,10 @@ void BatchEngine::spmm(int rows, const int* rp, const int* col, const double* va
   blocks = std::max<long long>(1, std::min<long long>(blocks, 1LL << 30));
   const int nb = static_cast<int>(blocks);
   switch (S) {
-    case 1: k_bspmm<1, Epi><<<nb, 256, 0, st_>>>(rows, W_, lg, rp, col, val, X, epi); break;
-    case 2: k_bspmm<2, Epi><<<nb, 256, 0, st_>>>(rows, W_, lg, rp, col, val, X, epi); break;
-    case 4: k_bspmm<4, Epi><<<nb, 256, 0, st_>>>(rows, W_, lg, rp, col, val, X, epi); break;
-    default: k_bspmm<8, Epi><<<nb, 256, 0, st_>>>(rows, W_, lg, rp, col, val, X, epi); break;
+    case 1: k_bspmm<1, Epi, TV, TX><<<nb, 256, 0, st_>>>(rows, W_, lg, rp, col, val, X, epi); break;
+    case 2: k_bspmm<2, Epi, TV, TX><<<nb, 256, 0, st_>>>(rows, W_, lg, rp, col, val, X, epi); break;
+    case 4: k_bspmm<4, Epi, TV, TX><<<nb, 256, 0, st_>>>(rows, W_, lg, rp, col, val, X, epi); break;
+    default: k_bspmm<8, Epi, TV, TX><<<nb, 256, 0, st_>>>(rows, W_, lg, rp, col, val, X, epi); break;
   }
   B200_LAUNCH_CHECK();
   ++launches_;
@@ -701,7 +735,45 @@ void BatchEngine::setup() {
                                                   mv_[Y0].get(), mv_[YH].get(), mv_[YB].get());
   B200_LAUNCH_CHECK();
   launches_ += 2;
+  if (o_.mixed) start_mixed();
   B200_CHECK(cudaStreamSynchronize(st_));
+}
+
+// The mixed form starts in fp32: the scaled matrix and every scaled-data and iterate block are
+// converted once (the fp64 blocks stay, for the checks and for the promotion).
+void BatchEngine::start_mixed() {
+  sp_.make_f32(st_);
+  const long long nw = static_cast<long long>(n_) * W_, mw = static_cast<long long>(m_) * W_;
+  const NVec ns[kFN] = {C, L, U, X, X0, XH, XB, DX};
+  const MVec ms[kFM] = {RL, RU, Y, Y0, YH, YB};
+  for (int k = 0; k < kFN; ++k) {
+    fn_[k].alloc(static_cast<std::size_t>(nw));
+    k_bconvert<float, double><<<grid_for(nw), kBlock, 0, st_>>>(nw, nv_[ns[k]].get(), fn_[k].get());
+  }
+  for (int k = 0; k < kFM; ++k) {
+    fm_[k].alloc(static_cast<std::size_t>(mw));
+    k_bconvert<float, double><<<grid_for(mw), kBlock, 0, st_>>>(mw, mv_[ms[k]].get(), fm_[k].get());
+  }
+  B200_LAUNCH_CHECK();
+  launches_ += kFN + kFM;
+  fspare_n_.alloc(static_cast<std::size_t>(nw)), fspare_m_.alloc(static_cast<std::size_t>(mw));
+  mixed_now_ = true;
+}
+
+// Promotion to fp64 (PrecisionPolicy's switch, engine.cpp:61-79, taken by the whole batch at
+// once): every iterate block converted float → double; the caller restarts every slot.
+void BatchEngine::promote() {
+  const long long nw = static_cast<long long>(n_) * W_, mw = static_cast<long long>(m_) * W_;
+  const std::pair<int, int> np[] = {{FX, X}, {FX0, X0}, {FXH, XH}, {FXB, XB}};
+  const std::pair<int, int> mp[] = {{FY, Y}, {FY0, Y0}, {FYH, YH}, {FYB, YB}};
+  for (const auto& pr : np)
+    k_bconvert<double, float><<<grid_for(nw), kBlock, 0, st_>>>(nw, fn_[pr.first].get(), nv_[pr.second].get());
+  for (const auto& pr : mp)
+    k_bconvert<double, float><<<grid_for(mw), kBlock, 0, st_>>>(mw, fm_[pr.first].get(), mv_[pr.second].get());
+  B200_LAUNCH_CHECK();
+  launches_ += 8;
+  mixed_now_ = false;
+  drop_graphs();  // the epoch graphs run the fp32 kernels
 }
 
 // The autotuner for the two step kernels (tune.hpp): every SpMM shape timed on this matrix and
@@ -738,12 +810,12 @@ void BatchEngine::tune_spmm() {
   };
   const int Kc = o_.check_every;
   shape_[0] = measure([&](int c) {
-    EpiBPrimal ep{nv_[C].get(), nv_[L].get(), nv_[U].get(), nv_[X0].get(), tau_.get(), nv_[X].get(), nv_[XH].get(),
+    EpiBPrimal<double> ep{nv_[C].get(), nv_[L].get(), nv_[U].get(), nv_[X0].get(), tau_.get(), nv_[X].get(), nv_[XH].get(),
                   nv_[XB].get(), inner0_.get(), 1, Kc - 1, 2 * o_.reflection, 1 - 2 * o_.reflection};
     spmm(n_, cs_.get(), sp_.t_ri.get(), sp_.sat.get(), mv_[Y].get(), ep, false, c);
   });
   shape_[1] = measure([&](int c) {
-    EpiBDual ed{mv_[RL].get(), mv_[RU].get(), mv_[Y0].get(), sigma_.get(), mv_[Y].get(), mv_[YH].get(), mv_[YB].get(),
+    EpiBDual<double> ed{mv_[RL].get(), mv_[RU].get(), mv_[Y0].get(), sigma_.get(), mv_[Y].get(), mv_[YH].get(), mv_[YB].get(),
                 inner0_.get(), 1, Kc - 1, 2 * o_.reflection, 1 - 2 * o_.reflection};
     spmm(m_, sp_.a_rp.get(), sp_.a_col.get(), sp_.sa.get(), nv_[XB].get(), ed, false, c);
   });
@@ -754,11 +826,22 @@ void BatchEngine::tune_spmm() {
 }
 
 void BatchEngine::step(int s) {
-  EpiBPrimal ep{nv_[C].get(), nv_[L].get(), nv_[U].get(), nv_[X0].get(), tau_.get(), nv_[X].get(), nv_[XH].get(),
-                nv_[XB].get(), inner0_.get(), s, o_.check_every - 1, 2 * o_.reflection, 1 - 2 * o_.reflection};
+  const int last = o_.check_every - 1;
+  const double a2 = 2 * o_.reflection, b2 = 1 - 2 * o_.reflection;
+  if (mixed_now_) {
+    EpiBPrimal<float> ep{fn_[FC].get(), fn_[FL].get(), fn_[FU].get(), fn_[FX0].get(), tau_.get(), fn_[FX].get(),
+                         fn_[FXH].get(), fn_[FXB].get(), inner0_.get(), s, last, a2, b2};
+    spmm(n_, cs_.get(), sp_.t_ri.get(), sp_.satf.get(), fm_[FY].get(), ep, false, shape_[0]);
+    EpiBDual<float> ed{fm_[FRL].get(), fm_[FRU].get(), fm_[FY0].get(), sigma_.get(), fm_[FY].get(), fm_[FYH].get(),
+                       fm_[FYB].get(), inner0_.get(), s, last, a2, b2};
+    spmm(m_, sp_.a_rp.get(), sp_.a_col.get(), sp_.saf.get(), fn_[FXB].get(), ed, false, shape_[1]);
+    return;
+  }
+  EpiBPrimal<double> ep{nv_[C].get(), nv_[L].get(), nv_[U].get(), nv_[X0].get(), tau_.get(), nv_[X].get(), nv_[XH].get(),
+                        nv_[XB].get(), inner0_.get(), s, last, a2, b2};
   spmm(n_, cs_.get(), sp_.t_ri.get(), sp_.sat.get(), mv_[Y].get(), ep, false, shape_[0]);
-  EpiBDual ed{mv_[RL].get(), mv_[RU].get(), mv_[Y0].get(), sigma_.get(), mv_[Y].get(), mv_[YH].get(), mv_[YB].get(),
-              inner0_.get(), s, o_.check_every - 1, 2 * o_.reflection, 1 - 2 * o_.reflection};
+  EpiBDual<double> ed{mv_[RL].get(), mv_[RU].get(), mv_[Y0].get(), sigma_.get(), mv_[Y].get(), mv_[YH].get(),
+                      mv_[YB].get(), inner0_.get(), s, last, a2, b2};
   spmm(m_, sp_.a_rp.get(), sp_.a_col.get(), sp_.sa.get(), nv_[XB].get(), ed, false, shape_[1]);
 }
 
@@ -815,21 +898,38 @@ void BatchEngine::launch_epoch(bool r0_section) {
 
 void BatchEngine::launch_residual(bool distances) {
   const long long nw = static_cast<long long>(n_) * W_;
-  k_bres_x<<<grid_for(nw), kBlock, 0, st_>>>(nw, nv_[XB].get(), nv_[XH].get(), nv_[X0].get(), nv_[DX].get(),
-                                             nv_[TPX].get(), distances ? nv_[TDXN].get() : nullptr);
+  double* tdxn = distances ? nv_[TDXN].get() : nullptr;
+  double* tdyn = distances ? mv_[TDYN].get() : nullptr;
+  if (mixed_now_) {
+    k_bres_x<float><<<grid_for(nw), kBlock, 0, st_>>>(nw, fn_[FXB].get(), fn_[FXH].get(), fn_[FX0].get(),
+                                                      fn_[FDX].get(), nv_[TPX].get(), tdxn);
+    B200_LAUNCH_CHECK();
+    ++launches_;
+    EpiBRes<float> er{fm_[FYB].get(), fm_[FYH].get(), fm_[FY0].get(), mv_[TPY].get(), mv_[TCR].get(), tdyn};
+    spmm(m_, sp_.a_rp.get(), sp_.a_col.get(), sp_.saf.get(), fn_[FDX].get(), er, false);
+    return;
+  }
+  k_bres_x<double><<<grid_for(nw), kBlock, 0, st_>>>(nw, nv_[XB].get(), nv_[XH].get(), nv_[X0].get(), nv_[DX].get(),
+                                                     nv_[TPX].get(), tdxn);
   B200_LAUNCH_CHECK();
   ++launches_;
-  EpiBRes er{mv_[YB].get(), mv_[YH].get(), mv_[Y0].get(), mv_[TPY].get(), mv_[TCR].get(),
-             distances ? mv_[TDYN].get() : nullptr};
+  EpiBRes<double> er{mv_[YB].get(), mv_[YH].get(), mv_[Y0].get(), mv_[TPY].get(), mv_[TCR].get(), tdyn};
   spmm(m_, sp_.a_rp.get(), sp_.a_col.get(), sp_.sa.get(), nv_[DX].get(), er, false);
 }
 
 void BatchEngine::launch_kkt() {
   const long long nw = static_cast<long long>(n_) * W_, mw = static_cast<long long>(m_) * W_;
-  k_bunscale_x<<<grid_for(nw), kBlock, 0, st_>>>(nw, W_, nv_[XH].get(), sp_.col_scale.get(), bs_.get(),
-                                                 nv_[OCL].get(), nv_[OCU].get(), nv_[XO].get());
-  k_bunscale_y<<<grid_for(mw), kBlock, 0, st_>>>(mw, W_, mv_[YH].get(), sp_.row_scale.get(), os_.get(),
-                                                 mv_[YO].get());
+  if (mixed_now_) {
+    k_bunscale_x<float><<<grid_for(nw), kBlock, 0, st_>>>(nw, W_, fn_[FXH].get(), sp_.col_scale.get(), bs_.get(),
+                                                          nv_[OCL].get(), nv_[OCU].get(), nv_[XO].get());
+    k_bunscale_y<float><<<grid_for(mw), kBlock, 0, st_>>>(mw, W_, fm_[FYH].get(), sp_.row_scale.get(), os_.get(),
+                                                          mv_[YO].get());
+  } else {
+    k_bunscale_x<double><<<grid_for(nw), kBlock, 0, st_>>>(nw, W_, nv_[XH].get(), sp_.col_scale.get(), bs_.get(),
+                                                           nv_[OCL].get(), nv_[OCU].get(), nv_[XO].get());
+    k_bunscale_y<double><<<grid_for(mw), kBlock, 0, st_>>>(mw, W_, mv_[YH].get(), sp_.row_scale.get(), os_.get(),
+                                                           mv_[YO].get());
+  }
   k_bzero_keys<<<(W_ + 127) / 128, 128, 0, st_>>>(W_, res_.get());
   B200_LAUNCH_CHECK();
   launches_ += 3;
@@ -845,7 +945,7 @@ void BatchEngine::compact(const std::vector<int>& keep) {
   const int W2 = static_cast<int>(keep.size());
   for (int t = 0; t < W2; ++t) h_int_[t] = keep[t];
   B200_CHECK(cudaMemcpyAsync(keep_.get(), h_int_.get(), W2 * sizeof(int), cudaMemcpyHostToDevice, st_));
-  auto gather = [&](DevBuf<double>& v, long long rows, DevBuf<double>& spare) {
+  auto gather = [&](auto& v, long long rows, auto& spare) {
     k_bgather<<<grid_for(rows * W2), kBlock, 0, st_>>>(rows, W_, W2, keep_.get(), v.get(), spare.get());
     B200_LAUNCH_CHECK();
     ++launches_;
@@ -853,6 +953,10 @@ void BatchEngine::compact(const std::vector<int>& keep) {
   };
   for (auto& v : nv_) gather(v, n_, spare_n_);
   for (auto& v : mv_) gather(v, m_, spare_m_);
+  if (mixed_now_) {
+    for (auto& v : fn_) gather(v, n_, fspare_n_);
+    for (auto& v : fm_) gather(v, m_, fspare_m_);
+  }
   drop_graphs();  // the blocks moved and the slot count changed: capture again
   std::vector<double> nbs(W2), nos(W2);
   for (int t = 0; t < W2; ++t) nbs[t] = hbs_[keep[t]], nos[t] = hos_[keep[t]];
@@ -910,6 +1014,8 @@ void BatchEngine::run(std::vector<BatchOutcome>& out) {
   const int K = static_cast<int>(out.size());
   std::vector<double> omega(K, 1.0), best_omega(K, 1.0), best_balance(K, 1e300), pid_int(K, 0.0), pid_last(K, 0.0);
   std::vector<double> r0(K, -1.0), r_last(K, std::numeric_limits<double>::infinity());
+  std::vector<double> pol_best(K, 1e300);
+  std::vector<int> pol_since(K, 0);
   std::vector<long long> inner(K, 0), fast_it(K, -1);
   std::vector<double> fast_s(K, -1.0);
   const int Kc = o_.check_every;
@@ -970,11 +1076,7 @@ void BatchEngine::run(std::vector<BatchOutcome>& out) {
       for (int t = 0; t < W_; ++t)
         if (inner[sid_[t]] == Kc) r0[sid_[t]] = resid_of(h_res_.get() + static_cast<std::size_t>(t) * kRes, sid_[t], kBPx0);
     const bool over_iter = it >= o_.iteration_limit, over_time = elapsed() > o_.time_limit;
-    std::vector<int> keep;
-    bool any_restart = false;
-    for (int t = 0; t < W_; ++t) h_int_[t] = 0;
-    for (int t = 0; t < W_; ++t) {
-      const int k = sid_[t];
+    auto kkt_at = [&](int t) {
       const double* r = h_res_.get() + static_cast<std::size_t>(t) * kRes;
       BKkt kk;
       kk.primal_residual = std::sqrt(r[kBRp2]);
@@ -989,8 +1091,39 @@ void BatchEngine::run(std::vector<BatchOutcome>& out) {
       std::memcpy(&cinf, r + kBCinf, sizeof cinf);
       kk.primal_max_rel = pmax;
       kk.dual_max_rel = dmax / (1.0 + cinf);
+      return kk;
+    };
+    // Mixed form: each running slot follows PrecisionPolicy::on_check (engine.cpp:61-79) — it asks
+    // for fp64 at rel KKT ≤ 1e-6 (when the target is tighter) or after 10 checks without a 10%
+    // gain — and the batch, which runs in lockstep in one precision, promotes when every slot
+    // that keeps running has asked.
+    bool promote_now = false;
+    if (mixed_now_) {
+      bool all = true, any = false;
+      for (int t = 0; t < W_; ++t) {
+        const int k = sid_[t];
+        const BKkt kk = kkt_at(t);
+        if (!kk.finite() || kk.converged(o_.tolerance) || over_iter || over_time) continue;
+        const double rk = kk.rel_kkt();
+        if (rk < 0.9 * pol_best[k]) pol_best[k] = rk, pol_since[k] = 0;
+        else ++pol_since[k];
+        const bool want = (rk <= 1e-6 && o_.tolerance < 1e-6) || pol_since[k] >= 10;
+        all = all && want;
+        any = true;
+      }
+      promote_now = any && all;
+    }
+    std::vector<int> keep;
+    bool any_restart = false;
+    for (int t = 0; t < W_; ++t) h_int_[t] = 0;
+    for (int t = 0; t < W_; ++t) {
+      const int k = sid_[t];
+      const BKkt kk = kkt_at(t);
       auto fin = [&](Status st, const std::string& msg) {
-        finish_slot(t, out[k], st, kk, it, msg);
+        std::string m2 = msg;
+        if (switch_it_ >= 0)
+          m2 += std::string(m2.empty() ? "" : "; ") + "fp32 -> fp64 at iteration " + std::to_string(switch_it_);
+        finish_slot(t, out[k], st, kk, it, m2);
         out[k].iterations_to_fast = fast_it[k];
         out[k].seconds_to_fast = fast_s[k];
         out[k].primal_weight = omega[k];
@@ -1009,9 +1142,10 @@ void BatchEngine::run(std::vector<BatchOutcome>& out) {
         continue;
       }
       keep.push_back(t);
+      const double* r = h_res_.get() + static_cast<std::size_t>(t) * kRes;
       const double rr = resid_of(r, k, kBPx);
       const bool ratios_ok = r0[k] > 0 && std::isfinite(r0[k]) && rr > 0;
-      const bool restart = (ratios_ok && (rr <= o_.restart_sufficient * r0[k] ||
+      const bool restart = promote_now || (ratios_ok && (rr <= o_.restart_sufficient * r0[k] ||
                                           (rr <= o_.restart_necessary * r0[k] && rr > r_last[k]))) ||
                            static_cast<double>(inner[k]) >= o_.restart_artificial * static_cast<double>(it);
       r_last[k] = rr;
@@ -1042,14 +1176,23 @@ void BatchEngine::run(std::vector<BatchOutcome>& out) {
     if (any_restart) {
       B200_CHECK(cudaMemcpyAsync(flag_.get(), h_int_.get(), W_ * sizeof(int), cudaMemcpyHostToDevice, st_));
       const long long nw = static_cast<long long>(n_) * W_, mw = static_cast<long long>(m_) * W_;
-      k_brestart<<<grid_for(std::max(nw, mw)), kBlock, 0, st_>>>(nw, mw, W_, flag_.get(), nv_[XH].get(),
-                                                                 nv_[X].get(), nv_[X0].get(), mv_[YH].get(),
-                                                                 mv_[Y].get(), mv_[Y0].get());
+      if (mixed_now_)
+        k_brestart<float><<<grid_for(std::max(nw, mw)), kBlock, 0, st_>>>(nw, mw, W_, flag_.get(), fn_[FXH].get(),
+                                                                          fn_[FX].get(), fn_[FX0].get(), fm_[FYH].get(),
+                                                                          fm_[FY].get(), fm_[FY0].get());
+      else
+        k_brestart<double><<<grid_for(std::max(nw, mw)), kBlock, 0, st_>>>(nw, mw, W_, flag_.get(), nv_[XH].get(),
+                                                                           nv_[X].get(), nv_[X0].get(), mv_[YH].get(),
+                                                                           mv_[Y].get(), mv_[Y0].get());
       B200_LAUNCH_CHECK();
       ++launches_;
       B200_CHECK(cudaStreamSynchronize(st_));  // h_int_ is reused by compact()
     }
     if (static_cast<int>(keep.size()) != W_) compact(keep);
+    if (promote_now && W_ > 0) {  // every kept slot restarted above from its x̂, ŷ
+      promote();
+      switch_it_ = it;
+    }
     if (o_.verbosity >= 2)
       std::fprintf(stderr, "batch it %lld  t %.2fs  running %d\n", it, elapsed(), W_);
   }

@@ -1585,7 +1585,8 @@ std::vector<Solution> solve_batch(const Model& base, const std::vector<Scenario>
     if (slots.empty()) return out;
     require_device();
     EngineOptions eo = engine_options(options);
-    eo.mixed = false;  // the batch engine is fp64 (batch.cpp:136)
+    // The reference's batch is fp64 only (batch.cpp:136); precision = mixed runs this engine's
+    // mixed form (fp32 until every slot reaches the switch, then fp64 to the target).
     std::vector<BatchOutcome> res = run_batch_host(base.view(), views, slots, eo, t0);
     for (int k : slots) {
       BatchOutcome& r = res[k];

@@ -130,3 +130,24 @@ def test_batch_is_deterministic():
     for r, s in zip(a, b):
         assert r.iterations == s.iterations and r.objective == s.objective
         np.testing.assert_array_equal(r.x, s.x)
+
+
+@pytest.mark.parametrize("name,make,K", [("random_m300_K12", lambda: g.random_lp(300, seed=6), 12),
+                                         ("staircase_T3_K8", lambda: g.staircase_lp(3, seed=2), 8)],
+                         ids=["random_m300_K12", "staircase_T3_K8"])
+def test_mixed_batch_reaches_the_target_like_fp64(name, make, K):
+    """The mixed form of the batch (fp32 SpMM and iterates until every running slot asks for fp64
+    under the reference's PrecisionPolicy, then fp64 to the target): every feasible scenario is
+    Optimal at 1e-8 KKT (checked in fp64 on the original model), and its objective is the fp64
+    batch's within 1e-6 relative — the error of mixed against fp64, per scenario."""
+    lp = make()
+    scen = g.feasible_scenarios(lp, K, sigma=0.1, seed=3)
+    A = (lp.col_start, lp.row_index, lp.value)
+    kw = dict(scenarios=scen, sense=lp.sense, offset=lp.offset, engine={"presolve": False})
+    d = ps26119.solve_batch(lp.c, A, lp.row_lower, lp.row_upper, lp.col_lower, lp.col_upper, **kw)
+    m = ps26119.solve_batch(lp.c, A, lp.row_lower, lp.row_upper, lp.col_lower, lp.col_upper, precision="mixed", **kw)
+    for k in range(K):
+        assert d[k].status == ps26119.OPTIMAL and m[k].status == ps26119.OPTIMAL, (k, d[k].message, m[k].message)
+        assert max(m[k].primal_residual, m[k].dual_residual, m[k].gap) <= 1e-8
+        err = abs(m[k].objective - d[k].objective) / (1.0 + abs(d[k].objective))
+        assert err <= 1e-6, (k, err)
