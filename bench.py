@@ -121,21 +121,25 @@ def run_serve(args, rank, world, local):
         seq.append(time.perf_counter() - t0)
         if r.status != ps26119.OPTIMAL:
             raise RuntimeError(f"sequential solve ended {r.status_name}")
-    t_seq = float(np.mean(seq))
-    rate = slots / t_seq
-    gaps = np.random.default_rng(2).exponential(1.0 / rate, N)
+    t_seq = max_over_ranks(float(np.mean(seq)), world)
+    rate = world * slots / t_seq
+    due = np.cumsum(np.random.default_rng(2).exponential(1.0 / rate, N))
+    # several GPUs: every rank serves its share of the stream (longest first to the least-loaded
+    # rank, by nonzeros), at the requests' own arrival times; no data crosses GPUs
+    from ps26119 import shard
+    mine = shard.assign(N, world, [lp.nnz for lp in reqs])[rank]
     steps = []
     with clock_sampler(local) as clocks:
         for _ in range(args.steps):
+            barrier(world)
             with ps26119.Server(slots=slots) as srv:
                 t0 = time.perf_counter()
-                ids, due = [], 0.0
-                for lp, gap in zip(reqs, gaps):
-                    due += gap
-                    pause = due - (time.perf_counter() - t0)
+                ids = []
+                for k in mine:
+                    pause = due[k] - (time.perf_counter() - t0)
                     if pause > 0:
                         time.sleep(pause)
-                    ids.append(srv.submit(lp, precision=args.precision))
+                    ids.append(srv.submit(reqs[k], precision=args.precision))
                 out = [srv.result(i) for i in ids]
             bad = [f"{r.status_name} ({r.message})" for r, _ in out if r.status != ps26119.OPTIMAL or r.check != "PASS"]
             if bad:
@@ -143,29 +147,35 @@ def run_serve(args, rank, world, local):
             sub = np.array([t[0] for _, t in out])
             fin = np.array([t[2] for _, t in out])
             start = np.array([t[1] for _, t in out])
-            steps.append((fin.max() - sub.min(), fin - sub, [r.iterations for r, _ in out], fin - start))
-    sec = max_over_ranks(float(np.mean([s[0] for s in steps])), world)
+            span = max_over_ranks(float(fin.max() - t0) if len(out) else 0.0, world)
+            got = shard.gather({k: (float(f - b), float(f - a), r.iterations)
+                                for k, (r, _), b, a, f in zip(mine, out, sub, start, fin)}, world)
+            steps.append((span, np.array([got[k][0] for k in range(N)]), [got[k][2] for k in range(N)],
+                          np.array([got[k][1] for k in range(N)])))
+    sec = float(np.mean([s[0] for s in steps]))
     lat = np.concatenate([s[1] for s in steps])
     svc = np.concatenate([s[3] for s in steps])
-    value = world * N / sec
+    value = N / sec
     h2d = sum(lp.nnz * 12 + (lp.num_cols + 1) * 4 + lp.num_cols * 24 + lp.num_rows * 16 for lp in reqs)
     d2h = sum(lp.num_cols * 16 + lp.num_rows * 8 for lp in reqs)
     unit = "solves/s"
     return {
         "metric": f"served LP solves/s on {args.workload} ({args.precision}, p50/p99 latency)", "value": value,
         "unit": unit, "n_gpus": world, "steps": args.steps, "warmup": 1, "ms_per_step": sec * 1e3,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "higher_is_better": True, "scaling": "strong" if world > 1 else "weak", "vs_baseline": None,
         "dtype": "f64" if args.precision == "fp64" else "f32+f64", "data": "synthetic (seeded generator)",
         "config": {"workload": w["desc"], "requests": N, "slots": slots, "precision": args.precision,
                    "tolerance": 1e-8, "arrival_rate_per_s": rate, "rows": [int(lp.num_rows) for lp in reqs],
                    "entry": "ps26119_server_submit / ps26119_server_poll (host arrays)",
                    "cuda_device_max_connections": os.environ.get("CUDA_DEVICE_MAX_CONNECTIONS"),
-                   "parallelism": f"replicas x{world}", "l2": "many small LPs: L2-resident, latency-bound"},
+                   "parallelism": f"requests sharded over {world} GPUs" if world > 1 else "1 GPU",
+                   "l2": "many small LPs: L2-resident, latency-bound"},
         "latency_ms": {"p50": float(np.percentile(lat, 50) * 1e3), "p99": float(np.percentile(lat, 99) * 1e3),
                        "mean": float(lat.mean() * 1e3), "note": "submission to completion (queueing included)"},
         "service_ms": {"p50": float(np.percentile(svc, 50) * 1e3), "p99": float(np.percentile(svc, 99) * 1e3),
                        "note": "admission to completion"},
         "sequential_fp64": {"solves_per_s": 1.0 / t_seq, "speedup": value * t_seq / world,
+                            "speedup_note": "per GPU: served solves/s / GPUs x the sequential solve time",
                             "sample": f"{S} of the requests (stratified by size) solved one at a time, plain "
                                       "fp64, ps26119_solve_lp_ex"},
         "iterations": steps[-1][2],
@@ -224,8 +234,12 @@ def run_batch(args, rank, world, local):
     import ps26119
     torch.cuda.set_device(local)
     lp = make_lp(args.workload)
-    scen = make_scenarios(args.workload, lp)
-    K = len(scen)
+    scen_all = make_scenarios(args.workload, lp)
+    # several GPUs: the scenarios are sharded over the ranks (each solves its share as one batch;
+    # no data crosses GPUs), so the whole job is the same K scenarios: strong scaling
+    from ps26119 import shard
+    scen = [scen_all[k] for k in shard.assign(len(scen_all), world)[rank]]
+    K = len(scen_all)
     limit = 0 if args.full else args.iterations
     A = (lp.col_start, lp.row_index, lp.value)
 
@@ -251,9 +265,9 @@ def run_batch(args, rank, world, local):
         sec = time.perf_counter() - t0
     sec = max_over_ranks(sec, world)
     res, st = results[-1]
-    scen_its = sum(r.iterations for r in res)
+    scen_its = sum_over_ranks(float(sum(r.iterations for r in res)), world)
     units = K * args.steps if args.full else scen_its * args.steps
-    value = world * units / sec
+    value = units / sec
     m, n, nnz = lp.num_rows, lp.num_cols, lp.nnz
     bpi = 2 * nnz * 12 + 4 * (m + n) + K * 8 * (9 * n + 7 * m)  # per lockstep iteration, all K slots
     unit = "scenario solves/s" if args.full else "scenario-iterations/s"
@@ -261,12 +275,12 @@ def run_batch(args, rank, world, local):
     line = {
         "metric": f"batched r2HPDHG on {args.workload} ({unit})", "value": value, "unit": unit, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3 / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
-        "data": "synthetic (seeded generator)",
+        "scaling": "strong" if world > 1 else "weak", "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "f32+f64", "data": "synthetic (seeded generator)",
         "config": {"workload": WORKLOADS[args.workload]["desc"], "m": m, "n": n, "nnz": nnz, "scenarios": K,
                    "precision": args.precision,
                    "tolerance": 1e-8, "iteration_cap": limit or None, "entry": "ps26119_solve_batch (host arrays)",
-                   "iterations_per_step": its, "parallelism": f"replicas x{world}",
+                   "iterations_per_step": its, "parallelism": f"scenarios sharded over {world} GPUs" if world > 1 else "1 GPU",
                    "l2": f"inputs larger than L2: {bpi / 1e6:.0f} MB streamed per lockstep iteration"},
         "roofline": roofline_batch(bpi, its, args, sec, results),
         "gpu_launches": int(sum(s["kernel_launches"] for _, s in results)),
@@ -463,6 +477,17 @@ def max_over_ranks(v, world):
     dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
     t = torch.tensor([v], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
     return float(t.item())
 
 
