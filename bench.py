@@ -132,7 +132,7 @@ def run_serve(args, rank, world, local):
     with clock_sampler(local) as clocks:
         for _ in range(args.steps):
             barrier(world)
-            with ps26119.Server(slots=slots) as srv:
+            with ps26119.Server(slots=slots, grouped=not args.serve_solo) as srv:
                 t0 = time.perf_counter()
                 ids = []
                 for k in mine:
@@ -167,6 +167,8 @@ def run_serve(args, rank, world, local):
         "config": {"workload": w["desc"], "requests": N, "slots": slots, "precision": args.precision,
                    "tolerance": 1e-8, "arrival_rate_per_s": rate, "rows": [int(lp.num_rows) for lp in reqs],
                    "entry": "ps26119_server_submit / ps26119_server_poll (host arrays)",
+                   "engines": "each request's own kernels" if args.serve_solo else
+                              "grouped: one launch per half-step over every running request",
                    "cuda_device_max_connections": os.environ.get("CUDA_DEVICE_MAX_CONNECTIONS"),
                    "parallelism": f"requests sharded over {world} GPUs" if world > 1 else "1 GPU",
                    "l2": "many small LPs: L2-resident, latency-bound"},
@@ -818,6 +820,8 @@ def main():
     ap.add_argument("--no-time-to-tol", action="store_true", help="skip the measured time-to-1e-8 records")
     ap.add_argument("--serve-sample", type=int, default=8, help="requests solved sequentially for the baseline")
     ap.add_argument("--serve-slots", type=int, default=0, help="server slots (0: the workload's)")
+    ap.add_argument("--serve-solo", action="store_true",
+                    help="each served request launches its own kernels (no grouped launches)")
     args = ap.parse_args()
     if WORKLOADS[args.workload]["kind"] == "serve":
         # one hardware work queue per slot (the default, 8, makes streams beyond 8 share queues);

@@ -236,6 +236,9 @@ typedef struct {
   double hbm_budget_bytes; /* device memory for the running requests (0 = 80% of free memory) */
   double dry_run_seconds;  /* > 0: requests are admitted and timed but not solved (each holds its
                               slot and memory this long); status NOT_SOLVED, engine "dry-run" */
+  int solo_engines;        /* 0 (default): the r²HPDHG epochs of all running requests are launched
+                              together, one grouped kernel per half-step over every request's
+                              slabs; 1: each request's engine launches its own kernels */
 } ps26119_server_options;
 
 typedef struct {

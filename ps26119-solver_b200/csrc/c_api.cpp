@@ -729,6 +729,7 @@ extern "C" ps26119_server* ps26119_server_create(const ps26119_server_options* o
     o.slots = opt->slots;
     o.hbm_budget_bytes = opt->hbm_budget_bytes;
     o.dry_run_seconds = opt->dry_run_seconds;
+    o.grouped = opt->solo_engines == 0;
   }
   try {
     return new ps26119_server(o);

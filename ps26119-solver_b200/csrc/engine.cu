@@ -18,10 +18,16 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <condition_variable>
 #include <cstdio>
+#include <exception>
 #include <limits>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <string>
+#include <thread>
+#include <vector>
 
 #include "checks.cuh"
 #include "engine.hpp"
@@ -130,6 +136,38 @@ class Engine {
 
   EngineResult run(const DeviceOutputs& out);
   EngineResult run_pdlp(const DeviceOutputs& out);
+  // run() as steps, for a scheduler that interleaves several engines on one stream:
+  // start() once (true: finished already); then per epoch begin_epoch(), the epoch's iteration
+  // kernels (launch_epoch(), or a scheduler's grouped kernels followed by launch_r0()),
+  // launch_check(), a synchronisation of the stream, end_epoch() (true: finished). result()
+  // holds the outcome once finished.
+  bool start(const DeviceOutputs& out);
+  void begin_epoch();
+  void launch_epoch();
+  void launch_r0();
+  void launch_check();
+  bool end_epoch();
+  const EngineResult& result() const { return R_; }
+  int check_every() const { return o_.check_every; }
+  // Moves the engine to another stream once its setup has finished (start() returned false):
+  // waits for the work enqueued so far, then every later launch goes to `s`.
+  void rebind_stream(cudaStream_t s) {
+    B200_CHECK(cudaStreamSynchronize(st_));
+    st_ = s;
+  }
+  bool mixed_now() const { return mixed_now_; }
+  // the operands of this engine's iteration kernels at step s of the current epoch
+  template <class T> EpiPrimal<T> primal_epi(int s);
+  template <class T> EpiDual<T> dual_epi(int s);
+  struct SlabOperands {
+    int rows, cap;
+    const int *rp, *col;
+    const void *val, *x;
+    const int2* slab;
+    unsigned* err;
+  };
+  template <class T> SlabOperands primal_operands();
+  template <class T> SlabOperands dual_operands();
   // Bulk-copy waits of this solve's kernels that ran out (synchronises the stream).
   unsigned stage_errors() {
     unsigned v = 0;
@@ -143,6 +181,18 @@ class Engine {
  private:
   using clock = std::chrono::steady_clock;
   unsigned* err() { return stage_err_.get(); }
+  void finish_run(Status s, bool hat, const std::string& m, int ray);
+  struct LoopState {  // the r²HPDHG loop's scalars (r2hpdhg.cpp:41-160)
+    double omega = 1.0, pid_integral = 0.0, pid_last = 0.0, best_omega = 1.0, best_balance = 1e300;
+    long long it = 0, inner = 0;
+    double r0 = -1.0, r_last = std::numeric_limits<double>::infinity();
+    std::string msg;
+    bool fresh = false, finished = false;
+    int variant = 0;
+  };
+  LoopState L_;
+  EngineResult R_;
+  const DeviceOutputs* out_ = nullptr;
   double elapsed() const { return std::chrono::duration<double>(clock::now() - t0_).count(); }
 
   template <class T> IterVecs<T>& vecs();
@@ -434,6 +484,29 @@ void Engine::launch_ray(const T* dx, const T* dy, double* r, double* d, int drif
   SumPlan& p = drift ? plan_ray2_ : plan_ray1_;
   p.launch(st_);
   B200_COUNT(4 + p.kernel_count());
+}
+
+template <class T>
+EpiPrimal<T> Engine::primal_epi(int s) {
+  IterVecs<T>& v = vecs<T>();
+  return EpiPrimal<T>{v.x.get(), v.xh.get(), v.xb.get(), v.x0.get(), sp_.c<T>(), sp_.l<T>(), sp_.u<T>(), params_.get(),
+                      s, 0, 0, 0};
+}
+template <class T>
+EpiDual<T> Engine::dual_epi(int s) {
+  IterVecs<T>& v = vecs<T>();
+  return EpiDual<T>{v.y.get(), v.yh.get(), v.yb.get(), v.y0.get(), sp_.rl<T>(), sp_.ru<T>(), params_.get(), s, 0, 0, 0,
+                    0};
+}
+template <class T>
+Engine::SlabOperands Engine::primal_operands() {  // Ãᵀy: rows of Ãᵀ (the columns), gathers y
+  return SlabOperands{M_.n, cap_t_, sp_.t_rp.get(), sp_.t_ri.get(), sp_.At_val<T>(), vecs<T>().y.get(), slab_t_.get(),
+                      err()};
+}
+template <class T>
+Engine::SlabOperands Engine::dual_operands() {  // Ãx̄: rows of Ã, gathers x̄
+  return SlabOperands{M_.m, cap_a_, sp_.a_rp.get(), sp_.a_col.get(), sp_.A_val<T>(), vecs<T>().xb.get(),
+                      slab_a_.get(), err()};
 }
 
 template <class T>
@@ -771,30 +844,36 @@ Status Engine::ray_verdict(const double* h, int which, const Kkt& k, std::string
   return Status::NotSolved;
 }
 
-EngineResult Engine::run(const DeviceOutputs& out) {
+// The r²HPDHG solve as steps. run() chains them on this engine's stream; the group scheduler
+// (group.cu) interleaves the steps of several engines on one stream, launching their iteration
+// kernels together. Either way each engine takes the same values and decisions.
+
+void Engine::finish_run(Status s, bool hat, const std::string& m, int ray) {
+  R_.loop_seconds = elapsed() - R_.setup_seconds;
+  finish(R_, s, hat, L_.it, m, *out_, ray);
+  R_.kernel_launches = kernels_;
+  R_.iter_kernel_ms = iter_ms_;
+  R_.iter_kernel_launches = iter_launches_;
+  R_.slab_variant_primal = var_t_, R_.slab_variant_dual = var_a_, R_.tuned = tuned_now_ ? 1 : 0;
+  R_.seconds = elapsed();
+  L_.finished = true;
+}
+
+bool Engine::start(const DeviceOutputs& out) {
   t0_ = clock::now();
-  EngineResult R;
+  out_ = &out;
+  R_ = EngineResult{};
+  L_ = LoopState{};
   setup();
   mixed_now_ = o_.mixed;
-  const double rho = o_.reflection;
-  double omega = initial_primal_weight();
+  L_.omega = initial_primal_weight();
   if (mixed_now_) init_iterates<float>();
   else init_iterates<double>();
   const bool warm = apply_warm_start();
-  primal_weight_ = omega;
-  std::string msg = warm ? "warm start" : "";
-  const int K = o_.check_every;
-  R.setup_seconds = elapsed();
-  auto done = [&](Status s, bool hat, long long it, const std::string& m, int ray) {
-    R.loop_seconds = elapsed() - R.setup_seconds;
-    finish(R, s, hat, it, m, out, ray);
-    R.kernel_launches = kernels_;
-    R.iter_kernel_ms = iter_ms_;
-    R.iter_kernel_launches = iter_launches_;
-    R.slab_variant_primal = var_t_, R.slab_variant_dual = var_a_, R.tuned = tuned_now_ ? 1 : 0;
-    R.seconds = elapsed();
-    return R;
-  };
+  primal_weight_ = L_.omega;
+  L_.best_omega = L_.omega;
+  L_.msg = warm ? "warm start" : "";
+  R_.setup_seconds = elapsed();
   if (warm) {  // the warm point may already be good enough (r2hpdhg.cpp:37-40)
     clear_maxima();
     if (mixed_now_) launch_kkt_scaled<float>(vf_.x.get(), vf_.y.get());
@@ -802,134 +881,173 @@ EngineResult Engine::run(const DeviceOutputs& out) {
     sync_results();
     const Kkt kw = read_kkt(hres_.get());
     if (fast_it_ < 0 && kw.rel_kkt() <= kFirstOrderFast) fast_it_ = 0;
-    if (kw.finite() && kw.converged(o_.tolerance)) return done(Status::Optimal, false, 0, "warm start already optimal", 0);
-  }
-  {
-    const long long m = M_.m, n = M_.n;
-    if (mixed_now_) {
-      B200_CHECK(cudaMemcpyAsync(vf_.x0.get(), vf_.x.get(), n * sizeof(float), cudaMemcpyDeviceToDevice, st_));
-      B200_CHECK(cudaMemcpyAsync(vf_.xh.get(), vf_.x.get(), n * sizeof(float), cudaMemcpyDeviceToDevice, st_));
-      B200_CHECK(cudaMemcpyAsync(vf_.y0.get(), vf_.y.get(), m * sizeof(float), cudaMemcpyDeviceToDevice, st_));
-      B200_CHECK(cudaMemcpyAsync(vf_.yh.get(), vf_.y.get(), m * sizeof(float), cudaMemcpyDeviceToDevice, st_));
-    } else {
-      B200_CHECK(cudaMemcpyAsync(vd_.x0.get(), vd_.x.get(), n * sizeof(double), cudaMemcpyDeviceToDevice, st_));
-      B200_CHECK(cudaMemcpyAsync(vd_.xh.get(), vd_.x.get(), n * sizeof(double), cudaMemcpyDeviceToDevice, st_));
-      B200_CHECK(cudaMemcpyAsync(vd_.y0.get(), vd_.y.get(), m * sizeof(double), cudaMemcpyDeviceToDevice, st_));
-      B200_CHECK(cudaMemcpyAsync(vd_.yh.get(), vd_.y.get(), m * sizeof(double), cudaMemcpyDeviceToDevice, st_));
+    if (kw.finite() && kw.converged(o_.tolerance)) {
+      finish_run(Status::Optimal, false, "warm start already optimal", 0);
+      return true;
     }
   }
-  double pid_integral = 0.0, pid_last = 0.0, best_omega = omega, best_balance = 1e300;
-  long long it = 0, inner = 0;
-  double r0 = -1.0, r_last = std::numeric_limits<double>::infinity();
+  const long long m = M_.m, n = M_.n;
+  if (mixed_now_) {
+    B200_CHECK(cudaMemcpyAsync(vf_.x0.get(), vf_.x.get(), n * sizeof(float), cudaMemcpyDeviceToDevice, st_));
+    B200_CHECK(cudaMemcpyAsync(vf_.xh.get(), vf_.x.get(), n * sizeof(float), cudaMemcpyDeviceToDevice, st_));
+    B200_CHECK(cudaMemcpyAsync(vf_.y0.get(), vf_.y.get(), m * sizeof(float), cudaMemcpyDeviceToDevice, st_));
+    B200_CHECK(cudaMemcpyAsync(vf_.yh.get(), vf_.y.get(), m * sizeof(float), cudaMemcpyDeviceToDevice, st_));
+  } else {
+    B200_CHECK(cudaMemcpyAsync(vd_.x0.get(), vd_.x.get(), n * sizeof(double), cudaMemcpyDeviceToDevice, st_));
+    B200_CHECK(cudaMemcpyAsync(vd_.xh.get(), vd_.x.get(), n * sizeof(double), cudaMemcpyDeviceToDevice, st_));
+    B200_CHECK(cudaMemcpyAsync(vd_.y0.get(), vd_.y.get(), m * sizeof(double), cudaMemcpyDeviceToDevice, st_));
+    B200_CHECK(cudaMemcpyAsync(vd_.yh.get(), vd_.y.get(), m * sizeof(double), cudaMemcpyDeviceToDevice, st_));
+  }
+  return false;
+}
+
+// The step scalars of the next epoch: τ = η/ω, σ = ηω (r2hpdhg.cpp:67), the Halpern counter.
+void Engine::begin_epoch() {
   StepParams& hp = *hparams_.get();
+  hp.tau = eta_ / L_.omega;
+  hp.sigma = eta_ * L_.omega;
+  hp.rho = o_.reflection;
+  hp.inner0 = L_.inner;
+  hp.K = o_.check_every;
+  hp.done = 0;
+  hp.skip_r0 = L_.inner != 0 ? 1 : 0;
+  B200_CHECK(cudaMemcpyAsync(params_.get(), &hp, sizeof(StepParams), cudaMemcpyHostToDevice, st_));
+  L_.fresh = L_.inner == 0;
+}
+
+void Engine::launch_epoch() {
+  const int pidx = mixed_now_ ? 1 : 0;
+  if (mixed_now_) capture_epoch<float>();
+  else capture_epoch<double>();
+  B200_CHECK(cudaGraphLaunch(g_epoch_[pidx], st_));
+  kernels_ += epoch_kernels_[pidx];
+}
+
+// The r⁰ residual after the first step of an epoch that starts a Halpern cycle (the section the
+// epoch graph holds), for epochs whose steps the group scheduler launches.
+void Engine::launch_r0() {
+  if (!L_.fresh) return;
+  if (mixed_now_) launch_residual<float>(false, nullptr, plan_r0_);
+  else launch_residual<double>(false, nullptr, plan_r0_);
+}
+
+void Engine::launch_check() {
+  const int K = o_.check_every;
+  L_.it += K;
+  L_.inner += K;
+  L_.variant = L_.it >= 4LL * K ? (((L_.it / K) % 4 == 0) ? 2 : 1) : 0;
+  const int pidx = mixed_now_ ? 1 : 0;
+  if (mixed_now_) capture_check<float>(L_.variant);
+  else capture_check<double>(L_.variant);
+  B200_CHECK(cudaGraphLaunch(g_check_[pidx][L_.variant], st_));
+  kernels_ += check_kernels_[pidx][L_.variant];
+}
+
+// The reference's decisions on the check's results (r2hpdhg.cpp:93-160, engine.cpp:56-192),
+// once the stream has synchronised. Returns true when the solve has ended (result in R_).
+bool Engine::end_epoch() {
+  LoopState& S = L_;
+  ++R_.checks;
+  const double* h = hres_.get();
+  const double omega = S.omega;
+  if (S.fresh) S.r0 = std::sqrt(std_max(omega * h[kPx0] + h[kPy0] / omega + 2.0 * eta_ * h[kCross0], 0.0));
+  const double r = std::sqrt(std_max(omega * h[kPx] + h[kPy] / omega + 2.0 * eta_ * h[kCross], 0.0));
+  const Kkt k = read_kkt(h);
+  if (o_.verbosity >= 2)
+    std::fprintf(stderr, "r2hpdhg-b200 it %8lld  t %7.2fs  pobj %+.10e  dobj %+.10e  rp %.2e  rd %.2e  gap %.2e  %s\n",
+                 S.it, elapsed(), k.primal_obj, k.dual_obj, k.rel_primal(), k.rel_dual(), k.rel_gap(),
+                 mixed_now_ ? "fp32" : "fp64");
+  auto done = [&](Status st, bool hat, const std::string& m, int ray) {
+    finish_run(st, hat, m, ray);
+    return true;
+  };
+  if (!k.finite() || !std::isfinite(r)) return done(Status::NumericalError, true, "non-finite iterate", 0);
+  if (fast_it_ < 0 && k.rel_kkt() <= kFirstOrderFast) fast_it_ = S.it;
+  if (k.converged(o_.tolerance)) return done(Status::Optimal, true, S.msg, 0);
+  if (S.it >= o_.iteration_limit) return done(Status::IterationLimit, true, S.msg, 0);
+  if (elapsed() > o_.time_limit) return done(Status::TimeLimit, true, S.msg, 0);
+  if (S.variant >= 1) {  // EngineContext::check_infeasibility + ray_test (engine.cpp:82-184)
+    auto test = [&](int which, std::string& why) { return ray_verdict(h, which, k, why); };
+    std::string why;
+    int which = 1;
+    Status st = test(1, why);
+    if (st == Status::NotSolved && S.variant == 2) {
+      which = 2;
+      st = test(2, why);
+      if (st != Status::NotSolved) why += " (drift since the restart anchor)";
+    }
+    if (st != Status::NotSolved) return done(st, true, why, which);
+  }
+  // PrecisionPolicy::on_check (engine.cpp:61-79)
+  bool promoted = false;
+  if (o_.mixed && mixed_now_) {
+    const double rk = k.rel_kkt();
+    if (rk < 0.9 * pol_best_) pol_best_ = rk, pol_since_best_ = 0;
+    else ++pol_since_best_;
+    const bool reached = rk <= kMixedPrecisionSwitch && o_.tolerance < kMixedPrecisionSwitch;
+    if (reached || pol_since_best_ >= 10) {
+      promote();
+      switch_it_ = S.it;
+      promoted = true;
+      S.msg += std::string(S.msg.empty() ? "" : "; ") + "fp32 -> fp64 at iteration " + std::to_string(S.it);
+    }
+  }
+  const bool ratios_ok = S.r0 > 0 && std::isfinite(S.r0) && r > 0;
+  const bool restart_now = promoted ||
+                           (ratios_ok && (r <= o_.restart_sufficient * S.r0 ||
+                                          (r <= o_.restart_necessary * S.r0 && r > S.r_last))) ||
+                           static_cast<double>(S.inner) >= o_.restart_artificial * static_cast<double>(S.it);
+  S.r_last = r;
+  if (!restart_now) return false;
+  // PID primal weight (r2hpdhg.cpp:126-148)
+  const double dxn = std::sqrt(h[kDxn2]), dyn = std::sqrt(h[kDyn2]);
+  const bool both_pos = k.rel_dual() > 0 && k.rel_primal() > 0;
+  const double ratio = both_pos ? k.rel_dual() / k.rel_primal() : 1.0;
+  if (dxn > 1e-16 && dyn > 1e-16 && dxn < 1e12 && dyn < 1e12 && ratio > 1e-8 && ratio < 1e8) {
+    const double e = std::log(dyn) - std::log(dxn) - std::log(S.omega);
+    S.pid_integral = o_.pid_integral_decay * S.pid_integral + e;
+    const double step = o_.pid_kp * e + o_.pid_ki * S.pid_integral + o_.pid_kd * (e - S.pid_last);
+    S.omega *= std::exp(std::clamp(step, -o_.pid_max_log_step, o_.pid_max_log_step));
+    S.pid_last = e;
+  } else {
+    S.omega = S.best_omega;
+    S.pid_integral = S.pid_last = 0.0;
+  }
+  const double balance = std::fabs(std::log10(ratio));
+  if (both_pos && balance < S.best_balance) {
+    S.best_balance = balance;
+    S.best_omega = S.omega;
+  }
+  primal_weight_ = S.omega;
+  ++R_.restarts;
+  if (o_.verbosity >= 2)
+    std::fprintf(stderr, "  restart at %lld: r/r0 %.3f  omega %.4e  dx %.3e dy %.3e\n", S.it, r / S.r0, S.omega, dxn,
+                 dyn);
+  if (mixed_now_) restart<float>();
+  else restart<double>();
+  S.inner = 0;
+  S.r_last = std::numeric_limits<double>::infinity();
+  return false;
+}
+
+EngineResult Engine::run(const DeviceOutputs& out) {
+  if (start(out)) return R_;
+  const int K = o_.check_every;
   for (;;) {
-    const double tau = eta_ / omega, sigma = eta_ * omega;
-    hp.tau = tau;
-    hp.sigma = sigma;
-    hp.rho = rho;
-    hp.inner0 = inner;
-    hp.K = K;
-    hp.done = 0;
-    hp.skip_r0 = inner != 0 ? 1 : 0;
-    B200_CHECK(cudaMemcpyAsync(params_.get(), &hp, sizeof(StepParams), cudaMemcpyHostToDevice, st_));
-    const bool fresh = inner == 0;
-    const int pidx = mixed_now_ ? 1 : 0;
-    if (mixed_now_) capture_epoch<float>();
-    else capture_epoch<double>();
-    B200_CHECK(cudaGraphLaunch(g_epoch_[pidx], st_));
-    kernels_ += epoch_kernels_[pidx];
-    it += K;
-    inner += K;
-    const int variant = it >= 4LL * K ? (((it / K) % 4 == 0) ? 2 : 1) : 0;
-    if (mixed_now_) capture_check<float>(variant);
-    else capture_check<double>(variant);
-    B200_CHECK(cudaGraphLaunch(g_check_[pidx][variant], st_));
-    kernels_ += check_kernels_[pidx][variant];
+    begin_epoch();
+    launch_epoch();
+    launch_check();
     B200_CHECK(cudaStreamSynchronize(st_));
-    ++R.checks;
-    {
+    {  // the iteration kernels' time, from the events inside the epoch graph
       float a = 0, b = 0;
       B200_CHECK(cudaEventElapsedTime(&a, ev_[0], ev_[1]));
       B200_CHECK(cudaEventElapsedTime(&b, ev_[2], ev_[3]));
       iter_ms_ += a + b;
       iter_launches_ += 2LL * K;
     }
-    const double* h = hres_.get();
-    if (fresh) r0 = std::sqrt(std_max(omega * h[kPx0] + h[kPy0] / omega + 2.0 * eta_ * h[kCross0], 0.0));
-    const double r = std::sqrt(std_max(omega * h[kPx] + h[kPy] / omega + 2.0 * eta_ * h[kCross], 0.0));
-    const Kkt k = read_kkt(h);
-    if (o_.verbosity >= 2)
-      std::fprintf(stderr, "r2hpdhg-b200 it %8lld  t %7.2fs  pobj %+.10e  dobj %+.10e  rp %.2e  rd %.2e  gap %.2e  %s\n",
-                   it, elapsed(), k.primal_obj, k.dual_obj, k.rel_primal(), k.rel_dual(), k.rel_gap(),
-                   mixed_now_ ? "fp32" : "fp64");
-    if (!k.finite() || !std::isfinite(r)) return done(Status::NumericalError, true, it, "non-finite iterate", 0);
-    if (fast_it_ < 0 && k.rel_kkt() <= kFirstOrderFast) fast_it_ = it;
-    if (k.converged(o_.tolerance)) return done(Status::Optimal, true, it, msg, 0);
-    if (it >= o_.iteration_limit) return done(Status::IterationLimit, true, it, msg, 0);
-    if (elapsed() > o_.time_limit) return done(Status::TimeLimit, true, it, msg, 0);
-    if (variant >= 1) {  // EngineContext::check_infeasibility + ray_test (engine.cpp:82-184)
-      auto test = [&](int which, std::string& why) { return ray_verdict(h, which, k, why); };
-      std::string why;
-      int which = 1;
-      Status s = test(1, why);
-      if (s == Status::NotSolved && variant == 2) {
-        which = 2;
-        s = test(2, why);
-        if (s != Status::NotSolved) why += " (drift since the restart anchor)";
-      }
-      if (s != Status::NotSolved) return done(s, true, it, why, which);
-    }
-    // PrecisionPolicy::on_check (engine.cpp:61-79)
-    bool promoted = false;
-    if (o_.mixed && mixed_now_) {
-      const double rk = k.rel_kkt();
-      if (rk < 0.9 * pol_best_) pol_best_ = rk, pol_since_best_ = 0;
-      else ++pol_since_best_;
-      const bool reached = rk <= kMixedPrecisionSwitch && o_.tolerance < kMixedPrecisionSwitch;
-      if (reached || pol_since_best_ >= 10) {
-        promote();
-        switch_it_ = it;
-        promoted = true;
-        msg += std::string(msg.empty() ? "" : "; ") + "fp32 -> fp64 at iteration " + std::to_string(it);
-      }
-    }
-    const bool ratios_ok = r0 > 0 && std::isfinite(r0) && r > 0;
-    const bool restart_now = promoted ||
-                             (ratios_ok && (r <= o_.restart_sufficient * r0 ||
-                                            (r <= o_.restart_necessary * r0 && r > r_last))) ||
-                             static_cast<double>(inner) >= o_.restart_artificial * static_cast<double>(it);
-    r_last = r;
-    if (!restart_now) continue;
-    // PID primal weight (r2hpdhg.cpp:126-148)
-    const double dxn = std::sqrt(h[kDxn2]), dyn = std::sqrt(h[kDyn2]);
-    const bool both_pos = k.rel_dual() > 0 && k.rel_primal() > 0;
-    const double ratio = both_pos ? k.rel_dual() / k.rel_primal() : 1.0;
-    if (dxn > 1e-16 && dyn > 1e-16 && dxn < 1e12 && dyn < 1e12 && ratio > 1e-8 && ratio < 1e8) {
-      const double e = std::log(dyn) - std::log(dxn) - std::log(omega);
-      pid_integral = o_.pid_integral_decay * pid_integral + e;
-      const double step = o_.pid_kp * e + o_.pid_ki * pid_integral + o_.pid_kd * (e - pid_last);
-      omega *= std::exp(std::clamp(step, -o_.pid_max_log_step, o_.pid_max_log_step));
-      pid_last = e;
-    } else {
-      omega = best_omega;
-      pid_integral = pid_last = 0.0;
-    }
-    const double balance = std::fabs(std::log10(ratio));
-    if (both_pos && balance < best_balance) {
-      best_balance = balance;
-      best_omega = omega;
-    }
-    primal_weight_ = omega;
-    ++R.restarts;
-    if (o_.verbosity >= 2)
-      std::fprintf(stderr, "  restart at %lld: r/r0 %.3f  omega %.4e  dx %.3e dy %.3e\n", it, r / r0, omega, dxn, dyn);
-    if (mixed_now_) restart<float>();
-    else restart<double>();
-    inner = 0;
-    r_last = std::numeric_limits<double>::infinity();
+    if (end_epoch()) return R_;
   }
 }
-
 
 // ============================================================================ PDLP
 // Restarted averaged PDHG (reference src/pdhg/pdlp.cpp:9-126) on the same fused kernels. The
@@ -1236,7 +1354,175 @@ EngineResult Engine::run_pdlp(const DeviceOutputs& out) {
     last_candidate = 1e300;
   }
 }
+// ================================================================ continuous batching
+// The group scheduler: one host thread and one stream per device run the r²HPDHG epochs of every
+// solve in flight together. Per epoch, each half-step is ONE launch of k_group_fed over the slabs
+// of all the solves in that working precision (instead of one launch per solve), each solve with
+// its own step scalars, iterates and epilogue; then every solve's own residual section (when its
+// epoch starts a Halpern cycle) and check graph follow on the same stream, one synchronisation
+// covers them all, and each solve takes its own decisions. A solve joins at the next epoch
+// boundary once its setup (on its caller's thread and stream) is done, and leaves when it has
+// finished, so requests that arrive while others run are admitted into the running group.
+// The grouped kernel runs each row's arithmetic exactly as the solve's own kernel, and the
+// checks are the solve's own graphs, so a solve's result does not depend on its company.
+class GroupScheduler {
+ public:
+  struct Job {
+    Engine* e = nullptr;
+    bool done = false;
+    unsigned timeouts = 0;
+    std::exception_ptr error;
+  };
+  static GroupScheduler& for_current_device() {
+    static std::mutex mu;
+    static std::map<int, GroupScheduler*> all;  // never destroyed: the threads live until exit
+    int dev = 0;
+    B200_CHECK(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(mu);
+    GroupScheduler*& g = all[dev];
+    if (!g) g = new GroupScheduler(dev);
+    return *g;
+  }
+  cudaStream_t stream() const { return st_; }
+  // Runs the engine's epochs in the group until it finishes (the caller's thread waits).
+  void run(Job& job) {
+    std::unique_lock<std::mutex> lk(mu_);
+    pending_.push_back(&job);
+    cv_.notify_all();
+    done_cv_.wait(lk, [&] { return job.done; });
+    if (job.error) std::rethrow_exception(job.error);
+  }
+
+ private:
+  explicit GroupScheduler(int dev) : dev_(dev) {
+    B200_CHECK(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
+    thread_ = std::thread([this] { loop(); });
+    thread_.detach();
+  }
+  template <class T>
+  struct Tables {  // the grouped launches' parts in one working precision (pinned and device)
+    std::vector<GroupPart<T, EpiPrimal<T>>> hp;
+    std::vector<GroupPart<T, EpiDual<T>>> hd;
+    PinnedBuf<GroupPart<T, EpiPrimal<T>>> pp;
+    PinnedBuf<GroupPart<T, EpiDual<T>>> pd;
+    DevBuf<GroupPart<T, EpiPrimal<T>>> dp;
+    DevBuf<GroupPart<T, EpiDual<T>>> dd;
+    int blocks_p = 0, blocks_d = 0, cap_p = 16, cap_d = 16;
+    void clear() { hp.clear(), hd.clear(), blocks_p = blocks_d = 0, cap_p = cap_d = 16; }
+  };
+  template <class T>
+  void add(Tables<T>& tb, Engine& e) {
+    const Engine::SlabOperands a = e.primal_operands<T>(), b = e.dual_operands<T>();
+    tb.hp.push_back({a.rows, a.cap, tb.blocks_p, a.rp, a.col, static_cast<const T*>(a.val),
+                     static_cast<const T*>(a.x), a.slab, a.err, e.primal_epi<T>(0)});
+    tb.hd.push_back({b.rows, b.cap, tb.blocks_d, b.rp, b.col, static_cast<const T*>(b.val),
+                     static_cast<const T*>(b.x), b.slab, b.err, e.dual_epi<T>(0)});
+    tb.blocks_p += slab_count(a.rows), tb.blocks_d += slab_count(b.rows);
+    tb.cap_p = std::max(tb.cap_p, a.cap), tb.cap_d = std::max(tb.cap_d, b.cap);
+  }
+  template <class T>
+  void upload(Tables<T>& tb) {
+    const std::size_t n = tb.hp.size();
+    if (n == 0) return;
+    if (tb.pp.size() < n) tb.pp.alloc(2 * n), tb.pd.alloc(2 * n), tb.dp.alloc(2 * n), tb.dd.alloc(2 * n);
+    std::copy(tb.hp.begin(), tb.hp.end(), tb.pp.get());
+    std::copy(tb.hd.begin(), tb.hd.end(), tb.pd.get());
+    B200_CHECK(cudaMemcpyAsync(tb.dp.get(), tb.pp.get(), n * sizeof(tb.hp[0]), cudaMemcpyHostToDevice, st_));
+    B200_CHECK(cudaMemcpyAsync(tb.dd.get(), tb.pd.get(), n * sizeof(tb.hd[0]), cudaMemcpyHostToDevice, st_));
+  }
+  // One half-step of every solve in precision T: the primal (Ãᵀy) or dual (Ãx̄) grouped kernel.
+  // pdl: programmatic dependent launch, as in the solo epoch graph (every dual; every primal
+  // whose predecessor is a grouped kernel).
+  template <class T, class Epi>
+  void launch(const DevBuf<GroupPart<T, Epi>>& parts, int nparts, int blocks, int cap, int step, bool pdl) {
+    if (nparts == 0 || blocks == 0) return;
+    const unsigned smem = fed_layout(Epi::kVecs, static_cast<int>(sizeof(T)), cap).bytes;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(static_cast<unsigned>(blocks));
+    cfg.blockDim = dim3(kSlabRows);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st_;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = (B200_PDL && pdl) ? 1 : 0;
+    B200_CHECK(cudaLaunchKernelEx(&cfg, k_group_fed<T, Epi>, parts.get(), nparts, step));
+  }
+  void epoch(std::vector<Job*>& active) {
+    tf_.clear(), td_.clear();
+    for (Job* j : active) {
+      j->e->begin_epoch();
+      if (j->e->mixed_now()) add(tf_, *j->e);
+      else add(td_, *j->e);
+    }
+    upload(tf_), upload(td_);
+    const int nf = static_cast<int>(tf_.hp.size()), nd = static_cast<int>(td_.hp.size());
+    const int K = active.front()->e->check_every();
+    for (int s = 0; s < K; ++s) {
+      const bool pdl_primal = s >= 2;  // step 1 follows the residual sections
+      launch(td_.dp, nd, td_.blocks_p, td_.cap_p, s, pdl_primal && nf == 0);
+      launch(tf_.dp, nf, tf_.blocks_p, tf_.cap_p, s, false);
+      launch(td_.dd, nd, td_.blocks_d, td_.cap_d, s, nf == 0);
+      launch(tf_.dd, nf, tf_.blocks_d, tf_.cap_d, s, false);
+      if (s == 0)
+        for (Job* j : active) j->e->launch_r0();
+    }
+    for (Job* j : active) j->e->launch_check();
+    B200_CHECK(cudaStreamSynchronize(st_));
+  }
+  void loop() {
+    (void)cudaSetDevice(dev_);
+    std::vector<Job*> active;
+    for (;;) {
+      {
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_.wait(lk, [&] { return !pending_.empty() || !active.empty(); });
+        for (Job* j : pending_) active.push_back(j);
+        pending_.clear();
+      }
+      std::vector<Job*> finished;
+      try {
+        epoch(active);
+        for (std::size_t k = 0; k < active.size();) {
+          Job* j = active[k];
+          if (j->e->end_epoch()) {
+            j->timeouts = j->e->stage_errors();
+            finished.push_back(j);
+            active.erase(active.begin() + static_cast<long>(k));
+          } else {
+            ++k;
+          }
+        }
+      } catch (...) {  // a device error: every solve in the group ends with it
+        const std::exception_ptr err = std::current_exception();
+        for (Job* j : active) j->error = err, finished.push_back(j);
+        active.clear();
+        (void)cudaGetLastError();
+      }
+      if (!finished.empty()) {
+        std::lock_guard<std::mutex> lk(mu_);
+        for (Job* j : finished) j->done = true;
+        done_cv_.notify_all();
+      }
+    }
+  }
+  int dev_ = 0;
+  cudaStream_t st_ = nullptr;
+  std::thread thread_;
+  std::mutex mu_;
+  std::condition_variable cv_, done_cv_;
+  std::vector<Job*> pending_;
+  Tables<double> td_;
+  Tables<float> tf_;
+};
+
 }  // namespace
+
+namespace {
+thread_local bool t_grouped = false;
+}
+void set_grouped_engine(bool on) { t_grouped = on; }
 
 EngineResult run_engine(const DeviceModel& M, const EngineOptions& opt, const DeviceOutputs& out, void* stream) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -1261,8 +1547,24 @@ EngineResult run_engine(const DeviceModel& M, const EngineOptions& opt, const De
   unsigned timeouts = 0;
   {
     auto e = std::make_unique<Engine>(M, opt, st);
-    R = opt.pdlp ? e->run_pdlp(out) : e->run(out);
-    timeouts = e->stage_errors();
+    if (t_grouped && !opt.pdlp && opt.check_every == 64) {
+      // setup here, on this caller's stream; the epochs in the device's group
+      if (e->start(out)) {
+        R = e->result();
+        timeouts = e->stage_errors();
+      } else {
+        GroupScheduler& g = GroupScheduler::for_current_device();
+        e->rebind_stream(g.stream());
+        GroupScheduler::Job job;
+        job.e = e.get();
+        g.run(job);
+        R = e->result();
+        timeouts = job.timeouts;
+      }
+    } else {
+      R = opt.pdlp ? e->run_pdlp(out) : e->run(out);
+      timeouts = e->stage_errors();
+    }
     const auto t = std::chrono::steady_clock::now();
     e.reset();
     R.teardown_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t).count();

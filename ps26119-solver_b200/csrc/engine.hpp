@@ -90,6 +90,11 @@ struct DeviceOutputs {
   double* primal_ray = nullptr;  // n (Unbounded)
 };
 
+// For the calling thread's later solves: run the r²HPDHG epochs in the device's group (one grouped
+// launch per half-step with every other grouped solve in flight) instead of on the solve's own
+// stream. Results are the same either way. The request loop's slot threads set it.
+void set_grouped_engine(bool on);
+
 // Runs r²HPDHG on the device model. `stream` is a cudaStream_t (nullptr = own stream).
 EngineResult run_engine(const DeviceModel& M, const EngineOptions& opt, const DeviceOutputs& out, void* stream);
 

@@ -76,6 +76,7 @@ int Server::take(long long id, bool wait, Solution& out, RequestTimes& times) {
 void Server::slot_main(int device) {
   (void)cudaSetDevice(device);
   (void)cudaGetLastError();
+  set_grouped_engine(opt_.grouped);  // this slot's solves run their epochs in the device's group
   std::unique_lock<std::mutex> lk(mu_);
   auto head_fits = [&] {
     if (queue_.empty()) return false;

@@ -28,6 +28,8 @@ struct ServerOptions {
   double hbm_budget_bytes = 0.0;  // device memory the running requests may hold; 0 = 80% of free memory
   double dry_run_seconds = 0.0;   // > 0: requests are admitted and timed but not solved; each holds
                                   // its slot and memory estimate this long (load tests of the policy)
+  bool grouped = true;            // the running requests' iteration kernels launched together (one
+                                  // grouped launch per half-step, engine.cu GroupScheduler)
 };
 
 struct RequestTimes {

@@ -381,12 +381,12 @@ inline int fed_tile_capacity(long long max_slab_nnz) {
 #define B200_FED_MIN_BLOCKS 5
 #endif
 
-template <class T, class Epi, int GB = kGatherBatch>
-__global__ void __launch_bounds__(kSlabRows, B200_FED_MIN_BLOCKS) k_slab_fed(int rows, const int* __restrict__ rp,
-                                                           const int* __restrict__ col,
-                                                           const T* __restrict__ val,
-                                                           const T* __restrict__ x, Epi epi,
-                                                           const int2* __restrict__ slab, int cap, unsigned* err) {
+// The body of k_slab_fed for slab `blk` (the block's slab: blockIdx.x in k_slab_fed, a slab of
+// one LP's matrix in the grouped kernel of several LPs).
+template <class T, class Epi, int GB>
+__device__ __forceinline__ void slab_fed_body(int blk, int rows, const int* __restrict__ rp, const int* __restrict__ col,
+                                              const T* __restrict__ val, const T* __restrict__ x, const Epi& epi,
+                                              const int2* __restrict__ slab, int cap, unsigned* err) {
   constexpr int V = Epi::kVecs;
   constexpr unsigned kLive = Epi::kLiveVecs;
   constexpr int kNumLive = __builtin_popcount(kLive);
@@ -403,7 +403,7 @@ __global__ void __launch_bounds__(kSlabRows, B200_FED_MIN_BLOCKS) k_slab_fed(int
   int* s_col = reinterpret_cast<int*>(fed_smem + L.col);
   T* s_val = reinterpret_cast<T*>(fed_smem + L.val);
   const int tid = static_cast<int>(threadIdx.x);
-  const int r0 = blockIdx.x * kSlabRows;
+  const int r0 = blk * kSlabRows;
   const int nr = min(kSlabRows, rows - r0);
   const unsigned vb = (static_cast<unsigned>(nr) * sizeof(T) + 15u) & ~15u;
   auto issue_tile = [&](int t0, int t1) {  // thread 0
@@ -425,7 +425,7 @@ __global__ void __launch_bounds__(kSlabRows, B200_FED_MIN_BLOCKS) k_slab_fed(int
 #pragma unroll
     for (int k = 0; k < V; ++k)
       if (!((kLive >> k) & 1u)) tma_load_1d(s_vec + k * kSlabRows, epi.vec(k) + r0, vb, &bar[0]);
-    const int2 kr = slab ? ld_keep(slab + blockIdx.x) : make_int2(__ldg(rp + r0), __ldg(rp + r0 + nr));
+    const int2 kr = slab ? ld_keep(slab + blk) : make_int2(__ldg(rp + r0), __ldg(rp + r0 + nr));
     *krange = kr;
     if (kr.x < kr.y) {
       issue_tile(kr.x, min(kr.x + cap, kr.y));
@@ -496,6 +496,48 @@ __global__ void __launch_bounds__(kSlabRows, B200_FED_MIN_BLOCKS) k_slab_fed(int
     epi_apply(epi, r0 + tid, s, pre, acc);
   }
   epi_flush(epi, acc);
+}
+
+template <class T, class Epi, int GB = kGatherBatch>
+__global__ void __launch_bounds__(kSlabRows, B200_FED_MIN_BLOCKS) k_slab_fed(int rows, const int* __restrict__ rp,
+                                                           const int* __restrict__ col,
+                                                           const T* __restrict__ val,
+                                                           const T* __restrict__ x, Epi epi,
+                                                           const int2* __restrict__ slab, int cap, unsigned* err) {
+  slab_fed_body<T, Epi, GB>(static_cast<int>(blockIdx.x), rows, rp, col, val, x, epi, slab, cap, err);
+}
+
+// ---------------------------------------------------------------------- several LPs in one launch
+// One LP's part of a grouped launch: its matrix, gathered vector, epilogue, and the first block of
+// the grid that works on it (its slabs are blocks first … first + ⌈rows/kSlabRows⌉ − 1).
+template <class T, class Epi>
+struct GroupPart {
+  int rows, cap, first;
+  const int *rp, *col;
+  const T *val, *x;
+  const int2* slab;
+  unsigned* err;
+  Epi epi;
+};
+// The iteration kernel of several LPs at once (the request loop's continuous batching): each block
+// finds its LP by a binary search over the parts' first blocks, then runs k_slab_fed's body on that
+// LP's slab with the epilogue at step `step` — the same arithmetic as the LP's own launch, so an
+// LP's iterates do not depend on which others share the launch. Shared memory is sized for the
+// largest tile capacity among the parts.
+template <class T, class Epi, int GB = kGatherBatch>
+__global__ void __launch_bounds__(kSlabRows, B200_FED_MIN_BLOCKS) k_group_fed(const GroupPart<T, Epi>* __restrict__ parts,
+                                                                             int nparts, int step) {
+  const int b = static_cast<int>(blockIdx.x);
+  int lo = 0, hi = nparts - 1;  // the last part whose first block is <= b
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (parts[mid].first <= b) lo = mid;
+    else hi = mid - 1;
+  }
+  const GroupPart<T, Epi>& g = parts[lo];
+  Epi epi = g.epi;
+  epi.step = step;
+  slab_fed_body<T, Epi, GB>(b - g.first, g.rows, g.rp, g.col, g.val, g.x, epi, g.slab, g.cap, g.err);
 }
 
 // Once per instantiation, outside any stream capture: prefer shared memory so that 8 CTAs of

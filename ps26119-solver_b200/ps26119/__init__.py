@@ -86,7 +86,8 @@ class _Scenario(ctypes.Structure):  # ps26119_scenario
 
 
 class _ServerOptions(ctypes.Structure):  # ps26119_server_options
-    _fields_ = [("slots", ctypes.c_int), ("hbm_budget_bytes", ctypes.c_double), ("dry_run_seconds", ctypes.c_double)]
+    _fields_ = [("slots", ctypes.c_int), ("hbm_budget_bytes", ctypes.c_double), ("dry_run_seconds", ctypes.c_double),
+                ("solo_engines", ctypes.c_int)]
 
 
 class _RequestTimes(ctypes.Structure):  # ps26119_request_times
@@ -341,9 +342,9 @@ class Server:
     ...     res, times = srv.result(rid)  # waits; times = (submitted, started, finished) seconds
     """
 
-    def __init__(self, slots=8, hbm_budget_bytes=0.0, dry_run_seconds=0.0):
+    def __init__(self, slots=8, hbm_budget_bytes=0.0, dry_run_seconds=0.0, grouped=True):
         self.L = load()
-        o = _ServerOptions(int(slots), float(hbm_budget_bytes), float(dry_run_seconds))
+        o = _ServerOptions(int(slots), float(hbm_budget_bytes), float(dry_run_seconds), 0 if grouped else 1)
         self.h = self.L.ps26119_server_create(ctypes.byref(o))
         if not self.h:
             raise ValueError("ps26119_server_create refused the options")

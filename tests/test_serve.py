@@ -117,16 +117,44 @@ def test_concurrent_submitters():
 
 
 @pytest.mark.gpu
-def test_served_results_equal_single_solves():
+@pytest.mark.parametrize("grouped", [True, False], ids=["grouped", "solo"])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_served_results_equal_single_solves(grouped, precision):
+    """Each request's result is the same alone and in the mix, bit for bit: with the grouped
+    kernels (the running requests' iteration kernels launched together, requests joining and
+    leaving the group at epoch boundaries) and with each request's own kernels; in fp64 and in
+    mixed precision (a request promotes to fp64 while its neighbours still run in fp32)."""
     lps = [_lp(m, seed) for m, seed in ((300, 1), (1200, 2), (50, 3), (2500, 4), (800, 5), (150, 6))]
-    with ps26119.Server(slots=4) as srv:
-        ids = [srv.submit(lp, precision="fp64") for lp in lps]
+    with ps26119.Server(slots=4, grouped=grouped) as srv:
+        ids = [srv.submit(lp, precision=precision) for lp in lps]
         served = [srv.result(i) for i in ids]
     for lp, (res, (sub, st, fin)) in zip(lps, served):
         alone = ps26119.solve_lp(lp.c, (lp.col_start, lp.row_index, lp.value), lp.row_lower, lp.row_upper,
-                                 lp.col_lower, lp.col_upper, sense=lp.sense, offset=lp.offset, algorithm="r2hpdhg")
+                                 lp.col_lower, lp.col_upper, sense=lp.sense, offset=lp.offset, algorithm="r2hpdhg",
+                                 precision=precision)
         assert res.status == alone.status == ps26119.OPTIMAL and res.check == alone.check == "PASS"
         assert res.iterations == alone.iterations and res.objective == alone.objective
         assert np.array_equal(res.x, alone.x) and np.array_equal(res.y, alone.y)
         assert res.certified_bound == alone.certified_bound
         assert sub <= st < fin
+
+
+@pytest.mark.gpu
+def test_grouped_requests_retire_and_refill():
+    """Continuous batching: with 3 slots and 9 requests of very different lengths, short requests
+    finish and leave the group while long ones keep running, and queued requests take the freed
+    slots and join the running group. Every request ends Optimal with the result of its solo
+    solve; some request starts before another that was admitted earlier has finished."""
+    lps = [_lp(m, seed) for m, seed in ((2000, 11), (40, 12), (60, 13), (1500, 14), (30, 15), (50, 16), (900, 17),
+                                        (20, 18), (70, 19))]
+    with ps26119.Server(slots=3, grouped=True) as srv:
+        ids = [srv.submit(lp) for lp in lps]
+        served = [srv.result(i) for i in ids]
+    spans = [(t[1], t[2]) for _, t in served]
+    # a refill: a later request started while an earlier, longer one was still running
+    assert any(spans[j][0] < spans[i][1] and spans[j][0] > spans[i][0] for i in range(len(lps)) for j in range(i + 1, len(lps)))
+    for lp, (res, _) in zip(lps, served):
+        alone = ps26119.solve_lp(lp.c, (lp.col_start, lp.row_index, lp.value), lp.row_lower, lp.row_upper,
+                                 lp.col_lower, lp.col_upper, sense=lp.sense, offset=lp.offset, algorithm="r2hpdhg")
+        assert res.status == ps26119.OPTIMAL and res.iterations == alone.iterations
+        assert np.array_equal(res.x, alone.x) and np.array_equal(res.y, alone.y)
