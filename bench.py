@@ -132,6 +132,7 @@ def run_serve(args, rank, world, local):
     with clock_sampler(local) as clocks:
         for _ in range(args.steps):
             barrier(world)
+            t_create = time.perf_counter()  # the server's clock (request times) starts here
             with ps26119.Server(slots=slots, grouped=not args.serve_solo) as srv:
                 t0 = time.perf_counter()
                 ids = []
@@ -147,7 +148,7 @@ def run_serve(args, rank, world, local):
             sub = np.array([t[0] for _, t in out])
             fin = np.array([t[2] for _, t in out])
             start = np.array([t[1] for _, t in out])
-            span = max_over_ranks(float(fin.max() - t0) if len(out) else 0.0, world)
+            span = max_over_ranks(float(fin.max() - (t0 - t_create)) if len(out) else 0.0, world)
             got = shard.gather({k: (float(f - b), float(f - a), r.iterations)
                                 for k, (r, _), b, a, f in zip(mine, out, sub, start, fin)}, world)
             steps.append((span, np.array([got[k][0] for k in range(N)]), [got[k][2] for k in range(N)],

@@ -144,17 +144,12 @@ class Engine {
   bool start(const DeviceOutputs& out);
   void begin_epoch();
   void launch_epoch();
-  void launch_r0();
+  void launch_r0(cudaStream_t on);
   void launch_check();
   bool end_epoch();
   const EngineResult& result() const { return R_; }
   int check_every() const { return o_.check_every; }
-  // Moves the engine to another stream once its setup has finished (start() returned false):
-  // waits for the work enqueued so far, then every later launch goes to `s`.
-  void rebind_stream(cudaStream_t s) {
-    B200_CHECK(cudaStreamSynchronize(st_));
-    st_ = s;
-  }
+  cudaStream_t stream() const { return st_; }
   bool mixed_now() const { return mixed_now_; }
   // the operands of this engine's iteration kernels at step s of the current epoch
   template <class T> EpiPrimal<T> primal_epi(int s);
@@ -925,10 +920,13 @@ void Engine::launch_epoch() {
 
 // The r⁰ residual after the first step of an epoch that starts a Halpern cycle (the section the
 // epoch graph holds), for epochs whose steps the group scheduler launches.
-void Engine::launch_r0() {
+void Engine::launch_r0(cudaStream_t on) {
   if (!L_.fresh) return;
+  const cudaStream_t own = st_;
+  st_ = on;  // launched on the group's stream, between the group's step 0 and step 1
   if (mixed_now_) launch_residual<float>(false, nullptr, plan_r0_);
   else launch_residual<double>(false, nullptr, plan_r0_);
+  st_ = own;
 }
 
 void Engine::launch_check() {
@@ -1372,6 +1370,7 @@ class GroupScheduler {
     bool done = false;
     unsigned timeouts = 0;
     std::exception_ptr error;
+    cudaEvent_t ready = nullptr;  // the engine's stream has its step scalars (and restart) in place
   };
   static GroupScheduler& for_current_device() {
     static std::mutex mu;
@@ -1396,6 +1395,7 @@ class GroupScheduler {
  private:
   explicit GroupScheduler(int dev) : dev_(dev) {
     B200_CHECK(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
+    B200_CHECK(cudaEventCreateWithFlags(&steps_done_, cudaEventDisableTiming));
     thread_ = std::thread([this] { loop(); });
     thread_.detach();
   }
@@ -1449,10 +1449,17 @@ class GroupScheduler {
     cfg.numAttrs = (B200_PDL && pdl) ? 1 : 0;
     B200_CHECK(cudaLaunchKernelEx(&cfg, k_group_fed<T, Epi>, parts.get(), nparts, step));
   }
+  // One epoch of every active solve: each solve's step scalars on its own stream; the grouped
+  // iteration kernels on the group's stream once every solve's stream is ready; each solve's
+  // residual section (when its epoch starts a Halpern cycle) on the group's stream after step 0;
+  // then every solve's check graph on its own stream, so the checks of different solves overlap.
   void epoch(std::vector<Job*>& active) {
     tf_.clear(), td_.clear();
     for (Job* j : active) {
       j->e->begin_epoch();
+      if (!j->ready) B200_CHECK(cudaEventCreateWithFlags(&j->ready, cudaEventDisableTiming));
+      B200_CHECK(cudaEventRecord(j->ready, j->e->stream()));
+      B200_CHECK(cudaStreamWaitEvent(st_, j->ready, 0));
       if (j->e->mixed_now()) add(tf_, *j->e);
       else add(td_, *j->e);
     }
@@ -1466,10 +1473,14 @@ class GroupScheduler {
       launch(td_.dd, nd, td_.blocks_d, td_.cap_d, s, nf == 0);
       launch(tf_.dd, nf, tf_.blocks_d, tf_.cap_d, s, false);
       if (s == 0)
-        for (Job* j : active) j->e->launch_r0();
+        for (Job* j : active) j->e->launch_r0(st_);
     }
-    for (Job* j : active) j->e->launch_check();
-    B200_CHECK(cudaStreamSynchronize(st_));
+    B200_CHECK(cudaEventRecord(steps_done_, st_));
+    for (Job* j : active) {
+      B200_CHECK(cudaStreamWaitEvent(j->e->stream(), steps_done_, 0));
+      j->e->launch_check();
+    }
+    for (Job* j : active) B200_CHECK(cudaStreamSynchronize(j->e->stream()));
   }
   void loop() {
     (void)cudaSetDevice(dev_);
@@ -1502,13 +1513,17 @@ class GroupScheduler {
       }
       if (!finished.empty()) {
         std::lock_guard<std::mutex> lk(mu_);
-        for (Job* j : finished) j->done = true;
+        for (Job* j : finished) {
+          if (j->ready) cudaEventDestroy(j->ready), j->ready = nullptr;
+          j->done = true;
+        }
         done_cv_.notify_all();
       }
     }
   }
   int dev_ = 0;
   cudaStream_t st_ = nullptr;
+  cudaEvent_t steps_done_ = nullptr;
   std::thread thread_;
   std::mutex mu_;
   std::condition_variable cv_, done_cv_;
@@ -1554,7 +1569,6 @@ EngineResult run_engine(const DeviceModel& M, const EngineOptions& opt, const De
         timeouts = e->stage_errors();
       } else {
         GroupScheduler& g = GroupScheduler::for_current_device();
-        e->rebind_stream(g.stream());
         GroupScheduler::Job job;
         job.e = e.get();
         g.run(job);
