@@ -1562,7 +1562,14 @@ EngineResult run_engine(const DeviceModel& M, const EngineOptions& opt, const De
   unsigned timeouts = 0;
   {
     auto e = std::make_unique<Engine>(M, opt, st);
-    if (t_grouped && !opt.pdlp && opt.check_every == 64) {
+    // Large LPs keep their own kernels: they fill the device alone, and in lockstep with a
+    // group their epochs would wait for everyone's checks. Small ones (launch-bound alone) join
+    // the group. The limit is PS26119_GROUP_MAX_NNZ nonzeros (default 100,000).
+    static const long long group_max_nnz = [] {
+      const char* e = std::getenv("PS26119_GROUP_MAX_NNZ");
+      return e && *e ? std::atoll(e) : 100000LL;
+    }();
+    if (t_grouped && !opt.pdlp && opt.check_every == 64 && M.nnz <= group_max_nnz) {
       // setup here, on this caller's stream; the epochs in the device's group
       if (e->start(out)) {
         R = e->result();
