@@ -601,7 +601,7 @@ def run_ours(args, rank, world, local):
         achieved_g = 2 * lp.nnz / (iter_ms * 1e-3)
         line["roofline"]["gather"] = {"achieved_gathers_per_s": achieved_g, "peak_gathers_per_s": g["gathers_per_s"],
                                       "frac": achieved_g / g["gathers_per_s"],
-                                      "peak_source": "measured live by lib/gather_rate (random 8-byte gathers "
+                                      "peak_source": "measured live by bench_gather_rate (random 8-byte gathers "
                                                      f"of a {lp.num_cols:,}-element vector resident in L2)"}
     if not args.no_e2e:
         line["e2e"] = run_e2e(args, lp, world, limit)
@@ -674,9 +674,9 @@ def time_to_tol_records(args):
 
 
 def gather_ceiling(m, lp):
-    """Runs lib/gather_rate (built with the library) for this matrix's shape: random gathers from
+    """Runs bench_gather_rate (built by __graft_entry__.build()) for this matrix's shape: random gathers from
     an n-element vector, nnz of them. None when the program is absent or fails."""
-    exe = os.path.join(ROOT, "ps26119-solver_b200", "lib", "gather_rate")
+    exe = os.path.join(ROOT, "bench_gather_rate")
     if m is None or not os.path.exists(exe):
         return None
     try:

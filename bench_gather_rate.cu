@@ -1,8 +1,8 @@
-// gather_rate — measures the device's rate of random 8-byte gathers from a vector that stays in
+// bench_gather_rate — bench.py's probe (not part of the library): the device's rate of random 8-byte gathers from a vector that stays in
 // L2, the second ceiling of the iteration kernels besides HBM bandwidth (each nonzero of Ã and
 // Ãᵀ gathers one element of x̄ or y: 2·nnz random gathers per iteration).
 //
-//   gather_rate [n] [count]     (defaults: n = 1,500,000 doubles, count = 6,000,000 gathers)
+//   bench_gather_rate [n] [count]     (defaults: n = 1,500,000 doubles, count = 6,000,000 gathers)
 //
 // Prints one JSON line: {"gathers_per_s": G, "n": n, "count": count, "us": T}. The indices are
 // drawn on the host in [0, n), so every access is in bounds; the gathered vector is brought into

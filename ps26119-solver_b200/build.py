@@ -21,7 +21,6 @@ BUILD = os.path.join(HERE, "_build")
 LIB_DIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIB_DIR, "libps26119.so")
 CLI = os.path.join(LIB_DIR, "ps26119")  # the command-line tool
-GATHER_RATE = os.path.join(LIB_DIR, "gather_rate")  # the random-gather ceiling bench.py reports
 CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA, "bin", "nvcc")
 
@@ -84,9 +83,6 @@ def build(force: bool = False, jobs: int = 4, verbose: bool = False) -> str:
         _compile(["g++"] + CXX_FLAGS + ["-c", cli_src, "-o", cli_obj])
     if not os.path.exists(CLI) or any(os.path.getmtime(o) > os.path.getmtime(CLI) for o in objs + [cli_obj]):
         _compile([NVCC] + ARCH + ["-o", CLI, cli_obj] + objs + ["-lpthread"])
-    gr_src = os.path.join(CSRC, "gather_rate.cu")
-    if force or _stale(GATHER_RATE, gr_src, []):
-        _compile([NVCC] + NVCC_FLAGS + ["-o", GATHER_RATE, gr_src])
     return LIB
 
 
