@@ -1,7 +1,7 @@
 """Benchmark of the B200 r²HPDHG engine on the 1M x 1.5M random LP and the other workloads below.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload random1m|random10k|staircase8760|batch720x64|serve48]
+                    [--workload random1m|random10k|staircase8760|batch720x64|batch720x64f|batch10kx64f|serve48]
                     [--precision fp64|mixed] [--reductions exact|fast]
                     [--iterations L | --full]
 
@@ -56,6 +56,9 @@ WORKLOADS = {
     "batch720x64f": {"desc": "64 feasible scenarios of the staircase LP T=720 (35,280 x 43,200, 126,024 nnz): "
                              "interior point, slacks and c x lognormal(0, 0.1), seed 1", "kind": "batch", "T": 720,
                      "K": 64, "feasible": True},
+    "batch10kx64f": {"desc": "64 feasible scenarios of the random equality LP m=10,000 n=15,000 (60,000 nnz): "
+                             "x0, c x lognormal(0, 0.1), b = A x', seed 1", "kind": "batch", "base": "random",
+                     "m": 10_000, "K": 64, "feasible": True},
     "serve48": {"desc": "48 LP requests from the random-LP generator, m log-uniform in [1e3, 2e4] (n = 1.5m, "
                         "6 nnz/row), Poisson arrivals, each solved to 1e-8 (a bounded sample of the "
                         "2,000-request stream with m up to 2e5), seed 1", "kind": "serve", "N": 48,
@@ -72,7 +75,8 @@ TIME_TO_TOL = [("random10k", "fp64"), ("random10k", "mixed"), ("staircase8760", 
 def make_lp(name):
     from ps26119 import generators as g
     w = WORKLOADS[name]
-    return g.random_lp(w["m"], seed=1) if w["kind"] == "random" else g.staircase_lp(w["T"], seed=1)
+    random = w["kind"] == "random" or w.get("base") == "random"
+    return g.random_lp(w["m"], seed=1) if random else g.staircase_lp(w["T"], seed=1)
 
 
 def make_scenarios(name, lp):
@@ -210,21 +214,32 @@ def hbm_peak():
     return (peak, "measured") if peak else (6650.0, "fallback")
 
 
-def roofline_batch(bpi, its, args, sec, results):
+def roofline_batch(lp, args, sec, results):
     """Kernel roofline of the batch's SpMM kernels (CUDA events over their launches in every
-    epoch) against the measured HBM copy peak, and the whole-step figure beside it."""
+    epoch) against the measured HBM copy peak, and the whole-step figure beside it. Finished
+    scenarios leave the lockstep batch (their slots are compacted away), so a lockstep iteration
+    moves Ã and Ãᵀ once plus the vectors of the slots still running: over the last step,
+    its_max·(2·nnz·(s_v + 4) + 4(m + n)) + Σ_k its_k·s_w·(9n + 7m) bytes, its_k being scenario
+    k's iterations. Mixed precision is counted at 4-byte values and vectors throughout (its
+    final fp64 stretch moves more), so its figure is a lower bound."""
     peak, peak_src = hbm_peak()
-    st = results[-1][1]
+    res, st = results[-1]
+    m, n, nnz = lp.num_rows, lp.num_cols, lp.nnz
+    s_v = s_w = 4 if args.precision == "mixed" else 8
+    its = [r.iterations for r in res]
+    total = max(its) * (2 * nnz * (s_v + 4) + 4 * (m + n)) + sum(its) * s_w * (9 * n + 7 * m)
+    bpi = total / max(1, max(its))
     kern_ms = st["spmv_kernel_ms"]
     pairs = max(1, st["spmv_kernel_launches"] // 2)
     out = {"bound": "hbm", "unit": "GB/s", "peak": peak, "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)",
            "algorithmic_bytes": bpi, "traffic": None,
-           "unit_of_work": "one lockstep iteration of all slots: the two fused SpMM+update kernels",
-           "achieved_whole_step": bpi * its * args.steps / sec / 1e9,
-           "note": "achieved: algorithmic bytes / live kernel time; achieved_whole_step: / step wall time"}
+           "unit_of_work": "one lockstep iteration of the running slots: the two fused SpMM+update kernels "
+                           "(algorithmic_bytes: the mean over the last step's lockstep iterations)",
+           "achieved_whole_step": total * len(results) / sec / 1e9 if len(results) == args.steps else None,
+           "note": "achieved: algorithmic bytes / live kernel time, last step; achieved_whole_step: every step's "
+                   "bytes / step wall time"}
     if kern_ms > 0:
-        us = 1e3 * kern_ms / pairs
-        out.update({"achieved": bpi / (us * 1e-6) / 1e9, "kernel_us_per_iteration": us})
+        out.update({"achieved": total / (kern_ms * 1e-3) / 1e9, "kernel_us_per_iteration": 1e3 * kern_ms / pairs})
         out["frac"] = out["achieved"] / peak
     return out
 
@@ -285,7 +300,7 @@ def run_batch(args, rank, world, local):
                    "tolerance": 1e-8, "iteration_cap": limit or None, "entry": "ps26119_solve_batch (host arrays)",
                    "iterations_per_step": its, "parallelism": f"scenarios sharded over {world} GPUs" if world > 1 else "1 GPU",
                    "l2": f"inputs larger than L2: {bpi / 1e6:.0f} MB streamed per lockstep iteration"},
-        "roofline": roofline_batch(bpi, its, args, sec, results),
+        "roofline": roofline_batch(lp, args, sec, results),
         "gpu_launches": int(sum(s["kernel_launches"] for _, s in results)),
         "clocks": clocks.summary(),
         "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": nnz * 12 + (n + 1) * 4 + K * 8 * (3 * n + 2 * m),
@@ -594,7 +609,8 @@ def run_ours(args, rank, world, local):
         "solve": {"status": r.status_name, "iterations": r.iterations, "objective": r.objective,
                   "primal_residual": r.primal_residual, "dual_residual": r.dual_residual, "gap": r.gap,
                   "check": r.check, "setup_s": st["setup_seconds"], "loop_s": st["loop_seconds"],
-                  "finish_s": st["finish_seconds"], "checks": st["checks"], "restarts": st["restarts"]},
+                  "finish_s": st["finish_seconds"], "checks": st["checks"], "restarts": st["restarts"],
+                  "slab_variants": {"primal": st["slab_variant_primal"], "dual": st["slab_variant_dual"]}},
     }
     g = gather_ceiling(lp.num_rows if args.workload.startswith("random") else None, lp)
     if g:  # the second ceiling: 2·nnz random gathers of x̄ / y per iteration

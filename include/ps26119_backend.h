@@ -96,12 +96,14 @@ PS26119_API int ps26119_backend_norm2_estimate(ps26119_backend* b, double* out);
 
 /* fp64 dot product Σ a_i·b_i of two DEVICE vectors of length n, written to the device double
  * *out on `stream` (a cudaStream_t; NULL = the legacy default stream). No counterpart in the
- * reference: it is for callers that may not allocate device memory (code inside a CUDA graph
- * capture, callers whose device memory belongs to their own pool). It calls no cudaMalloc or
- * cudaFree; its scratch is one fixed array in this library's device code, at most n = 2,097,152
- * elements (16 MiB); larger n is rejected with PS26119_INVALID_ARGUMENT. The first call on a
- * device looks up that array's address (make it before any stream capture). All calls on a
- * device share the array, so calls that overlap on the GPU race: serialise them on one stream.
+ * reference: it is for callers that cannot allocate device memory when they need the sum (a
+ * caller whose device memory all belongs to its own pool, a loop that may not wait on the
+ * allocator). It calls no cudaMalloc or cudaFree; its scratch is one fixed array in this
+ * library's device code, at most n = 2,097,152 elements (16 MiB), held by every device that
+ * loads the library until exit; larger n is rejected with PS26119_INVALID_ARGUMENT. The first
+ * call on a device looks up that array's address (make it before any stream capture) and keeps
+ * it: not for use after cudaDeviceReset. All calls on a device share the array, so calls that
+ * overlap on the GPU race: serialise them on one stream.
  * exact = 1 sums in the reference's la::parallel_sum order and equals ps26119_backend_dot of an
  * exact backend bit for bit; exact = 0 equals the fast-mode ps26119_backend_dot.
  * Returns 0, or a PS26119_* status with the reason in ps26119_backend_last_error(). */

@@ -1,22 +1,24 @@
 // noalloc.cu — ps26119_dot_noalloc: the fp64 dot product of two device vectors for callers
 // that must not allocate device memory.
 //
-// Who needs it: code that runs where cudaMalloc is not allowed or not wanted — inside a region
-// being captured into a CUDA graph (an allocation there fails the capture), inside a caller
-// whose device memory is owned by its own pool and budgeted to the byte, or in a real-time
-// loop that may not take the allocator's locks. The backend's Backend::dot
-// (ps26119_backend_dot) materialises its per-element terms and partial sums in buffers it
-// allocates; this entry point does the same arithmetic with that scratch in one file-scope
-// device array instead, so a call allocates nothing.
+// Who needs it: callers that cannot call cudaMalloc at the point where they need the dot
+// product — a caller whose device memory is all handed out by its own pool and budgeted to the
+// byte (an allocation behind its back can fail or push it out of memory), or a loop with a
+// latency bound that may not wait on the allocator's locks and the driver calls behind them.
+// The backend's Backend::dot (ps26119_backend_dot) materialises its per-element terms and
+// partial sums in buffers it allocates; this entry point does the same arithmetic with that
+// scratch in one file-scope device array instead, so a call allocates nothing.
 //
 // The scratch: g_noalloc_scratch, kNoAllocMaxN + 256 doubles (16 MiB + 2 KiB) per device,
-// reserved when the CUDA runtime loads this library's device code. Its address is taken once
-// per device (cudaGetSymbolAddress, with that device current) on the first call made while the
-// device is current, so that first call should come before any stream capture. Every call on
-// a device shares the one array: calls whose kernels overlap on the GPU (two streams, or two
-// host threads with different streams) race on it and may return wrong sums; serialise them on
-// one stream. Nothing in the scratch needs to start at zero: every term and partial is written
-// before it is read.
+// reserved when the CUDA runtime loads this library's device code and held until the process
+// exits. Its address is taken once per device (cudaGetSymbolAddress, with that device current)
+// on the first call made while the device is current, so that first call should come before any
+// stream capture. The address is kept for the life of the process: do not call this entry point
+// again on a device after cudaDeviceReset (the reset unloads the array the address points to).
+// Every call on a device shares the one array: calls whose kernels overlap on the GPU (two
+// streams, or two host threads with different streams) race on it and may return wrong sums;
+// serialise them on one stream. Nothing in the scratch needs to start at zero: every term and
+// partial is written before it is read.
 //
 // Results: exact = 1 sums in la::parallel_sum's order (64 contiguous chunks, each summed in
 // order, then the chunk sums in order) and equals ps26119_backend_dot of an exact-mode backend

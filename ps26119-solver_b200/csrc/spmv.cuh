@@ -119,6 +119,11 @@ __device__ __forceinline__ void tma_load_1d(void* dst, const void* src, unsigned
                : "memory");
 #endif
 }
+// A bulk prefetch of [src, src + bytes) into L2 (no shared memory, no completion to wait for);
+// src 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void prefetch_l2(const void* src, unsigned bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
 __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
   unsigned ok;
   asm volatile(
@@ -235,6 +240,24 @@ __device__ __forceinline__ void epi_apply(const E& e, int i, double s, const P& 
 template <class E, class A>
 __device__ __forceinline__ void epi_flush(const E& e, const A& acc) {
   if constexpr (!std::is_same<A, NoAcc>::value) e.flush(acc);
+}
+
+// gather() without the conversion to double.
+template <class T>
+__device__ __forceinline__ T gather_t(const T* __restrict__ x, int i) {
+#if B200_GATHER_NA
+  if constexpr (sizeof(T) == 8) {
+    double v;
+    asm volatile("ld.global.nc.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(x + i));
+    return v;
+  } else {
+    float v;
+    asm volatile("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(x + i));
+    return v;
+  }
+#else
+  return x[i];
+#endif
 }
 
 constexpr int kGatherBatch = B200_GATHER_BATCH;  // independent x-gathers issued per round trip
@@ -381,12 +404,31 @@ inline int fed_tile_capacity(long long max_slab_nnz) {
 #define B200_FED_MIN_BLOCKS 5
 #endif
 
+// The fp64 product of staged nonzero k, written over the staged tile once its col and val are
+// read: in the val slot for fp64 values; for fp32 values its high word in the col slot and its low
+// word in the val slot (k's 8 bytes of tile), so the tile needs no extra room.
+template <class T>
+__device__ __forceinline__ void put_product(int* s_col, T* s_val, int ic, int iv, double p) {
+  if constexpr (sizeof(T) == 8) {
+    s_val[iv] = p;
+  } else {
+    s_col[ic] = __double2hiint(p);
+    reinterpret_cast<int*>(s_val)[iv] = __double2loint(p);
+  }
+}
+template <class T>
+__device__ __forceinline__ double get_product(const int* s_col, const T* s_val, int ic, int iv) {
+  if constexpr (sizeof(T) == 8) return static_cast<double>(s_val[iv]);
+  else return __hiloint2double(s_col[ic], reinterpret_cast<const int*>(s_val)[iv]);
+}
+
 // The body of k_slab_fed for slab `blk` (the block's slab: blockIdx.x in k_slab_fed, a slab of
 // one LP's matrix in the grouped kernel of several LPs).
 template <class T, class Epi, int GB>
 __device__ __forceinline__ void slab_fed_body(int blk, int rows, const int* __restrict__ rp, const int* __restrict__ col,
                                               const T* __restrict__ val, const T* __restrict__ x, const Epi& epi,
-                                              const int2* __restrict__ slab, int cap, unsigned* err) {
+                                              const int2* __restrict__ slab, int cap, unsigned* err,
+                                              int ahead = 0) {
   constexpr int V = Epi::kVecs;
   constexpr unsigned kLive = Epi::kLiveVecs;
   constexpr int kNumLive = __builtin_popcount(kLive);
@@ -431,6 +473,26 @@ __device__ __forceinline__ void slab_fed_body(int blk, int rows, const int* __re
       issue_tile(kr.x, min(kr.x + cap, kr.y));
       tile_pending = true;
     }
+    // Wave-ahead prefetch: bring the operands of slab blk + ahead (the block that takes this
+    // block's place about one wave of resident blocks later) from DRAM into L2 now, with the same
+    // 16-byte widened ranges its own copies will request; its copies then complete from L2. A
+    // prefetch only warms the cache: the values that block reads are the ones in memory then.
+    const int pb = blk + ahead;
+    if (ahead > 0 && pb < (rows + kSlabRows - 1) / kSlabRows) {
+      const int pr0 = pb * kSlabRows, pnr = min(kSlabRows, rows - pr0);
+      prefetch_l2(rp + pr0, (static_cast<unsigned>(pnr + 1) * 4u + 15u) & ~15u);
+      const unsigned pvb = (static_cast<unsigned>(pnr) * sizeof(T) + 15u) & ~15u;
+#pragma unroll
+      for (int k = 0; k < V; ++k) prefetch_l2(epi.vec(k) + pr0, pvb);
+      const int2 pk = slab ? ld_keep(slab + pb) : make_int2(__ldg(rp + pr0), __ldg(rp + pr0 + pnr));
+      if (pk.x < pk.y) {
+        const int t1 = min(pk.x + cap, pk.y);
+        const int c0 = pk.x & ~3, v0 = pk.x & ~(kValAlign - 1);
+        const int c1 = (t1 + 3) & ~3, v1 = (t1 + kValAlign - 1) & ~(kValAlign - 1);
+        prefetch_l2(col + c0, static_cast<unsigned>(c1 - c0) * 4u);
+        prefetch_l2(val + v0, static_cast<unsigned>(v1 - v0) * sizeof(T));
+      }
+    }
   }
   pdl_wait();  // from here on the previous kernels' outputs are complete and visible
   int ok = 1;
@@ -472,14 +534,38 @@ __device__ __forceinline__ void slab_fed_body(int blk, int rows, const int* __re
     }
     const int c0 = t0 & ~3, v0 = t0 & ~(kValAlign - 1);
     const int a = max(beg, t0), b = min(end, t1);
-    for (int k = a; k < b; k += GB) {  // GB gathers in flight, then their products added in CSR order
-      double p[GB];
+    if constexpr (GB == 0) {
+      // Spread: the tile's products are formed by the whole block, nonzero t0 + tid + j·kSlabRows
+      // by thread tid, every gather of a thread issued before the first is used, and written back
+      // over the tile; then each thread adds its row's products in CSR order. A thread issues
+      // about nnz/rows gathers whatever its row's length, all in one round trip.
+      constexpr int kSpread = (kSlabTile + kSlabRows - 1) / kSlabRows;  // cap <= kSlabTile
+      const int base = t0 + tid;
+      int cl[kSpread];
 #pragma unroll
-      for (int q = 0; q < GB; ++q)
-        p[q] = (k + q < b) ? static_cast<double>(s_val[k + q - v0]) * gather(x, s_col[k + q - c0]) : 0.0;
+      for (int q = 0; q < kSpread; ++q) cl[q] = (base + q * kSlabRows < t1) ? s_col[base + q * kSlabRows - c0] : 0;
+      T g[kSpread];  // x[col] in T: the fp64 product below is the same (float -> double is exact)
 #pragma unroll
-      for (int q = 0; q < GB; ++q)
-        if (k + q < b) s += p[q];  // in CSR order
+      for (int q = 0; q < kSpread; ++q) g[q] = (base + q * kSlabRows < t1) ? gather_t(x, cl[q]) : T(0);
+#pragma unroll
+      for (int q = 0; q < kSpread; ++q) {
+        const int k = base + q * kSlabRows;
+        if (k < t1)
+          put_product<T>(s_col, s_val, k - c0, k - v0,
+                         static_cast<double>(s_val[k - v0]) * static_cast<double>(g[q]));
+      }
+      __syncthreads();
+      for (int k = a; k < b; ++k) s += get_product<T>(s_col, s_val, k - c0, k - v0);  // in CSR order
+    } else {
+      for (int k = a; k < b; k += GB) {  // GB gathers in flight, then their products added in CSR order
+        double p[GB];
+#pragma unroll
+        for (int q = 0; q < GB; ++q)
+          p[q] = (k + q < b) ? static_cast<double>(s_val[k + q - v0]) * gather(x, s_col[k + q - c0]) : 0.0;
+#pragma unroll
+        for (int q = 0; q < GB; ++q)
+          if (k + q < b) s += p[q];  // in CSR order
+      }
     }
   }
   if (!staged) {  // never expected: record, wait (bounded) for copies still in flight, report NaN
@@ -503,8 +589,9 @@ __global__ void __launch_bounds__(kSlabRows, B200_FED_MIN_BLOCKS) k_slab_fed(int
                                                            const int* __restrict__ col,
                                                            const T* __restrict__ val,
                                                            const T* __restrict__ x, Epi epi,
-                                                           const int2* __restrict__ slab, int cap, unsigned* err) {
-  slab_fed_body<T, Epi, GB>(static_cast<int>(blockIdx.x), rows, rp, col, val, x, epi, slab, cap, err);
+                                                           const int2* __restrict__ slab, int cap, unsigned* err,
+                                                           int ahead) {
+  slab_fed_body<T, Epi, GB>(static_cast<int>(blockIdx.x), rows, rp, col, val, x, epi, slab, cap, err, ahead);
 }
 
 // ---------------------------------------------------------------------- several LPs in one launch
@@ -584,16 +671,30 @@ inline void launch_slab_tma(int rows, const int* rp, const int* col, const T* va
 #define B200_PDL 1
 #endif
 
-// Launch variants of k_slab_fed, chosen per matrix by the autotuner (tune.cuh): `gather` = GB
-// (2, 4 or 8 gathers in flight per thread), `ctas` = resident CTAs per SM (0: as many as the
-// registers and shared memory allow; k: dynamic shared memory padded so that no more than k
-// fit). Every variant computes
-// the same sums in the same order: the results do not depend on the choice.
+// Launch variants of k_slab_fed, chosen per matrix by the autotuner (tune.hpp): `gather` = GB
+// (2, 4 or 8 gathers in flight per thread, each thread walking its own row; 0: the spread form,
+// where the block forms the tile's products together, an equal share per thread, before each
+// thread adds its row's), `ctas` = resident CTAs per SM (0: as many as the registers and shared
+// memory allow; k: dynamic shared memory padded so that no more than k fit), `ahead` = the
+// wave-ahead L2 prefetch distance in waves of resident blocks (0: none). Every variant computes
+// the same products and adds them in the same order: the results do not depend on the choice.
 struct SlabVariant {
-  int gather, ctas;
+  int gather, ctas, ahead;
 };
-constexpr SlabVariant kSlabVariants[] = {{4, 0}, {2, 0}, {8, 0}, {4, 5}, {4, 4}};
+constexpr SlabVariant kSlabVariants[] = {{4, 0, 0}, {2, 0, 0}, {8, 0, 0}, {4, 5, 0}, {4, 4, 0}, {0, 0, 0}, {4, 0, 1}};
 constexpr int kNumSlabVariants = static_cast<int>(sizeof(kSlabVariants) / sizeof(kSlabVariants[0]));
+
+// Streaming multiprocessors of the current device (read once; 148 on a B200).
+inline int device_sm_count() {
+  static const int sms = [] {
+    int dev = 0, v = 0;
+    (void)cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) v = 148;
+    (void)cudaGetLastError();
+    return v;
+  }();
+  return sms;
+}
 
 // Dynamic shared memory of a k_slab_fed launch that needs `bytes` under variant `v`.
 inline unsigned fed_smem_bytes(unsigned bytes, const SlabVariant& v) {
@@ -619,7 +720,8 @@ inline unsigned fed_smem_bytes(unsigned bytes, const SlabVariant& v) {
 
 template <class T, class Epi, int GB>
 inline void launch_fed_gb(int grid, unsigned smem, cudaStream_t st, bool pdl, int rows, const int* rp, const int* col,
-                          const T* val, const T* x, const Epi& epi, const int2* slab, int cap, unsigned* err) {
+                          const T* val, const T* x, const Epi& epi, const int2* slab, int cap, unsigned* err,
+                          int ahead) {
   if (smem > 48u * 1024u) {  // once per instantiation, outside any capture: allow the padded size
     static const bool opt = [] {
       (void)cudaFuncSetAttribute(k_slab_fed<T, Epi, GB>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
@@ -639,10 +741,10 @@ inline void launch_fed_gb(int grid, unsigned smem, cudaStream_t st, bool pdl, in
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    B200_CHECK(cudaLaunchKernelEx(&cfg, k_slab_fed<T, Epi, GB>, rows, rp, col, val, x, epi, slab, cap, err));
+    B200_CHECK(cudaLaunchKernelEx(&cfg, k_slab_fed<T, Epi, GB>, rows, rp, col, val, x, epi, slab, cap, err, ahead));
     return;
   }
-  k_slab_fed<T, Epi, GB><<<grid, kSlabRows, smem, st>>>(rows, rp, col, val, x, epi, slab, cap, err);
+  k_slab_fed<T, Epi, GB><<<grid, kSlabRows, smem, st>>>(rows, rp, col, val, x, epi, slab, cap, err, ahead);
   B200_LAUNCH_CHECK();
 }
 
@@ -666,10 +768,13 @@ inline void launch_slab_fed(int rows, const int* rp, const int* col, const T* va
   const SlabVariant v = kSlabVariants[(variant >= 0 && variant < kNumSlabVariants) ? variant : 0];
   const int grid = (rows + kSlabRows - 1) / kSlabRows;
   const unsigned smem = fed_smem_bytes(L.bytes, v);
+  // one wave: the blocks resident at once (SMs x blocks per SM, the padded count or the usual 5)
+  const int ahead = v.ahead * device_sm_count() * (v.ctas > 0 ? v.ctas : B200_FED_MIN_BLOCKS);
   switch (v.gather) {
-    case 2: return launch_fed_gb<T, Epi, 2>(grid, smem, st, pdl, rows, rp, col, val, x, epi, slab, cap, err);
-    case 8: return launch_fed_gb<T, Epi, 8>(grid, smem, st, pdl, rows, rp, col, val, x, epi, slab, cap, err);
-    default: return launch_fed_gb<T, Epi, 4>(grid, smem, st, pdl, rows, rp, col, val, x, epi, slab, cap, err);
+    case 2: return launch_fed_gb<T, Epi, 2>(grid, smem, st, pdl, rows, rp, col, val, x, epi, slab, cap, err, ahead);
+    case 8: return launch_fed_gb<T, Epi, 8>(grid, smem, st, pdl, rows, rp, col, val, x, epi, slab, cap, err, ahead);
+    case 0: return launch_fed_gb<T, Epi, 0>(grid, smem, st, pdl, rows, rp, col, val, x, epi, slab, cap, err, ahead);
+    default: return launch_fed_gb<T, Epi, 4>(grid, smem, st, pdl, rows, rp, col, val, x, epi, slab, cap, err, ahead);
   }
 }
 

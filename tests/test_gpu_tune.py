@@ -12,7 +12,7 @@ from ps26119 import generators as g
 
 pytestmark = pytest.mark.gpu
 
-NUM_VARIANTS = 5  # kSlabVariants in csrc/spmv.cuh
+NUM_VARIANTS = 7  # kSlabVariants in csrc/spmv.cuh
 
 
 def solve(lp, exact=True, precision="fp64"):

@@ -45,6 +45,12 @@ def test_noalloc_dot_matches_backend_dot_twice(exact):
         assert abs(got - want) <= TOL * (1.0 + abs(want)), (got, want)
         if exact:
             assert got == want  # the reference order: bit for bit
+    # once set up, calls take no device memory: the device's free memory does not move
+    free_before = torch.cuda.mem_get_info()[0]
+    for _ in range(3):
+        assert _noalloc(L, da, db, n, exact, out) == 0
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free_before
 
 
 @pytest.mark.gpu
