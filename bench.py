@@ -66,7 +66,7 @@ WORKLOADS = {
 }
 # DRAM bytes per iteration (both fused kernels: dram__bytes_read.sum + dram__bytes_write.sum of
 # one launch each) from the ncu capture summarised in the named profile.
-NCU_TRAFFIC = {("random1m", "fp64"): (146.1e6 + 5.7e6) + (120.1e6 + 3.6e6)}
+NCU_TRAFFIC = {("random1m", "fp64"): (146.08e6 + 5.14e6) + (120.07e6 + 3.59e6)}
 NCU_TRAFFIC_SOURCE = {("random1m", "fp64"): "profiles/k_slab_fed_random1m.md"}
 # Measured to-tolerance solves a default single-LP run adds after its timed steps.
 TIME_TO_TOL = [("random10k", "fp64"), ("random10k", "mixed"), ("staircase8760", "mixed")]
@@ -659,21 +659,30 @@ def reference_gpu_sample(args, lp, ours):
                     "update kernels) built for sm_100a, driven by its own r2HPDHG loop (host setup and checks)"}
 
 
-def time_to_tol_records(args):
+def time_to_tol_records(args, cases=None):
     """Measured time to 1e-8 KKT, one cold call of ps26119_solve_lp_ex each (presolve, the engine,
     the in-process check and the certified bound), wall clock, on the named LPs; the 10k LP also
-    through the reference's own CUDA backend on the same GPU. Outside the timed steps."""
+    through the reference's own CUDA backend on the same GPU. Outside the timed steps.
+    `cases`: (workload, precision) pairs, default TIME_TO_TOL."""
     import ps26119
     out = []
-    for name, precision in TIME_TO_TOL:
-        lp = make_lp(name)
+    last = None
+    for case in cases or TIME_TO_TOL:
+        name, precision = case[0], case[1]
+        stall = int(case[2]) if len(case) > 2 else 0  # mixed: the precision switch's stall window
+        lp = last[1] if last and last[0] == name else make_lp(name)
+        last = (name, lp)
         t0 = time.perf_counter()
         r = ps26119.solve_lp(lp.c, (lp.col_start, lp.row_index, lp.value), lp.row_lower, lp.row_upper,
                              lp.col_lower, lp.col_upper, sense=lp.sense, offset=lp.offset, algorithm="r2hpdhg",
-                             precision=precision, time_limit=900)
+                             precision=precision, time_limit=1800,
+                             engine={"presolve": True, "mixed_stall_checks": stall} if stall else None)
         sec = time.perf_counter() - t0
+        st = ps26119.last_stats()
         rec = {"workload": name, "precision": precision, "seconds": sec, "status": r.status_name,
-               "iterations": r.iterations, "objective": r.objective, "certified_bound": r.certified_bound,
+               "mixed_stall_checks": stall or None,
+               "iterations": r.iterations, "switch_iteration": st["switch_iteration"],
+               "engine_loop_s": st["loop_seconds"], "objective": r.objective, "certified_bound": r.certified_bound,
                "error_to_certified_bound": abs(r.objective - r.certified_bound) / (1.0 + abs(r.objective)),
                "rel_kkt": max(r.primal_residual, r.dual_residual, r.gap), "check": r.check,
                "entry": "ps26119_solve_lp_ex (presolve, engine, in-process check, certified bound)"}
@@ -835,6 +844,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-reference-gpu", action="store_true", help="skip the reference CUDA backend's sample")
     ap.add_argument("--no-time-to-tol", action="store_true", help="skip the measured time-to-1e-8 records")
+    ap.add_argument("--time-to-tol", default="",
+                    help="only the time-to-1e-8 records of these comma-separated workload:precision[:stall] "
+                         "cases (e.g. random1m:fp64,random1m:mixed:100; stall = the mixed precision switch's "
+                         "stall window in checks, default the reference's 10); no timed steps")
     ap.add_argument("--serve-sample", type=int, default=8, help="requests solved sequentially for the baseline")
     ap.add_argument("--serve-slots", type=int, default=0, help="server slots (0: the workload's)")
     ap.add_argument("--serve-solo", action="store_true",
@@ -845,7 +858,16 @@ def main():
         # read when the CUDA context is created, so it is set before anything touches CUDA
         os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
     rank, world, local = dist_setup()
-    if args.impl == "reference":
+    if args.time_to_tol:
+        import torch
+        torch.cuda.set_device(local)
+        cases = [tuple(c.split(":")) for c in args.time_to_tol.split(",")]
+        bad = [c for c in cases if len(c) not in (2, 3) or c[0] not in WORKLOADS or c[1] not in ("fp64", "mixed")
+               or (len(c) == 3 and not c[2].isdigit())]
+        if bad:
+            raise SystemExit(f"--time-to-tol: bad case(s) {bad}")
+        line = {"time_to_tol": time_to_tol_records(args, cases)} if rank == 0 else None
+    elif args.impl == "reference":
         line = run_reference(args, rank, world)
     elif WORKLOADS[args.workload]["kind"] == "batch":
         line = run_batch(args, rank, world, local)

@@ -121,6 +121,10 @@ typedef struct {
   int bound_objective_rescaling; /* -1 = default 1 */
   double reflection;         /* 0 = default 1.0 */
   double warm_primal_weight; /* > 0: start from this primal weight */
+  int mixed_stall_checks;    /* precision = mixed: checks without a 10% gain of the best relative KKT
+                                before the switch to fp64 (0 = the reference's 10; the switch at
+                                relative KKT 1e-6 applies either way) */
+  int reserved;              /* 0 */
 } ps26119_engine_options;
 
 PS26119_API void ps26119_default_engine_options(ps26119_engine_options* eo);

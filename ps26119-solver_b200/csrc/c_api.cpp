@@ -76,6 +76,8 @@ const char* apply_engine_options(const ps26119_engine_options* eo, Options& o) {
   if (eo->reflection != 0) o.reflection = eo->reflection;
   if (!(eo->warm_primal_weight >= 0)) return "warm_primal_weight must be >= 0";
   o.warm_primal_weight = eo->warm_primal_weight;
+  if (eo->mixed_stall_checks < 0) return "mixed_stall_checks must be >= 0";
+  if (eo->mixed_stall_checks > 0) o.mixed_stall_checks = eo->mixed_stall_checks;
   return nullptr;
 }
 
@@ -259,6 +261,8 @@ void ps26119_default_engine_options(ps26119_engine_options* eo) {
   eo->bound_objective_rescaling = -1;
   eo->reflection = 0.0;
   eo->warm_primal_weight = 0.0;
+  eo->mixed_stall_checks = 0;
+  eo->reserved = 0;
 }
 
 int ps26119_solve_lp(int num_rows, int num_cols, int sense, double obj_offset, const double* c,
@@ -379,6 +383,7 @@ int ps26119_solve_lp_device(int num_rows, int num_cols, int sense, double obj_of
     e.scaling = o.scaling;
     e.reflection = o.reflection;
     e.warm_primal_weight = o.warm_primal_weight;
+    e.mixed_stall_checks = o.mixed_stall_checks;
     e.verbosity = o.verbosity;
     const EngineResult R = run_engine(M, e, DeviceOutputs{d_x, d_y, d_z, nullptr, nullptr}, stream);
     Solution s;

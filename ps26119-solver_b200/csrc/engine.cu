@@ -129,6 +129,10 @@ class Engine {
           if (g) cudaGraphExecDestroy(g);
     for (auto& e : ev_)
       if (e) cudaEventDestroy(e);
+    for (auto& e : fork_)
+      if (e) cudaEventDestroy(e);
+    for (auto& q : side_)
+      if (q) cudaStreamDestroy(q);
 #ifdef B200_TEARDOWN_TRACE
     std::fprintf(stderr, "teardown: graphs+events %.1f ms\n",
                  std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tt0).count());
@@ -194,9 +198,11 @@ class Engine {
   template <class T> IterVecs<T>& vecs();
   template <class T> void capture_epoch();
   template <class T> void capture_check(int variant);
-  template <class T> void launch_residual(bool with_restart_terms, const int* skip, SumPlan& plan);
-  template <class T> void launch_kkt_scaled(const T* xs, const T* ys);
-  void launch_kkt_original();
+  template <class T> void launch_residual(bool with_restart_terms, const int* skip, SumPlan& plan,
+                                          cudaStream_t sums_on = nullptr);
+  template <class T> void launch_kkt_scaled(const T* xs, const T* ys, cudaStream_t on = nullptr);
+  void launch_kkt_original(cudaStream_t on = nullptr);
+  void make_side_streams();
   template <class T> void launch_ray(const T* dx, const T* dy, double* r, double* d, int drift);
   Kkt read_kkt(const double* h) const;
   Status ray_verdict(const double* h, int which, const Kkt& k, std::string& why) const;
@@ -256,6 +262,11 @@ class Engine {
   SumPlan plan_dist_;
   long long epoch_kernels_[2] = {0, 0}, check_kernels_[2][3] = {{0, 0, 0}, {0, 0, 0}};
   cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};
+  // The check graph's side branches: side_[0] runs the KKT statistics, side_[1] the residual's
+  // and restart distances' sums, while the engine's stream runs the ray tests (fork_[0..3]: the
+  // forks and joins that order them).
+  cudaStream_t side_[2] = {nullptr, nullptr};
+  cudaEvent_t fork_[4] = {nullptr, nullptr, nullptr, nullptr};
   long long kernels_ = 0;  // counted launches (graph kernel nodes per replay)
   long long capture_count_ = 0;
   bool capturing_ = false;
@@ -420,8 +431,10 @@ void Engine::build_plans() {
 }
 
 // The residual: dx = x̄ − x̂, adx = Ã dx, dy = ȳ − ŷ and the terms of the five dots.
+// sums_on: the stream of the dots' sums (nullptr: the engine's; another stream must already wait for
+// the engine's stream, and the caller joins it back).
 template <class T>
-void Engine::launch_residual(bool with_restart_terms, const int* skip, SumPlan& plan) {
+void Engine::launch_residual(bool with_restart_terms, const int* skip, SumPlan& plan, cudaStream_t sums_on) {
   IterVecs<T>& v = vecs<T>();
   const int m = M_.m, n = M_.n;
   double* px = rt_.get();
@@ -435,36 +448,52 @@ void Engine::launch_residual(bool with_restart_terms, const int* skip, SumPlan& 
   EpiResY<T> e{v.yb.get(), v.yh.get(), v.y0.get(), v.dy.get(), v.adx.get(), py, cross,
                with_restart_terms ? dyn : nullptr, skip};
   launch_slab_tma<T>(m, sp_.a_rp.get(), sp_.a_col.get(), sp_.A_val<T>(), v.dx.get(), e, st_, nullptr, err());
-  plan.launch(st_);
+  cudaStream_t ss = st_;
+  if (sums_on) {
+    B200_CHECK(cudaEventRecord(fork_[2], st_));
+    B200_CHECK(cudaStreamWaitEvent(sums_on, fork_[2], 0));
+    ss = sums_on;
+  }
+  plan.launch(ss);
   B200_COUNT(2 + plan.kernel_count());
   if (with_restart_terms) {
-    plan_pid_.launch(st_);
+    plan_pid_.launch(ss);
     B200_COUNT(plan_pid_.kernel_count());
   }
 }
 
-void Engine::launch_kkt_original() {
+void Engine::launch_kkt_original(cudaStream_t on) {
+  const cudaStream_t s = on ? on : st_;
   const int m = M_.m, n = M_.n;
   const long long L = static_cast<long long>(m) + n;
   double* K0 = kt_.get();
   EpiKktRows er{{}, yo_.get(), M_.row_lower, M_.row_upper, K0, K0 + L, K0 + 2 * L, res_.get()};
-  launch_slab_tma<double>(m, sp_.a_rp.get(), sp_.a_col.get(), sp_.a_v0.get(), xo_.get(), er, st_, nullptr, err());
+  launch_slab_tma<double>(m, sp_.a_rp.get(), sp_.a_col.get(), sp_.a_v0.get(), xo_.get(), er, s, nullptr, err());
   EpiKktCols ec{{}, xo_.get(), M_.c, M_.col_lower, M_.col_upper, static_cast<double>(M_.sense), m,
                 K0 + 3 * L, K0 + L, K0 + 2 * L, res_.get()};
-  launch_slab<double>(n, M_.col_start, M_.row_index, M_.value, yo_.get(), ec, st_, nullptr, err());
-  plan_kkt_.launch(st_);
+  launch_slab<double>(n, M_.col_start, M_.row_index, M_.value, yo_.get(), ec, s, nullptr, err());
+  plan_kkt_.launch(s);
   B200_COUNT(2 + plan_kkt_.kernel_count());
 }
 
 template <class T>
-void Engine::launch_kkt_scaled(const T* xs, const T* ys) {
+void Engine::launch_kkt_scaled(const T* xs, const T* ys, cudaStream_t on) {
+  const cudaStream_t s = on ? on : st_;
   const int m = M_.m, n = M_.n;
-  k_unscale_x<T><<<grid_for(n), kBlock, 0, st_>>>(n, xs, sp_.col_scale.get(), sp_.bound_scale, M_.col_lower,
-                                                  M_.col_upper, xo_.get());
-  k_unscale_y<T><<<grid_for(m), kBlock, 0, st_>>>(m, ys, sp_.row_scale.get(), sp_.obj_scale, yo_.get());
+  k_unscale_x<T><<<grid_for(n), kBlock, 0, s>>>(n, xs, sp_.col_scale.get(), sp_.bound_scale, M_.col_lower,
+                                                M_.col_upper, xo_.get());
+  k_unscale_y<T><<<grid_for(m), kBlock, 0, s>>>(m, ys, sp_.row_scale.get(), sp_.obj_scale, yo_.get());
   B200_LAUNCH_CHECK();
   B200_COUNT(2);
-  launch_kkt_original();
+  launch_kkt_original(s);
+}
+
+// The check graph's two side streams and its fork / join events, made once per engine outside
+// any capture.
+void Engine::make_side_streams() {
+  if (side_[0]) return;
+  for (auto& q : side_) B200_CHECK(cudaStreamCreateWithFlags(&q, cudaStreamNonBlocking));
+  for (auto& e : fork_) B200_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
 }
 
 template <class T>
@@ -565,13 +594,23 @@ void Engine::capture_check(int variant) {
   slab_prepare<double, EpiKktRows, B200_STAGE_TMA != 0>();
   slab_prepare<double, EpiKktCols, false>();
   slab_prepare<double, EpiRayRows, B200_STAGE_TMA != 0>();
+  make_side_streams();
   capturing_ = true;
   capture_count_ = 0;
   auto capture_scope = std::make_unique<CaptureScope>();  // no device-wide syncs elsewhere meanwhile
   B200_CHECK(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
   clear_maxima();
-  launch_residual<T>(true, nullptr, plan_res_);
-  launch_kkt_scaled<T>(v.xh.get(), v.yh.get());
+  // Three branches that share no buffer and write disjoint result slots: the KKT statistics of
+  // (x̂, ŷ) on side_[0]; the residual's kernels on the engine's stream, then their sums and the
+  // restart distances on side_[1] while the ray tests (which read dx, dy) run on the engine's
+  // stream. Each branch's order is the serial one, so every value is the same; the short sum
+  // kernels of one branch overlap the matrix products of another.
+  B200_CHECK(cudaEventRecord(fork_[0], st_));
+  B200_CHECK(cudaStreamWaitEvent(side_[0], fork_[0], 0));
+  launch_kkt_scaled<T>(v.xh.get(), v.yh.get(), side_[0]);
+  B200_CHECK(cudaEventRecord(fork_[1], side_[0]));
+  launch_residual<T>(true, nullptr, plan_res_, side_[1]);
+  B200_CHECK(cudaEventRecord(fork_[3], side_[1]));
   if (variant >= 1) launch_ray<T>(v.dx.get(), v.dy.get(), r1_.get(), d1_.get(), 0);
   if (variant == 2) {
     k_diff<T><<<grid_for(M_.n), kBlock, 0, st_>>>(M_.n, v.xh.get(), v.x0.get(), v.ddx.get());
@@ -580,6 +619,8 @@ void Engine::capture_check(int variant) {
     capture_count_ += 2;
     launch_ray<T>(v.ddx.get(), v.ddy.get(), r2_.get(), d2_.get(), 1);
   }
+  B200_CHECK(cudaStreamWaitEvent(st_, fork_[1], 0));  // join the KKT branch
+  B200_CHECK(cudaStreamWaitEvent(st_, fork_[3], 0));  // join the sums branch
   B200_CHECK(cudaMemcpyAsync(hres_.get(), res_.get(), kNumSlots * sizeof(double), cudaMemcpyDeviceToHost, st_));
   const cudaError_t e = cudaStreamEndCapture(st_, &g);
   capture_scope.reset();
@@ -991,7 +1032,7 @@ bool Engine::end_epoch() {
     if (rk < 0.9 * pol_best_) pol_best_ = rk, pol_since_best_ = 0;
     else ++pol_since_best_;
     const bool reached = rk <= kMixedPrecisionSwitch && o_.tolerance < kMixedPrecisionSwitch;
-    if (reached || pol_since_best_ >= 10) {
+    if (reached || pol_since_best_ >= o_.mixed_stall_checks) {
       promote();
       switch_it_ = S.it;
       promoted = true;
@@ -1332,7 +1373,7 @@ EngineResult Engine::run_pdlp(const DeviceOutputs& out) {
       if (e < 0.9 * pol_best_) pol_best_ = e, pol_since_best_ = 0;
       else ++pol_since_best_;
       const bool reached = e <= kMixedPrecisionSwitch && o_.tolerance < kMixedPrecisionSwitch;
-      if (reached || pol_since_best_ >= 10) {
+      if (reached || pol_since_best_ >= o_.mixed_stall_checks) {
         promote_pdlp();
         switch_it_ = it;
         promoted = true;

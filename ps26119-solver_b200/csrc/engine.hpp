@@ -45,6 +45,9 @@ struct EngineOptions {
   // warm start in the ORIGINAL space (host memory), engine.cpp:237-266
   std::vector<double> warm_x, warm_y;
   double warm_primal_weight = 0.0;
+  // mixed precision: checks without a 10% gain of the best relative KKT before the switch to fp64
+  // (PrecisionPolicy, engine.cpp:61-79, uses 10)
+  int mixed_stall_checks = 10;
   // termination normalisation overrides (set by the presolve wrapper), engine.h:31
   double kkt_b_norm = -1, kkt_c_norm = -1, kkt_obj_shift = 0;
   int verbosity = 0;

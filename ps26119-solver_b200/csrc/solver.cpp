@@ -1114,6 +1114,7 @@ EngineOptions engine_options(const Options& o) {  // engine.cpp:168-186
   e.warm_x = o.warm_x;
   e.warm_y = o.warm_y;
   e.warm_primal_weight = o.warm_primal_weight;
+  e.mixed_stall_checks = o.mixed_stall_checks;
   e.kkt_b_norm = o.kkt_b_norm;
   e.kkt_c_norm = o.kkt_c_norm;
   e.kkt_obj_shift = o.kkt_obj_shift;

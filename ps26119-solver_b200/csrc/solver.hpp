@@ -59,6 +59,7 @@ struct Options {
   std::vector<double> warm_x, warm_y;
   double warm_primal_weight = 0.0;
   double kkt_b_norm = -1, kkt_c_norm = -1, kkt_obj_shift = 0;
+  int mixed_stall_checks = 10;  // PrecisionPolicy's stall window (engine.cpp:61-79)
 };
 
 struct Solution {

@@ -65,7 +65,8 @@ class _EngineOptions(ctypes.Structure):  # ps26119_engine_options
     _fields_ = [("presolve", ctypes.c_int), ("check_every", ctypes.c_int), ("exact_reductions", ctypes.c_int),
                 ("ruiz_iterations", ctypes.c_int), ("pock_chambolle", ctypes.c_int),
                 ("bound_objective_rescaling", ctypes.c_int), ("reflection", ctypes.c_double),
-                ("warm_primal_weight", ctypes.c_double)]
+                ("warm_primal_weight", ctypes.c_double), ("mixed_stall_checks", ctypes.c_int),
+                ("reserved", ctypes.c_int)]
 
 
 class _Stats(ctypes.Structure):  # ps26119_stats
@@ -273,7 +274,8 @@ def _options(algorithm, precision, gpu, tolerance, time_limit, iteration_limit, 
 
 
 def engine_options(presolve=True, check_every=64, exact=False, ruiz_iterations=-1, pock_chambolle=-1,
-                   bound_objective_rescaling=-1, reflection=0.0, warm_primal_weight=0.0) -> _EngineOptions:
+                   bound_objective_rescaling=-1, reflection=0.0, warm_primal_weight=0.0,
+                   mixed_stall_checks=0) -> _EngineOptions:
     eo = _EngineOptions()
     load().ps26119_default_engine_options(ctypes.byref(eo))
     eo.presolve = int(bool(presolve))
@@ -284,6 +286,7 @@ def engine_options(presolve=True, check_every=64, exact=False, ruiz_iterations=-
     eo.bound_objective_rescaling = int(bound_objective_rescaling)
     eo.reflection = float(reflection)
     eo.warm_primal_weight = float(warm_primal_weight)
+    eo.mixed_stall_checks = int(mixed_stall_checks)
     return eo
 
 

@@ -130,3 +130,16 @@ def test_no_device_reports_not_solved():
 def test_solve_mps_argument_errors():
     r = ps26119.solve_mps(None)
     assert r.status == ps26119.INVALID_ARGUMENT and "path is NULL" in r.message
+
+
+def test_engine_options_layout_and_validation():
+    """ps26119_engine_options (this library's addition): its defaults, and a negative precision
+    switch stall window refused before the engine starts."""
+    L = ps26119.load()
+    assert ctypes.sizeof(ps26119._EngineOptions) == 48
+    eo = ps26119._EngineOptions()
+    L.ps26119_default_engine_options(ctypes.byref(eo))
+    assert (eo.presolve, eo.check_every, eo.exact_reductions, eo.mixed_stall_checks) == (1, 64, 0, 0)
+    r = ps26119.solve_lp([3, 5], [[1, 0], [0, 2], [3, 2]], [-np.inf] * 3, [4, 12, 18], sense=-1, precision="mixed",
+                         engine={"mixed_stall_checks": -1})
+    assert r.status == ps26119.INVALID_ARGUMENT and "mixed_stall_checks" in r.message

@@ -194,3 +194,21 @@ def test_random_10k_matches_recorded_reference_run():
     assert abs(s.iterations - rec["iterations"]) <= K, (s.iterations, rec["iterations"])
     ref_obj = float.fromhex(rec["objective"])
     assert abs(s.objective - ref_obj) <= REL_OBJ * (1 + abs(ref_obj))
+
+
+def test_mixed_precision_stall_window():
+    """mixed_stall_checks (this library's addition to the reference's PrecisionPolicy): a window of
+    one check switches to fp64 no later than the reference's 10, a window of 10,000 keeps fp32
+    until the 1e-6 switch; every answer is Optimal, checked, and within 1e-6 of the fp64 answer."""
+    lp = g.random_lp(3000, seed=8)
+    base = gpu_solve(lp, "fp64")
+    assert base.status == ps26119.OPTIMAL, base.message
+    switches = {}
+    for window in (1, 0, 10000):
+        s = ps26119.solve_lp(lp.c, (lp.col_start, lp.row_index, lp.value), lp.row_lower, lp.row_upper,
+                             lp.col_lower, lp.col_upper, sense=lp.sense, offset=lp.offset, algorithm="r2hpdhg",
+                             precision="mixed", engine={"presolve": False, "mixed_stall_checks": window})
+        switches[window] = ps26119.last_stats()["switch_iteration"]
+        assert s.status == ps26119.OPTIMAL and s.check == "PASS", (window, s.message)
+        assert abs(s.objective - base.objective) <= 1e-6 * (1 + abs(base.objective)), window
+    assert 0 < switches[1] <= switches[0] <= switches[10000], switches
