@@ -61,7 +61,12 @@ __device__ __forceinline__ double block_sum_fixed(double v, double* sh) {
 //             of the chain's earlier tiles), then the tile's XRun (exact int64: change of S, its
 //             lowest and highest running value, parity after, per parity before); a term with
 //             |t/u| ≥ 2^51 (or non-finite) marks the tile;
-//   k_xchain  one warp per chain walks its tiles in order with the EXACT s: a tile is committed
+//   k_xgroup  per group of kXGroup consecutive tiles of a long chain: the composition of the
+//             tiles' XRuns when all of them count in one grid with no split and no bad term;
+//   k_xchain  one warp per chain walks its groups, then its tiles, in order with the EXACT s: a
+//             run of whole groups is committed like one tile (below) as far as every running S
+//             provably stays inside the binade; the first group that is not is walked tile by
+//             tile. A tile is committed
 //             as s ← (S0 + K[S0 mod 2])·u when s = S0·u lies in the guessed binade and every
 //             running S stays within [2^52 + 1, 2^53 − 1] (then each exact partial sum lies inside
 //             the binade, at least u/2 from its ends, and rounds to that grid); any other tile is
@@ -79,8 +84,11 @@ struct XChain {
   long long lo, hi;  // terms t[lo, hi)
   double init;
   double* out;
-  int tile0, ntiles;  // this chain's tiles in the tile arrays (ntiles = 0: windows only)
+  int tile0, ntiles;    // this chain's tiles in the tile arrays (ntiles = 0: windows only)
+  int group0, ngroups;  // its groups of kXGroup tiles in the group array (ngroups = 0: none)
 };
+constexpr int kXGroup = 32;  // tiles per group (one warp lane per tile)
+constexpr int kXChainWarps = 4;  // warps per block of k_xchain / k_xgroup
 struct XTileStat {
   double sum, pmin, pmax;  // approximate: Σ t, min / max of the running sums from the tile start
   int bad;                 // a non-finite term
@@ -104,6 +112,12 @@ struct XTileAgg {
   XRun pre, suf;
   int split;
   int pad;
+};
+// A group of kXGroup consecutive tiles of one chain that all count in the same grid u with no
+// split and no bad term: the composition of their runs. u = 0: the group cannot be taken whole.
+struct XGroupAgg {
+  double u;
+  XRun run;
 };
 
 constexpr long long kX52 = 1LL << 52, kX53 = 1LL << 53;
@@ -522,15 +536,50 @@ __device__ __forceinline__ bool x_commit(double& s, double u, const XRun& r) {
   return true;
 }
 
+// One warp per group of kXGroup tiles: lane l composes tile l's run in order (an ordered warp
+// reduction); the group is whole when every tile counts in lane 0's grid, has no split and no bad
+// term. group_chain[g]: the chain of group g.
+static __global__ void __launch_bounds__(32 * kXChainWarps) k_xgroup(const XChain* ch, const int* group_chain,
+                                                                      int ngroups, const XTileAgg* ag,
+                                                                      XGroupAgg* gg, const int* skip) {
+  if (skip && *skip) return;
+  const int g = static_cast<int>((blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (g >= ngroups) return;
+  const XChain c = ch[group_chain[g]];
+  const int tile = c.tile0 + (g - c.group0) * kXGroup + lane;
+  const bool mine = tile < c.tile0 + c.ntiles;
+  XRun r = x_identity();
+  double u = 0.0;
+  bool ok = true;
+  if (mine) {
+    const XTileAgg& G = ag[tile];
+    r = G.pre;
+    u = G.u;
+    ok = !G.pre.bad && G.split < 0 && G.u != 0.0;
+  }
+  const double u0 = __shfl_sync(kFull, u, 0);
+  ok = __all_sync(kFull, !mine || (ok && u == u0)) != 0;
+  for (int off = 1; off < 32; off <<= 1) {  // ordered reduction: lane 0 ends with tiles 0 … 31
+    const XRun o = x_shfl_down(r, off);
+    if ((lane & (2 * off - 1)) == 0 && lane + off < 32) r = x_compose(r, o);
+  }
+  if (lane == 0) {
+    XGroupAgg out;
+    out.u = ok ? u0 : 0.0;
+    out.run = r;
+    gg[g] = out;
+  }
+}
+
 // One warp per chain (4 warps per block): tiles in order, the rest walked in windows. The tile
 // summaries are brought into shared memory 32 at a time; the lanes take one tile each and a warp
 // scan of their XRuns gives every tile its exact incoming S, so one step commits every tile up
 // to the first one that is not valid for the exact s or whose running sum changes binade. Such a
 // tile is taken on its own: its part before the change, the changing term as a plain addition,
 // its part after; what does not commit is walked in windows.
-constexpr int kXChainWarps = 4;
 static __global__ void __launch_bounds__(32 * kXChainWarps) k_xchain(const XChain* ch, int nch, const XTileAgg* ag,
-                                                                      const int* skip) {
+                                                                      const XGroupAgg* gg, const int* skip) {
   __shared__ XTileAgg sg[kXChainWarps][32];
   if (skip && *skip) return;
   const int warp = static_cast<int>((blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x) >> 5);
@@ -541,7 +590,50 @@ static __global__ void __launch_bounds__(32 * kXChainWarps) k_xchain(const XChai
   if (c.ntiles == 0) {
     s = x_window_walk(c.t, c.lo, c.hi, s);
   } else {
-    for (int g0 = 0; g0 < c.ntiles; g0 += 32) {
+    int g0 = 0;  // the next tile, a multiple of kXGroup
+    while (g0 < c.ntiles) {
+      if (gg && c.ngroups > 0) {
+        // whole groups first: up to 32 groups (32 · kXGroup tiles) per scan, committed up to the
+        // first group that is not whole, not in this binade, or whose running sum leaves it
+        const int gi = g0 / kXGroup;
+        const int cntg = c.ngroups - gi < 32 ? c.ngroups - gi : 32;
+        int e;
+        const bool have = x_binade(s, e);
+        const double u = have ? x_pow2(e - 52) : 0.0;
+        const long long S0 = have ? static_cast<long long>(s * x_pow2(52 - e)) : 0;
+        const int p0 = static_cast<int>(S0 & 1);
+        XRun r = x_identity();
+        bool mine_ok = false;
+        if (lane < cntg) {
+          const XGroupAgg& G = gg[c.group0 + gi + lane];
+          mine_ok = have && G.u == u && !G.run.bad;
+          r = G.run;
+        }
+        XRun inc = r;
+        for (int off = 1; off < 32; off <<= 1) {
+          const XRun o = x_shfl_up(inc, off);
+          if (lane >= off) inc = x_compose(o, inc);
+        }
+        XRun ex = x_shfl_up(inc, 1);
+        if (lane == 0) ex = x_identity();
+        const long long Kb = p0 ? ex.K[1] : ex.K[0];
+        const int pb = p0 ? ex.out[1] : ex.out[0];
+        bool valid = false;
+        if (mine_ok) {
+          const long long mn = pb ? r.mn[1] : r.mn[0], mx = pb ? r.mx[1] : r.mx[0];
+          valid = x_inside(S0, S0 + Kb + mn) && x_inside(S0, S0 + Kb + mx);
+        }
+        const unsigned bad = __ballot_sync(kFull, lane < cntg && !valid);
+        const int f = bad ? __ffs(bad) - 1 : cntg;  // first group not committed
+        if (f > 0) {
+          const long long K = f < 32 ? __shfl_sync(kFull, Kb, f & 31) : __shfl_sync(kFull, p0 ? inc.K[1] : inc.K[0], 31);
+          s = static_cast<double>(S0 + K) * u;
+        }
+        g0 += f * kXGroup;
+        if (f == cntg) continue;  // every loaded group taken: the next 32 groups
+      }
+      if (g0 >= c.ntiles) break;
+      // tiles g0 … g0 + 31 one by one
       const int cnt = c.ntiles - g0 < 32 ? c.ntiles - g0 : 32;
       __syncwarp();
       if (lane < cnt) sg[wl][lane] = ag[c.tile0 + g0 + lane];
@@ -605,6 +697,7 @@ static __global__ void __launch_bounds__(32 * kXChainWarps) k_xchain(const XChai
         }
         j = f + 1;
       }
+      g0 += 32;
     }
   }
   if (lane == 0) *c.out = s;
@@ -656,7 +749,7 @@ class SumPlan {
         if (j.order == SumOrder::kChunk64) ++nchunk_jobs;
       partials_.alloc(static_cast<std::size_t>(nchunk_jobs > 0 ? nchunk_jobs * kChunks : 1));
       auto chain = [&](const double* t, long long lo, long long hi, double init, double* out) {
-        XChain c{t, lo, hi, init, out, static_cast<int>(tile_chain.size()), 0};
+        XChain c{t, lo, hi, init, out, static_cast<int>(tile_chain.size()), 0, 0, 0};
         const long long n = hi - lo;
         if (n >= 2LL * kXTile) {  // long chains go by tiles; short ones by windows only
           c.ntiles = static_cast<int>((n + kXTile - 1) / kXTile);
@@ -675,11 +768,23 @@ class SumPlan {
           for (long long c = 0; c < chunks; ++c)
             chain(j.t, j.lo + n * c / chunks, j.lo + n * (c + 1) / chunks, 0.0, part + c);
           // parallel_sum: s = 0; s += part[c] in order — then the caller's init (0 for dots)
-          phase2.push_back({part, 0, chunks, j.init, j.out, 0, 0});
+          phase2.push_back({part, 0, chunks, j.init, j.out, 0, 0, 0, 0});
           ++slot;
         }
       }
       ntiles_ = static_cast<int>(tile_chain.size());
+      // chains of more than one group of tiles also get group summaries (k_xgroup)
+      std::vector<int> group_chain;
+      for (std::size_t k = 0; k < phase1.size(); ++k) {
+        XChain& c = phase1[k];
+        if (c.ntiles <= kXGroup) continue;
+        c.group0 = static_cast<int>(group_chain.size());
+        c.ngroups = (c.ntiles + kXGroup - 1) / kXGroup;
+        for (int g = 0; g < c.ngroups; ++g) group_chain.push_back(static_cast<int>(k));
+      }
+      ngroups_ = static_cast<int>(group_chain.size());
+      upload(group_chain, group_chain_, st);
+      group_agg_.alloc(static_cast<std::size_t>(ngroups_ > 0 ? ngroups_ : 1) * sizeof(XGroupAgg));
       upload(phase1, seg1_, st);
       upload(phase2, seg2_, st);
       upload(tile_chain, tile_chain_, st);
@@ -701,18 +806,24 @@ class SumPlan {
       const int* tc = reinterpret_cast<const int*>(tile_chain_.get());
       XTileStat* ts = reinterpret_cast<XTileStat*>(tile_stat_.get());
       XTileAgg* ta = reinterpret_cast<XTileAgg*>(tile_agg_.get());
+      XGroupAgg* tg = ngroups_ > 0 ? reinterpret_cast<XGroupAgg*>(group_agg_.get()) : nullptr;
       if (ntiles_ > 0) {
         k_xstat<<<ntiles_, kXThreads, 0, st>>>(c1, tc, ts, skip_);
         k_xagg<<<ntiles_, kXThreads, 0, st>>>(c1, tc, ts, ta, skip_);
         B200_LAUNCH_CHECK();
       }
+      if (ngroups_ > 0) {
+        k_xgroup<<<(ngroups_ + kXChainWarps - 1) / kXChainWarps, 32 * kXChainWarps, 0, st>>>(
+            c1, reinterpret_cast<const int*>(group_chain_.get()), ngroups_, ta, tg, skip_);
+        B200_LAUNCH_CHECK();
+      }
       if (n1_ > 0) {
-        k_xchain<<<(n1_ + kXChainWarps - 1) / kXChainWarps, 32 * kXChainWarps, 0, st>>>(c1, n1_, ta, skip_);
+        k_xchain<<<(n1_ + kXChainWarps - 1) / kXChainWarps, 32 * kXChainWarps, 0, st>>>(c1, n1_, ta, tg, skip_);
         B200_LAUNCH_CHECK();
       }
       if (n2_ > 0) {
         k_xchain<<<(n2_ + kXChainWarps - 1) / kXChainWarps, 32 * kXChainWarps, 0, st>>>(
-            reinterpret_cast<const XChain*>(seg2_.get()), n2_, ta, skip_);
+            reinterpret_cast<const XChain*>(seg2_.get()), n2_, ta, nullptr, skip_);
         B200_LAUNCH_CHECK();
       }
     } else if (nt_ > 0) {
@@ -723,7 +834,9 @@ class SumPlan {
       B200_LAUNCH_CHECK();
     }
   }
-  int kernel_count() const { return exact_ ? 2 * (ntiles_ > 0) + (n1_ > 0) + (n2_ > 0) : (nt_ > 0 ? 2 : 0); }
+  int kernel_count() const {
+    return exact_ ? 2 * (ntiles_ > 0) + (ngroups_ > 0) + (n1_ > 0) + (n2_ > 0) : (nt_ > 0 ? 2 : 0);
+  }
   bool empty() const { return jobs_.empty(); }
 
  private:
@@ -746,10 +859,10 @@ class SumPlan {
   std::vector<Job> jobs_;
   bool exact_ = false;
   const int* skip_ = nullptr;
-  DevBuf<unsigned char> seg1_, seg2_, tseg_, tile_chain_;
-  mutable DevBuf<unsigned char> tile_stat_, tile_agg_;
+  DevBuf<unsigned char> seg1_, seg2_, tseg_, tile_chain_, group_chain_;
+  mutable DevBuf<unsigned char> tile_stat_, tile_agg_, group_agg_;
   mutable DevBuf<double> partials_;
-  int n1_ = 0, n2_ = 0, nt_ = 0, ntiles_ = 0;
+  int n1_ = 0, n2_ = 0, nt_ = 0, ntiles_ = 0, ngroups_ = 0;
 };
 
 }  // namespace b200
