@@ -16,9 +16,11 @@
 #include "solver.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <limits>
+#include <memory>
 #include <thread>
 
 namespace b200 {
@@ -189,10 +191,9 @@ SafeBound bound_with(const Model& M, const std::vector<double>& y, const std::ve
   // per-column terms min over the enclosure [z_lo, z_hi] of z_j x_j, independent per column
   std::vector<DD>& col_term = t_certify.col_term;
   std::vector<char>& col_inf = t_certify.col_inf;
-  col_term.assign(static_cast<std::size_t>(n), DD{});
-  col_inf.assign(static_cast<std::size_t>(n), 0);
-  parallel_ranges(n, [&](long long jb, long long je) {
-    Expansion ex;
+  size_for_copy(col_term, static_cast<std::size_t>(n));  // every entry is written below before it is read
+  size_for_copy(col_inf, static_cast<std::size_t>(n));
+  auto columns = [&](long long jb, long long je, Expansion& ex) {
     for (long long jj = jb; jj < je; ++jj) {
       const int j = static_cast<int>(jj);
       if (jj + 2 < je)  // the multipliers of the column after next: random reads, started early
@@ -237,25 +238,63 @@ SafeBound bound_with(const Model& M, const std::vector<double>& y, const std::ve
       bool inf_lo = false, inf_hi = false;
       const DD tlo = min_term(zlo, col_lo[j], col_up[j], inf_lo);
       const DD thi = min_term(zhi, col_lo[j], col_up[j], inf_hi);
-      if (inf_lo || inf_hi) {
-        col_inf[j] = 1;
-        continue;
-      }
+      col_inf[j] = (inf_lo || inf_hi) ? 1 : 0;
+      if (col_inf[j]) continue;
       col_term[j] = tlo < thi ? tlo : thi;
     }
-  });
-  // the sum in the reference's order: rows, then columns
+  };
+  // The sum in the reference's order: rows, then columns. The columns are cut into chunks taken
+  // in index order from a shared counter by every task; task 0 first sums the rows, then sums
+  // each chunk's terms in order as soon as the chunk is done, taking chunks itself while the one
+  // it needs is not started, so the sequential sum runs beside the column pass instead of after
+  // it. The operations and their order are those of a column pass followed by the sum.
+  constexpr long long kChunkCols = 8192;
+  const long long nchunks = (static_cast<long long>(n) + kChunkCols - 1) / kChunkCols;
+  std::unique_ptr<std::atomic<int>[]> done(new std::atomic<int>[static_cast<std::size_t>(std::max(1LL, nchunks))]);
+  for (long long k = 0; k < nchunks; ++k) done[k].store(0, std::memory_order_relaxed);
+  std::atomic<long long> next{0};
+  std::atomic<bool> failed{false};
+  auto take_one = [&](Expansion& ex) {  // false: no chunk left to take
+    const long long k = next.fetch_add(1, std::memory_order_relaxed);
+    if (k >= nchunks) return false;
+    try {
+      columns(k * kChunkCols, std::min<long long>(n, (k + 1) * kChunkCols), ex);
+    } catch (...) {
+      failed.store(true);
+      done[k].store(1, std::memory_order_release);
+      throw;
+    }
+    done[k].store(1, std::memory_order_release);
+    return true;
+  };
   SafeSum L;
-  for (int i = 0; i < m; ++i) {
-    bool inf = false;
-    const DD t = min_term(sense * y[i], M.row_lower[i], M.row_upper[i], inf);
-    if (inf) ++r.unbounded_row_terms;
-    else L.add(t);
-  }
-  for (int j = 0; j < n; ++j) {
-    if (col_inf[j]) ++r.unbounded_col_terms;
-    else L.add(col_term[j]);
-  }
+  const int T = n < 65536 ? 1 : static_cast<int>(std::min<long long>(nchunks, host_thread_limit()));
+  parallel_tasks(T, [&](int t) {
+    Expansion ex;
+    if (t != 0) {
+      while (!failed.load(std::memory_order_relaxed) && take_one(ex)) {
+      }
+      return;
+    }
+    for (int i = 0; i < m; ++i) {
+      bool inf = false;
+      const DD tr = min_term(sense * y[i], M.row_lower[i], M.row_upper[i], inf);
+      if (inf) ++r.unbounded_row_terms;
+      else L.add(tr);
+    }
+    for (long long k = 0; k < nchunks; ++k) {
+      while (done[k].load(std::memory_order_acquire) == 0) {
+        if (failed.load()) return;
+        if (!take_one(ex)) std::this_thread::yield();  // chunk k is being computed by another task
+      }
+      if (failed.load()) return;
+      const long long je = std::min<long long>(n, (k + 1) * kChunkCols);
+      for (long long j = k * kChunkCols; j < je; ++j) {
+        if (col_inf[j]) ++r.unbounded_col_terms;
+        else L.add(col_term[j]);
+      }
+    }
+  });
   if (r.unbounded_row_terms > 0 || r.unbounded_col_terms > 0) {
     r.finite = false;
     r.bound = sense > 0 ? -std::numeric_limits<double>::infinity() : std::numeric_limits<double>::infinity();

@@ -199,6 +199,44 @@ void parallel_ranges(long long n, F&& f, long long min_parallel = 65536) {
   if (err) std::rethrow_exception(err);
 }
 
+// Runs task(t) for t in [0, T) on the pool (task 0 on the calling thread), or, when the pool is
+// in use, on threads of this call's own. Tasks may run one after another (T = 1, no thread could
+// be started): a task must never wait for work that only another task would do. The first
+// exception is rethrown on the calling thread once every task has returned.
+template <class F>
+void parallel_tasks(int T, F&& task) {
+  if (T <= 1) {
+    task(0);
+    return;
+  }
+  const std::function<void(int)> fn = [&](int t) { task(t); };
+  if (HostPool::instance().run(T, fn)) return;
+  std::mutex err_mu;
+  std::exception_ptr err;
+  auto guarded = [&](int t) {
+    try {
+      task(t);
+    } catch (...) {
+      std::lock_guard<std::mutex> lk(err_mu);
+      if (!err) err = std::current_exception();
+    }
+  };
+  std::vector<std::thread> th;
+  th.reserve(static_cast<std::size_t>(T - 1));
+  int started = 1;
+  for (; started < T; ++started) {
+    try {
+      th.emplace_back(guarded, started);
+    } catch (const std::system_error&) {
+      break;
+    }
+  }
+  guarded(0);
+  for (int t = started; t < T; ++t) guarded(t);
+  for (auto& x : th) x.join();
+  if (err) std::rethrow_exception(err);
+}
+
 // One host-to-host copy of `bytes` bytes (non-overlapping buffers).
 struct CopyJob {
   void* dst;
