@@ -32,6 +32,7 @@
 
 #include "checks.cuh"
 #include "engine.hpp"
+#include "parallel.hpp"
 #include "problem.cuh"
 #include "tune.hpp"
 
@@ -1642,6 +1643,99 @@ EngineResult run_engine(const DeviceModel& M, const EngineOptions& opt, const De
   return R;
 }
 
+namespace {
+
+// Host <-> device copies of pageable host arrays through two page-locked staging blocks: the host
+// threads fill (or empty) one block while the copy engine moves the other, so a copy runs at
+// the host threads' memcpy rate instead of the single-threaded staging of a pageable
+// cudaMemcpyAsync. `jobs` hold device and host addresses and sizes; blocks come from (and go back
+// to) the process's pinned-block cache.
+struct StagedCopy {
+  void* dev;
+  void* host;
+  std::size_t bytes;
+};
+constexpr std::size_t kStageBytes = std::size_t{16} << 20;
+
+// The pieces of the concatenated jobs, at most kStageBytes per block: block b takes bytes
+// [b·kStageBytes, (b+1)·kStageBytes) of the concatenation.
+template <class F>
+void for_each_piece(const std::vector<StagedCopy>& jobs, std::size_t block, F&& f) {
+  const std::size_t lo = block * kStageBytes, hi = lo + kStageBytes;
+  std::size_t off = 0;
+  for (const StagedCopy& j : jobs) {
+    const std::size_t a = std::max(lo, off), e = std::min(hi, off + j.bytes);
+    if (a < e) f(j, a - off, a - lo, e - a);  // job, offset in the job, offset in the block, bytes
+    off += j.bytes;
+  }
+}
+
+class StagingBlocks {
+ public:
+  explicit StagingBlocks(cudaStream_t st) : st_(st) {
+    for (int b = 0; b < 2; ++b) {
+      buf_[b] = static_cast<char*>(PinnedBlockCache::instance().acquire(kStageBytes));
+      B200_CHECK(cudaEventCreateWithFlags(&ev_[b], cudaEventDisableTiming));
+    }
+  }
+  ~StagingBlocks() {
+    for (int b = 0; b < 2; ++b) {  // the copies of both blocks have completed before they go back
+      cudaEventSynchronize(ev_[b]);
+      cudaEventDestroy(ev_[b]);
+      PinnedBlockCache::instance().release(buf_[b], kStageBytes);
+    }
+  }
+  void upload(const std::vector<StagedCopy>& jobs) {
+    const std::size_t nb = blocks(jobs);
+    for (std::size_t k = 0; k < nb; ++k) {
+      const int b = static_cast<int>(k & 1);
+      B200_CHECK(cudaEventSynchronize(ev_[b]));  // this block's previous copy has left it
+      std::vector<CopyJob> fill;
+      for_each_piece(jobs, k, [&](const StagedCopy& j, std::size_t jo, std::size_t bo, std::size_t n) {
+        fill.push_back({buf_[b] + bo, static_cast<const char*>(j.host) + jo, n});
+      });
+      parallel_copy(fill.data(), fill.size());
+      for_each_piece(jobs, k, [&](const StagedCopy& j, std::size_t jo, std::size_t bo, std::size_t n) {
+        B200_CHECK(cudaMemcpyAsync(static_cast<char*>(j.dev) + jo, buf_[b] + bo, n, cudaMemcpyHostToDevice, st_));
+      });
+      B200_CHECK(cudaEventRecord(ev_[b], st_));
+    }
+  }
+  void download(const std::vector<StagedCopy>& jobs) {
+    const std::size_t nb = blocks(jobs);
+    auto issue = [&](std::size_t k) {
+      const int b = static_cast<int>(k & 1);
+      for_each_piece(jobs, k, [&](const StagedCopy& j, std::size_t jo, std::size_t bo, std::size_t n) {
+        B200_CHECK(cudaMemcpyAsync(buf_[b] + bo, static_cast<const char*>(j.dev) + jo, n, cudaMemcpyDeviceToHost, st_));
+      });
+      B200_CHECK(cudaEventRecord(ev_[b], st_));
+    };
+    if (nb > 0) issue(0);
+    for (std::size_t k = 0; k < nb; ++k) {
+      const int b = static_cast<int>(k & 1);
+      if (k + 1 < nb) issue(k + 1);  // the other block: its previous contents were copied out below
+      B200_CHECK(cudaEventSynchronize(ev_[b]));
+      std::vector<CopyJob> drain;
+      for_each_piece(jobs, k, [&](const StagedCopy& j, std::size_t jo, std::size_t bo, std::size_t n) {
+        drain.push_back({static_cast<char*>(j.host) + jo, buf_[b] + bo, n});
+      });
+      parallel_copy(drain.data(), drain.size());
+    }
+  }
+
+ private:
+  static std::size_t blocks(const std::vector<StagedCopy>& jobs) {
+    std::size_t total = 0;
+    for (const StagedCopy& j : jobs) total += j.bytes;
+    return (total + kStageBytes - 1) / kStageBytes;
+  }
+  cudaStream_t st_;
+  char* buf_[2] = {nullptr, nullptr};
+  cudaEvent_t ev_[2] = {nullptr, nullptr};
+};
+
+}  // namespace
+
 EngineResult run_engine_host(const HostModelView& H, const EngineOptions& opt, HostOutputs& out) {
   cudaStream_t st;
   B200_CHECK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
@@ -1651,14 +1745,20 @@ EngineResult run_engine_host(const HostModelView& H, const EngineOptions& opt, H
   } guard{st};
   const int m = H.m, n = H.n;
   const long long nnz = H.col_start[n];
+  const std::size_t mm = static_cast<std::size_t>(m), nn = static_cast<std::size_t>(n);
+  const std::size_t nz = static_cast<std::size_t>(nnz);
   DevBuf<double> c, cl, cu, rl, ru, v, x, y, z, dr, pr;
   DevBuf<int> cs, ri;
-  c.upload(H.c, n, st), cl.upload(H.col_lower, n, st), cu.upload(H.col_upper, n, st);
-  rl.upload(H.row_lower, m, st), ru.upload(H.row_upper, m, st);
-  cs.upload(H.col_start, static_cast<std::size_t>(n) + 1, st);
-  ri.upload(H.row_index, static_cast<std::size_t>(nnz), st);
-  v.upload(H.value, static_cast<std::size_t>(nnz), st);
-  x.alloc(n), z.alloc(n), pr.alloc(n), y.alloc(m), dr.alloc(m);
+  c.alloc(nn), cl.alloc(nn), cu.alloc(nn), rl.alloc(mm), ru.alloc(mm), cs.alloc(nn + 1), ri.alloc(nz), v.alloc(nz);
+  x.alloc(nn), z.alloc(nn), pr.alloc(nn), y.alloc(mm), dr.alloc(mm);
+  {
+    StagingBlocks stage(st);
+    const auto d = [](const double* h) { return const_cast<double*>(h); };
+    stage.upload({{c.get(), d(H.c), nn * 8}, {cl.get(), d(H.col_lower), nn * 8}, {cu.get(), d(H.col_upper), nn * 8},
+                  {rl.get(), d(H.row_lower), mm * 8}, {ru.get(), d(H.row_upper), mm * 8},
+                  {cs.get(), const_cast<int*>(H.col_start), (nn + 1) * 4}, {ri.get(), const_cast<int*>(H.row_index), nz * 4},
+                  {v.get(), d(H.value), nz * 8}});
+  }
   DeviceModel M;
   M.m = m, M.n = n, M.sense = H.sense, M.offset = H.offset, M.nnz = nnz;
   M.c = c.get(), M.col_lower = cl.get(), M.col_upper = cu.get(), M.row_lower = rl.get(), M.row_upper = ru.get();
@@ -1666,11 +1766,14 @@ EngineResult run_engine_host(const HostModelView& H, const EngineOptions& opt, H
   DeviceOutputs o{x.get(), y.get(), z.get(), dr.get(), pr.get()};
   EngineResult R = run_engine(M, opt, o, st);
   out.x = pooled_vector(n), out.y = pooled_vector(m), out.z = pooled_vector(n);
-  x.download(out.x.data(), n, st);
-  y.download(out.y.data(), m, st);
-  z.download(out.z.data(), n, st);
-  if (R.have_dual_ray) out.dual_ray.resize(m), dr.download(out.dual_ray.data(), m, st);
-  if (R.have_primal_ray) out.primal_ray.resize(n), pr.download(out.primal_ray.data(), n, st);
+  std::vector<StagedCopy> back = {{x.get(), out.x.data(), nn * 8}, {y.get(), out.y.data(), mm * 8},
+                                  {z.get(), out.z.data(), nn * 8}};
+  if (R.have_dual_ray) out.dual_ray.resize(m), back.push_back({dr.get(), out.dual_ray.data(), mm * 8});
+  if (R.have_primal_ray) out.primal_ray.resize(n), back.push_back({pr.get(), out.primal_ray.data(), nn * 8});
+  {
+    StagingBlocks stage(st);
+    stage.download(back);
+  }
   B200_CHECK(cudaStreamSynchronize(st));
   return R;
 }
