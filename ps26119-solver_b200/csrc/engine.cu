@@ -16,6 +16,7 @@
 //     bit-identical to the reference CPU engine; in fast mode only the reductions differ
 //     (fixed-order trees), by rounding.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
@@ -1422,18 +1423,35 @@ class GroupScheduler {
     std::exception_ptr error;
     cudaEvent_t ready = nullptr;  // the engine's stream has its step scalars (and restart) in place
   };
+  // A device has PS26119_GROUPS_PER_DEVICE groups (default 2), each with its own host thread
+  // and stream, so that one group's host decisions between epochs overlap another group's
+  // kernels; a solve joins the group with the fewest solves.
   static GroupScheduler& for_current_device() {
     static std::mutex mu;
-    static std::map<int, GroupScheduler*> all;  // never destroyed: the threads live until exit
+    static std::map<int, std::vector<GroupScheduler*>> all;  // never destroyed: the threads live until exit
+    static const int per_device = [] {
+      const char* e = std::getenv("PS26119_GROUPS_PER_DEVICE");
+      const int k = e && *e ? std::atoi(e) : 2;
+      return std::min(64, std::max(1, k));
+    }();
     int dev = 0;
     B200_CHECK(cudaGetDevice(&dev));
     std::lock_guard<std::mutex> lk(mu);
-    GroupScheduler*& g = all[dev];
-    if (!g) g = new GroupScheduler(dev);
-    return *g;
+    std::vector<GroupScheduler*>& v = all[dev];
+    while (static_cast<int>(v.size()) < per_device) v.push_back(new GroupScheduler(dev));
+    GroupScheduler* best = v.front();
+    for (GroupScheduler* g : v)
+      if (g->load_.load() < best->load_.load()) best = g;
+    ++best->load_;  // counted from the choice, so that concurrent joiners spread out
+    return *best;
   }
-  // Runs the engine's epochs in the group until it finishes (the caller's thread waits).
+  // Runs the engine's epochs in the group until it finishes (the caller's thread waits). The
+  // scheduler came from for_current_device(), which counted the solve in.
   void run(Job& job) {
+    struct Leave {
+      std::atomic<int>& n;
+      ~Leave() { --n; }
+    } leave{load_};
     std::unique_lock<std::mutex> lk(mu_);
     pending_.push_back(&job);
     cv_.notify_all();
@@ -1571,6 +1589,7 @@ class GroupScheduler {
     }
   }
   int dev_ = 0;
+  std::atomic<int> load_{0};  // solves joined and not yet finished
   cudaStream_t st_ = nullptr;
   cudaEvent_t steps_done_ = nullptr;
   std::thread thread_;
