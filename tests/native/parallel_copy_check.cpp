@@ -4,7 +4,9 @@
 // documented; parallel_ranges covers every index exactly once when sections run from several
 // threads at once (all but one fall back to threads of their own), when a section is started
 // inside another, in a child process made by fork() after the pool has started, and when a range
-// throws (the exception reaches the caller after every range has run). Prints "ok"
+// throws (the exception reaches the caller after every range has run); parallel_tasks runs every
+// task once (pool, nested, single), lets a task wait on work items others took, and returns an
+// exception after every task has returned. Prints "ok"
 // and exits 0, or names the first failure and exits 1.
 #include <sys/wait.h>
 #include <unistd.h>
@@ -112,6 +114,67 @@ int main() {
     if (!caught || visited.load() != 200000 || !covers(90001) || !covers(70000)) {
       std::printf("exception from a range (nested %d): caught %d, visited %lld\n", nested, caught ? 1 : 0,
                   visited.load());
+      return 1;
+    }
+  }
+  // parallel_tasks: every task index runs once, on the pool, nested (threads of its own) and as a
+  // single task; a task that takes shared work items from a counter and waits only for items
+  // another task has taken finishes in every case; an exception reaches the caller after every
+  // task has returned
+  auto tasks_ok = [](int T) {
+    std::vector<std::atomic<int>> ran(static_cast<std::size_t>(T));
+    for (auto& a : ran) a.store(0);
+    constexpr int kItems = 97;
+    std::vector<std::atomic<int>> done(kItems);
+    for (auto& a : done) a.store(0);
+    std::atomic<int> next{0};
+    long long order_sum = 0;  // task 0 consumes the items in index order
+    parallel_tasks(T, [&](int t) {
+      ran[static_cast<std::size_t>(t)].fetch_add(1);
+      auto take = [&] {
+        const int k = next.fetch_add(1);
+        if (k >= kItems) return false;
+        done[static_cast<std::size_t>(k)].store(1, std::memory_order_release);
+        return true;
+      };
+      if (t != 0) {
+        while (take()) {
+        }
+        return;
+      }
+      for (int k = 0; k < kItems; ++k) {
+        while (done[static_cast<std::size_t>(k)].load(std::memory_order_acquire) == 0)
+          if (!take()) std::this_thread::yield();
+        order_sum += k;
+      }
+    });
+    for (auto& a : ran)
+      if (a.load() != 1) return false;
+    return order_sum == static_cast<long long>(kItems) * (kItems - 1) / 2;
+  };
+  if (!tasks_ok(1) || !tasks_ok(8) || !tasks_ok(static_cast<int>(T))) {
+    std::printf("parallel_tasks\n");
+    return 1;
+  }
+  std::atomic<int> nested_ok{0};
+  parallel_ranges(100000, [&](long long, long long) { nested_ok += tasks_ok(4) ? 1 : 0; });
+  if (nested_ok.load() != T) {
+    std::printf("parallel_tasks nested: %d\n", nested_ok.load());
+    return 1;
+  }
+  {
+    std::atomic<int> returned{0};
+    bool caught = false;
+    try {
+      parallel_tasks(6, [&](int t) {
+        ++returned;
+        if (t == 3) throw std::runtime_error("planted task");
+      });
+    } catch (const std::runtime_error& e) {
+      caught = std::strcmp(e.what(), "planted task") == 0;
+    }
+    if (!caught || returned.load() != 6 || !covers(70000)) {
+      std::printf("exception from a task: caught %d, returned %d\n", caught ? 1 : 0, returned.load());
       return 1;
     }
   }

@@ -1,7 +1,9 @@
 """The host threading helpers (csrc/parallel.hpp) that the C API's model copy, presolve,
 postsolve and the checks use: tests/native/parallel_copy_check.cpp, compiled here, checks
-parallel_copy byte for byte against memcpy, and that the worker pool behind parallel_ranges
-covers every index once with concurrent callers, nested sections and a forked child. CPU only."""
+parallel_copy byte for byte against memcpy, that the worker pool behind parallel_ranges
+covers every index once with concurrent callers, nested sections and a forked child, and that
+parallel_tasks (the certified bound's pipelined sum) runs every task once and never deadlocks a
+task that waits on work items others took. CPU only."""
 import os
 import subprocess
 
