@@ -287,11 +287,21 @@ template <> IterVecs<float>& Engine::vecs<float>() { return vf_; }
 #define B200_COUNT(k) (capturing_ ? capture_count_ += (k) : kernels_ += (k))
 
 void Engine::setup() {
+  // verbosity >= 2: the setup's phases on the host clock, the stream synchronised at each mark
+  std::vector<std::pair<const char*, double>> marks;
+  auto mark = [&](const char* name) {
+    if (o_.verbosity < 2) return;
+    B200_CHECK(cudaStreamSynchronize(st_));
+    marks.emplace_back(name, elapsed());
+  };
+  mark("start");
   stage_err_.alloc(1);
   B200_CHECK(cudaMemsetAsync(stage_err_.get(), 0, sizeof(unsigned), st_));
   sp_.build(M_, o_.scaling, o_.exact, st_);
+  mark("structure+scaling");
   if (o_.mixed) sp_.make_f32(st_);
   const double norm = sp_.lanczos(st_, err());
+  mark("lanczos");
   eta_ = norm > 0 ? 0.998 / norm : 1.0;  // engine.cpp:203-204
   kernels_ += sp_.kernels;
   const int m = M_.m, n = M_.n;
@@ -318,8 +328,20 @@ void Engine::setup() {
   xo_.alloc(nn), yo_.alloc(mm), r1_.alloc(mm), d1_.alloc(nn), r2_.alloc(mm), d2_.alloc(nn);
   objt_.alloc(mm + 2 * nn);
   build_plans();
+  mark("tables+buffers+plans");
   if (o_.mixed) tune_slab<float>();
   else tune_slab<double>();
+  mark("tuner");
+  if (o_.verbosity >= 2) {
+    std::string line = "setup phases:";
+    char buf[96];
+    for (std::size_t k = 1; k < marks.size(); ++k) {
+      std::snprintf(buf, sizeof buf, " %s %.2f ms", marks[k].first, 1e3 * (marks[k].second - marks[k - 1].second));
+      line += buf;
+    }
+    std::snprintf(buf, sizeof buf, " (Lanczos steps launched: %d)", sp_.lanczos_launched);
+    std::fprintf(stderr, "%s%s\n", line.c_str(), buf);
+  }
 }
 
 // The autotuner (tune.hpp): times the k_slab_fed variants on this matrix, for both iteration

@@ -85,6 +85,7 @@ struct ScaledDevice {
   // original-space constants of kkt_general (cpu_backend.cpp:233-262): ‖b‖₂, ‖c‖₂, ‖c‖∞
   double b_norm = 0, c_norm = 0, c_inf = 0;
   long long kernels = 0;
+  int lanczos_launched = 0;  // Lanczos steps launched by the last lanczos() (counted or not)
 
   // Scratch for the setup reductions.
   DevBuf<double> tmp_m, tmp_n, fac_m, fac_n, sums;
@@ -257,6 +258,7 @@ struct ScaledDevice {
     }
     nv = std::sqrt(nv);
     for (double& e : hv) e /= nv;
+    lanczos_launched = 0;
     DevBuf<double> v(n), vprev(n), w(n), t(m), terms(n);
     B200_CHECK(cudaMemcpyAsync(v.get(), hv.data(), hv.size() * sizeof(double), cudaMemcpyHostToDevice, st));
     B200_CHECK(cudaMemsetAsync(vprev.get(), 0, static_cast<std::size_t>(n) * sizeof(double), st));
@@ -290,6 +292,7 @@ struct ScaledDevice {
         B200_LAUNCH_CHECK();
         kernels += 5 + pal.kernel_count() + pbn.kernel_count();
       }
+      lanczos_launched = done + batch;
       B200_CHECK(cudaMemcpyAsync(h.data() + 2 * done, hist.get() + 2 * done, 2 * batch * sizeof(double),
                                  cudaMemcpyDeviceToHost, st));
       B200_CHECK(cudaStreamSynchronize(st));
