@@ -187,18 +187,21 @@ int solve_host(int num_rows, int num_cols, int sense, double obj_offset, const d
     Options o;
     if (const char* bad = to_options(opt, num_rows, num_cols, o)) return phase_log_begin(false), invalid(bad);
     if (const char* bad = apply_engine_options(eo, o)) return phase_log_begin(false), invalid(bad);
+    o.model_validated = true;  // validated just above
     Solution s = solve(m, o);
     fill(s, result);
     fill_stats(s, s.engine_result.iterations > 0 ? num_rows : 0, num_cols, nnz);
     g_stats.call_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - call_t0).count();
-    auto out = [](double* dst, const std::vector<double>& v, int len) {
-      if (dst && v.size() == static_cast<std::size_t>(len)) std::memcpy(dst, v.data(), sizeof(double) * len);
+    std::vector<CopyJob> outs;  // the caller's outputs, copied on the host threads
+    auto out = [&outs](double* dst, const std::vector<double>& v, int len) {
+      if (dst && v.size() == static_cast<std::size_t>(len)) outs.push_back({dst, v.data(), sizeof(double) * len});
     };
     out(x, s.x, num_cols);
     out(y, s.y, num_rows);
     out(z, s.z, num_cols);
     out(dual_ray, s.dual_ray, num_rows);
     out(primal_ray, s.primal_ray, num_cols);
+    parallel_copy(outs.data(), outs.size());
     pool_vector(std::move(s.x)), pool_vector(std::move(s.y)), pool_vector(std::move(s.z));  // for the next call
     phase_note("call", std::chrono::duration<double>(std::chrono::steady_clock::now() - call_t0).count());
     phase_log_end("solve_lp");

@@ -1136,7 +1136,7 @@ Solution solve_direct(const Model& model, const Options& options, bool certify =
   const auto t0 = clock_t_::now();
   Solution sol;
   sol.precision = options.precision == Precision::Mixed ? "mixed" : "fp64";
-  if (auto err = model.validate(); !err.empty()) {
+  if (auto err = options.model_validated ? std::string() : model.validate(); !err.empty()) {
     sol.status = Status::NotSolved;
     sol.message = "invalid model: " + err;
     return sol;
@@ -1237,7 +1237,8 @@ Solution solve_impl(const Model& model, const Options& options) {
                         (!options.warm_y.empty() && static_cast<int>(options.warm_y.size()) != model.num_rows);
   auto finite = [](const std::vector<double>& v) { return std::all_of(v.begin(), v.end(), [](double a) { return std::isfinite(a); }); };
   const bool bad_warm_values = !finite(options.warm_x) || !finite(options.warm_y);
-  if (!options.presolve || bad_warm || bad_warm_values || !model.validate().empty()) return solve_direct(model, options);
+  if (!options.presolve || bad_warm || bad_warm_values || (!options.model_validated && !model.validate().empty()))
+    return solve_direct(model, options);
   if (auto why = model.crossed_bounds(); !why.empty()) return trivially_infeasible(options, why);
   const auto t0 = clock_t_::now();
   // this thread's presolve result, its memory reused from the previous call (host_keep)
@@ -1267,6 +1268,7 @@ Solution solve_impl(const Model& model, const Options& options) {
   }
   Options inner = options;
   inner.presolve = false;
+  inner.model_validated = false;  // the reduced model is checked before it reaches the device
   {
     double b2 = 0, c2 = 0;
     for (int i = 0; i < model.num_rows; ++i) {

@@ -60,6 +60,10 @@ struct Options {
   double warm_primal_weight = 0.0;
   double kkt_b_norm = -1, kkt_c_norm = -1, kkt_obj_shift = 0;
   int mixed_stall_checks = 10;  // PrecisionPolicy's stall window (engine.cpp:61-79)
+  // Internal: the caller has validated this model (the C API does, before its copy is solved), so
+  // the solve skips repeating that pass over it, and over presolve's reduced model, which is
+  // valid by construction. Off for every other caller.
+  bool model_validated = false;
 };
 
 struct Solution {
