@@ -18,6 +18,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <cstdarg>
 #include <cstdio>
 #include <limits>
 #include <memory>
@@ -435,77 +436,112 @@ ImpliedBounds implied_bounds(const Model& M, int max_passes) {  // implied_bound
   return r;
 }
 
+namespace {
+
+// The interval part of the Farkas tolerance test. A multiplier t on a row (t = r_i) or a column
+// (t = −(Aᵀr)_j) picks the lower bound when positive and the upper bound when negative; a
+// picked bound that is finite adds t·bound to the certificate's objective and a magnitude term
+// to its scale, an infinite one is a violation of size |t|. Zero (and NaN) multipliers pick
+// nothing. Terms are taken in the order the caller offers them.
+struct FarkasTally {
+  double obj = 0.0, mag = 0.0, viol = 0.0;
+  template <class Magnitude>
+  void take(double t, double lo, double hi, Magnitude&& magnitude) {
+    if (!(t > 0) && !(t < 0)) return;
+    const double bound = t > 0 ? lo : hi;
+    if (std::isfinite(bound)) {
+      obj += t * bound;
+      mag += magnitude(bound);
+    } else {
+      viol = std::max(viol, t > 0 ? t : -t);
+    }
+  }
+};
+
+// Largest step a direction value v takes outside the finite sides of an interval: −v past a
+// finite lower side, then v past a finite upper side (in that order).
+inline double widen(double viol, double v, double lo, double hi) {
+  if (std::isfinite(lo)) viol = std::max(viol, -v);
+  if (std::isfinite(hi)) viol = std::max(viol, v);
+  return viol;
+}
+
+std::string format_detail(const char* fmt, ...) {
+  char buf[200];
+  va_list ap;
+  va_start(ap, fmt);
+  std::vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  return buf;
+}
+
+}  // namespace
+
+// A Farkas vector r proves infeasibility when the best objective of the zero-cost model bounded
+// through r is positive. First the rounding-proof way: the certified bound of the model with its
+// objective set to zero, from multipliers r. Failing that, the fp64 tolerance test: the tally of
+// r over the row intervals, then of −Aᵀr over the column intervals, scaled by max(‖r‖∞,
+// violation) (reference src/core/certificates.cpp:14-86; the same terms in the same order).
 CertificateCheck check_infeasibility_certificate(const Model& model, const std::vector<double>& r) {
-  CertificateCheck c;  // certificates.cpp:14-86
-  if (static_cast<int>(r.size()) != model.num_rows || model.num_rows == 0) {
+  CertificateCheck c;
+  const int m = model.num_rows, n = model.num_cols;
+  if (static_cast<int>(r.size()) != m || m == 0) {
     c.detail = "no dual ray";
     return c;
   }
   c.present = true;
-  for (double v : r)
-    if (!std::isfinite(v)) {
-      c.detail = "dual ray is not finite";
-      return c;
-    }
-  // stage 1, rigorous: the certified bound of the same feasible set with objective 0 is L₀(r)
+  if (!std::all_of(r.begin(), r.end(), [](double v) { return std::isfinite(v); })) {
+    c.detail = "dual ray is not finite";
+    return c;
+  }
   Model zero = model;
   zero.sense = 1;
   zero.obj_offset = 0.0;
   std::fill(zero.obj.begin(), zero.obj.end(), 0.0);
   const SafeBound sb = certified_dual_bound(zero, r);
-  char buf[200];
   if (sb.finite && sb.bound > 0.0) {
     c.passed = c.rigorous = true;
     c.measure = sb.bound;
-    std::snprintf(buf, sizeof buf, "Farkas certificate: certified L0(r) = %.3g > 0 (rounding-proof)", sb.bound);
-    c.detail = buf;
+    c.detail = format_detail("Farkas certificate: certified L0(r) = %.3g > 0 (rounding-proof)", sb.bound);
     return c;
   }
-  // stage 2: the fp64 tolerance test with the parts pointing at infinite bounds as violation
-  const int m = model.num_rows, n = model.num_cols;
-  double rmax = 0.0, obj = 0.0, viol = 0.0, mag = 0.0;
+  FarkasTally tally;
+  double rmax = 0.0;
   for (int i = 0; i < m; ++i) {
     rmax = std::max(rmax, std::fabs(r[i]));
-    if (r[i] > 0) {
-      if (std::isfinite(model.row_lower[i])) obj += r[i] * model.row_lower[i], mag += std::fabs(r[i] * model.row_lower[i]);
-      else viol = std::max(viol, r[i]);
-    } else if (r[i] < 0) {
-      if (std::isfinite(model.row_upper[i])) obj += r[i] * model.row_upper[i], mag += std::fabs(r[i] * model.row_upper[i]);
-      else viol = std::max(viol, -r[i]);
-    }
+    tally.take(r[i], model.row_lower[i], model.row_upper[i], [&](double bound) { return std::fabs(r[i] * bound); });
   }
-  std::vector<double> atr(n, 0.0), atr_abs(n, 0.0);
-  for (int j = 0; j < n; ++j)
-    for (int k = model.col_start[j]; k < model.col_start[j + 1]; ++k) {
-      atr[j] += model.value[k] * r[model.row_index[k]];
-      atr_abs[j] += std::fabs(model.value[k] * r[model.row_index[k]]);
-    }
   for (int j = 0; j < n; ++j) {
-    const double lam = -atr[j];
-    if (lam > 0) {
-      if (std::isfinite(model.col_lower[j])) obj += lam * model.col_lower[j], mag += atr_abs[j] * std::fabs(model.col_lower[j]);
-      else viol = std::max(viol, lam);
-    } else if (lam < 0) {
-      if (std::isfinite(model.col_upper[j])) obj += lam * model.col_upper[j], mag += atr_abs[j] * std::fabs(model.col_upper[j]);
-      else viol = std::max(viol, -lam);
+    double atr = 0.0, atr_abs = 0.0;  // (Aᵀr)_j and Σ|a_ij r_i|, in the column's entry order
+    for (int k = model.col_start[j]; k < model.col_start[j + 1]; ++k) {
+      const double p = model.value[k] * r[model.row_index[k]];
+      atr += p;
+      atr_abs += std::fabs(p);
     }
+    tally.take(-atr, model.col_lower[j], model.col_upper[j], [&](double bound) { return atr_abs * std::fabs(bound); });
   }
-  const double scale = std::max(rmax, viol);
-  c.measure = scale > 0 ? obj / scale : 0.0;
-  c.violation = scale > 0 ? viol / scale : 0.0;
-  c.passed = std::isfinite(c.measure) && c.measure > 0 && obj > kVerifyRay * mag && c.violation <= kVerifyRay * c.measure;
-  std::snprintf(buf, sizeof buf,
-                "Farkas certificate: rigorous L0(r) = %.3g; tolerance test L0/s = %.3g, violation/s = %.3g, "
-                "L0/sum|terms| = %.3g (%s)",
-                sb.bound, c.measure, c.violation, mag > 0 ? obj / mag : 0.0,
-                c.passed ? "infeasibility shown within tolerance, not rounding-proof" : "FAIL");
-  c.detail = buf;
+  const double scale = std::max(rmax, tally.viol);
+  c.measure = scale > 0 ? tally.obj / scale : 0.0;
+  c.violation = scale > 0 ? tally.viol / scale : 0.0;
+  const bool positive = std::isfinite(c.measure) && c.measure > 0;
+  const bool above_noise = tally.obj > kVerifyRay * tally.mag;
+  const bool small_violation = c.violation <= kVerifyRay * c.measure;
+  c.passed = positive && above_noise && small_violation;
+  c.detail = format_detail(
+      "Farkas certificate: rigorous L0(r) = %.3g; tolerance test L0/s = %.3g, violation/s = %.3g, "
+      "L0/sum|terms| = %.3g (%s)",
+      sb.bound, c.measure, c.violation, tally.mag > 0 ? tally.obj / tally.mag : 0.0,
+      c.passed ? "infeasibility shown within tolerance, not rounding-proof" : "FAIL");
   return c;
 }
 
+// A point x and a ray prove unboundedness when x is feasible (the gate's primal test) and the
+// ray, scaled to ‖d‖∞ = 1, lowers the objective by at least the ray tolerance while leaving the
+// recession cone by at most that tolerance relative to the decrease (reference
+// src/core/certificates.cpp:88-136; the same terms in the same order).
 CertificateCheck check_unboundedness_certificate(const Model& model, const std::vector<double>& x,
                                                  const std::vector<double>& ray) {
-  CertificateCheck c;  // certificates.cpp:88-136
+  CertificateCheck c;
   const int m = model.num_rows, n = model.num_cols;
   if (static_cast<int>(ray.size()) != n || static_cast<int>(x.size()) != n || n == 0) {
     c.detail = "no primal ray / point";
@@ -525,31 +561,23 @@ CertificateCheck check_unboundedness_certificate(const Model& model, const std::
     c.detail = "zero ray";
     return c;
   }
-  // 1. x is feasible (the gate's primal test); 2. d (‖d‖∞ = 1) decreases the objective and
-  // lies in the recession cone
-  const CheckReport rep = check_solution(model, x, std::vector<double>(m, 0.0));
+  const CheckReport point = check_solution(model, x, std::vector<double>(m, 0.0));
   std::vector<double> d(n);
-  double cd = 0.0, viol = 0.0;
+  double slope = 0.0, cone = 0.0;  // c'd in the model's sense; the largest step out of the cone
   for (int j = 0; j < n; ++j) {
     d[j] = ray[j] / dmax;
-    cd += model.sense * model.obj[j] * d[j];
-    if (std::isfinite(model.col_lower[j])) viol = std::max(viol, -d[j]);
-    if (std::isfinite(model.col_upper[j])) viol = std::max(viol, d[j]);
+    slope += model.sense * model.obj[j] * d[j];
+    cone = widen(cone, d[j], model.col_lower[j], model.col_upper[j]);
   }
   const std::vector<double> ad = model.row_activity(d);
-  for (int i = 0; i < m; ++i) {
-    if (std::isfinite(model.row_lower[i])) viol = std::max(viol, -ad[i]);
-    if (std::isfinite(model.row_upper[i])) viol = std::max(viol, ad[i]);
-  }
-  c.measure = -cd;
-  c.violation = viol;
-  const bool decreases = -cd >= kVerifyRay * std::max(1.0, cmax);
-  const bool in_cone = viol <= kVerifyRay * (-cd);
-  c.passed = rep.primal_ok && decreases && in_cone;
-  char buf[200];
-  std::snprintf(buf, sizeof buf, "unbounded ray: -c'd = %.3g, cone violation %.3g, point primal violation %.3g (%s)",
-                -cd, viol, rep.max_primal_violation, c.passed ? "unboundedness proven" : "FAIL");
-  c.detail = buf;
+  for (int i = 0; i < m; ++i) cone = widen(cone, ad[i], model.row_lower[i], model.row_upper[i]);
+  c.measure = -slope;
+  c.violation = cone;
+  const bool decreases = -slope >= kVerifyRay * std::max(1.0, cmax);
+  const bool in_cone = cone <= kVerifyRay * (-slope);
+  c.passed = point.primal_ok && decreases && in_cone;
+  c.detail = format_detail("unbounded ray: -c'd = %.3g, cone violation %.3g, point primal violation %.3g (%s)",
+                           -slope, cone, point.max_primal_violation, c.passed ? "unboundedness proven" : "FAIL");
   return c;
 }
 

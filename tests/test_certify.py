@@ -103,3 +103,28 @@ def test_invalid_arguments():
     ri[0] = lp.num_rows  # a row index out of range
     with pytest.raises(ValueError):
         ps26119.certified_bound(lp.with_data(row_index=ri), np.zeros(lp.num_rows))
+
+
+def test_certificate_tests_with_infinite_bounds_match_reference(ref):
+    """Both certificate tests on models whose rows and columns are one-sided, free or boxed, with
+    random multipliers, points and rays: every field (passed, rigorous, measure, violation) equals
+    the reference's, so the infinite-bound branches (a picked bound that is infinite counts as a
+    violation; the recession cone only constrains the finite sides) take the same terms in the
+    same order."""
+    rng = np.random.default_rng(12)
+    for trial in range(12):
+        lp = g.random_lp(300, seed=20 + trial)
+        m, n = lp.num_rows, lp.num_cols
+        kind_r = rng.integers(0, 4, m)  # 0 equality, 1 >=, 2 <=, 3 free
+        b = lp.row_lower.copy()
+        rl = np.where((kind_r == 2) | (kind_r == 3), -np.inf, b - (kind_r == 1) * rng.uniform(0, 1, m))
+        ru = np.where((kind_r == 1) | (kind_r == 3), np.inf, b + (kind_r == 2) * rng.uniform(0, 1, m))
+        kind_c = rng.integers(0, 4, n)  # 0 boxed, 1 lower only, 2 upper only, 3 free
+        cl = np.where((kind_c == 2) | (kind_c == 3), -np.inf, 0.0)
+        cu = np.where((kind_c == 1) | (kind_c == 3), np.inf, 10.0)
+        model = lp.with_data(row_lower=rl, row_upper=ru, col_lower=cl, col_upper=cu)
+        r = rng.standard_normal(m) * (rng.uniform(0, 1, m) < 0.7)
+        assert ps26119.check_certificate(model, r) == ref.certificate(model, r), trial
+        x = np.clip(rng.uniform(-1, 11, n), np.where(np.isfinite(cl), cl, -1e3), np.where(np.isfinite(cu), cu, 1e3))
+        ray = rng.standard_normal(n) * (rng.uniform(0, 1, n) < 0.5)
+        assert ps26119.check_certificate(model, ray, x=x) == ref.certificate(model, ray, x=x), trial
