@@ -12,6 +12,9 @@
 // Every solve runs on the GPU (--gpu is accepted for compatibility and implied).
 // Exit codes as the reference's: 0 optimal, 1 infeasible / unbounded / limit, 2 usage,
 // 3 read error, 4 cannot write the output, 5 numerical error / not solved.
+#include <sys/stat.h>
+#include <unistd.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -72,15 +75,14 @@ double number_arg(const char* flag, const char* s) {
   return v;
 }
 
-bool writable(const std::string& path) {  // fails fast instead of after a long solve
-  std::FILE* probe = std::fopen(path.c_str(), "r");
-  const bool existed = probe != nullptr;
-  if (probe) std::fclose(probe);
-  std::FILE* f = std::fopen(path.c_str(), "a");
-  if (!f) return false;
-  std::fclose(f);
-  if (!existed) std::remove(path.c_str());
-  return true;
+// Whether the solution file can be written, checked before a long solve rather than after it:
+// an existing file must be writable in place; a new one must be creatable in its directory.
+bool writable(const std::string& path) {
+  struct stat st;
+  if (::stat(path.c_str(), &st) == 0) return !S_ISDIR(st.st_mode) && ::access(path.c_str(), W_OK) == 0;
+  const std::size_t slash = path.find_last_of('/');
+  const std::string dir = slash == std::string::npos ? "." : (slash == 0 ? "/" : path.substr(0, slash));
+  return ::access(dir.c_str(), W_OK | X_OK) == 0;
 }
 
 bool load(const std::string& path, Model& m, ModelInfo& info) {

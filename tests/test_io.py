@@ -197,6 +197,20 @@ def test_cli_usage_errors():
     assert cli("--version").stdout.startswith("ps26119")
 
 
+def test_cli_refuses_an_unwritable_solution_file_before_solving(tmp_path):
+    """Exit code 4 (write error) before the model is solved: a missing directory, a directory
+    given as the file; a new file in a writable directory is accepted (the solve then runs)."""
+    mps = tmp_path / "tiny.mps"
+    mps.write_text("NAME TINY\nROWS\n N COST\n L LIM1\nCOLUMNS\n X1 COST 1.0 LIM1 1.0\nRHS\n RHS LIM1 4.0\n"
+                   "BOUNDS\n UP BND X1 4.0\nENDATA\n")
+    for out in (tmp_path / "missing" / "x.sol", tmp_path):
+        r = cli("solve", mps, "--out", out)
+        assert r.returncode == 4 and "cannot write the solution file" in r.stderr, (out, r.stderr)
+        assert "status" not in r.stdout  # nothing was solved
+    r = cli("solve", mps, "--out", tmp_path / "new.sol")
+    assert r.returncode != 4 and "cannot write" not in r.stderr
+
+
 # ------------------------------------------------------------------------------- GPU
 def parse_sol(path):
     head, cols = {}, []
