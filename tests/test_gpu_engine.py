@@ -1,6 +1,6 @@
 """The full r²HPDHG solve on the GPU against the reference CPU engine, through the C ABI.
 
-Parity bars (the north-star contract, stated per test):
+Parity bars (stated per test):
   * exact mode (reference summation order): the trajectory is BIT-IDENTICAL to the reference
     CPU engine — same status, same iteration count, identical x, y, z and objective.
   * fast mode (tree order for the decision-only sums): same status, iteration count within one
@@ -75,7 +75,7 @@ def fast_mode_bar(name, s, r):
     objectives, ray tests, the restart residual); every sum that enters the iterates' arithmetic
     (scaling, ‖Ã‖₂, ω0, the PID distances) is in the reference's order. So the trajectory is the
     reference's unless a decision lands within rounding of its threshold, and the bar is the
-    north star's: iteration count within one check (K = 64), objective within 1e-9 relative."""
+    iteration count within one check (K = 64) and the objective within 1e-9 relative."""
     assert abs(s.iterations - r.iterations) <= K, (s.iterations, r.iterations)
     assert abs(s.objective - r.objective) <= REL_OBJ * (1 + abs(r.objective))
 
