@@ -16,6 +16,7 @@
 #include <unistd.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -128,7 +129,9 @@ int info_one(const char* path, PresolveResult& r) {
   }
   // what the safe presolve (R1-R4) would do, and a digest of all its decisions
   if (m.validate().empty()) {
+    const auto t0 = std::chrono::steady_clock::now();
     presolve_into(m, r);
+    const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     const char* what = r.outcome == PresolveResult::Outcome::Reduced      ? "reduced"
                        : r.outcome == PresolveResult::Outcome::Infeasible ? "infeasible"
                                                                            : "unchanged";
@@ -138,6 +141,7 @@ int info_one(const char* path, PresolveResult& r) {
       std::printf("  reduced            %d rows, %d columns, %zu nonzeros\n", r.reduced.num_rows, r.reduced.num_cols,
                   r.reduced.nnz());
     std::printf("  presolve digest    %016llx\n", static_cast<unsigned long long>(presolve_digest(r)));
+    std::printf("  presolve time      %.1f ms\n", ms);
   }
   return 0;
 }
